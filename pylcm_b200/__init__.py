@@ -1,0 +1,78 @@
+"""pylcm_b200: a B200-native backward-induction solver with PyLCM's model API.
+
+Declare a model with the same objects as PyLCM (``Model``, ``Regime``, grids,
+processes, ``MarkovTransition``, ``categorical``) and call
+``model.solve(params=...)`` / ``model.simulate(...)``.  Model functions are
+lowered to CUDA C, compiled with NVRTC for sm_100a and run by the kernels in
+``pylcm_b200/csrc`` through the C-ABI library ``liblcmx.so``.
+"""
+
+from pylcm_b200 import jnp
+from pylcm_b200.ages import AgeGrid
+from pylcm_b200.exceptions import (
+    AdmissionError,
+    GridInitializationError,
+    InvalidParamsError,
+    InvalidValueFunctionError,
+    KernelError,
+    ModelInitializationError,
+    PyLCMError,
+    RegimeInitializationError,
+    TracingError,
+)
+from pylcm_b200.grids import (
+    DiscreteGrid,
+    IrregSpacedGrid,
+    LinSpacedGrid,
+    LogSpacedGrid,
+    categorical,
+)
+from pylcm_b200.model import Model
+from pylcm_b200.processes import (
+    LogNormalIIDProcess,
+    NormalIIDProcess,
+    RouwenhorstAR1Process,
+    TauchenAR1Process,
+    UniformIIDProcess,
+)
+from pylcm_b200.regime import (
+    ConsumptionSavingsRegime,
+    ExtremeValueTasteShocks,
+    LiquidMargin,
+    MarkovTransition,
+    Regime,
+)
+from pylcm_b200.solvers import DCEGM, FUESEnvelope, GridSearch
+
+__all__ = [
+    "DCEGM",
+    "AdmissionError",
+    "AgeGrid",
+    "ConsumptionSavingsRegime",
+    "DiscreteGrid",
+    "ExtremeValueTasteShocks",
+    "FUESEnvelope",
+    "GridInitializationError",
+    "GridSearch",
+    "InvalidParamsError",
+    "InvalidValueFunctionError",
+    "IrregSpacedGrid",
+    "KernelError",
+    "LinSpacedGrid",
+    "LiquidMargin",
+    "LogNormalIIDProcess",
+    "LogSpacedGrid",
+    "MarkovTransition",
+    "Model",
+    "ModelInitializationError",
+    "NormalIIDProcess",
+    "PyLCMError",
+    "Regime",
+    "RegimeInitializationError",
+    "RouwenhorstAR1Process",
+    "TauchenAR1Process",
+    "TracingError",
+    "UniformIIDProcess",
+    "categorical",
+    "jnp",
+]

@@ -1,0 +1,41 @@
+"""Exception classes, named after the reference's (``src/lcm/exceptions.py``)."""
+
+
+class PyLCMError(Exception):
+    """Base class for all errors raised by this package."""
+
+
+class GridInitializationError(PyLCMError):
+    """A grid or process was declared with invalid arguments."""
+
+
+class RegimeInitializationError(PyLCMError):
+    """A regime was declared with invalid arguments."""
+
+
+class ModelInitializationError(PyLCMError):
+    """A model could not be built from its regimes."""
+
+
+class InvalidParamsError(PyLCMError):
+    """The params passed to solve/simulate do not match the model."""
+
+
+class InvalidValueFunctionError(PyLCMError):
+    """A solved value function contains NaN."""
+
+
+class TracingError(PyLCMError):
+    """A model function uses a construct the CUDA lowering does not support."""
+
+
+class KernelError(PyLCMError):
+    """The native library reported a failure (compile, launch, bounded wait, ...)."""
+
+    def __init__(self, status: int, message: str) -> None:
+        super().__init__(f"[lcmx status {status}] {message}")
+        self.status = status
+
+
+class AdmissionError(PyLCMError):
+    """A serving request does not fit the configured HBM budget."""
