@@ -1,0 +1,114 @@
+/*
+ * lcmx.h -- C ABI of the B200 backward-induction solver (liblcmx.so).
+ *
+ * The reference (OpenSourceEconomics/pylcm) has no foreign-function boundary
+ * on its solve path: the per-period step is a JAX program dispatched from the
+ * Python loop in src/_lcm/solution/backward_induction.py:155-275.  The entry
+ * points below replace, one for one, the calls that loop makes:
+ *
+ *   lcmx_module_compile  <- AOT compile of the per-period cores,
+ *                           backward_induction.py:577-720 (jax.jit(...).lower
+ *                           .compile); here NVRTC for sm_100a, cached by key.
+ *   lcmx_bellman_step    <- _GridSearchPeriodKernel.__call__,
+ *                           src/_lcm/solution/grid_search.py:192-212 (the
+ *                           max_Q_over_a program, max_Q_over_a.py:30-191).
+ *   lcmx_expectation     <- the continuation expectation inside Q_and_F,
+ *                           src/_lcm/regime_building/Q_and_F.py:466-681 and
+ *                           _expectation_over_stochastic_nodes :1145-1209.
+ *   lcmx_simulate        <- the per-period simulation step,
+ *                           src/_lcm/simulation/simulate.py:465-668.
+ *   lcmx_egm_step        <- the DC-EGM per-period core,
+ *                           src/_lcm/egm/step_core.py:156-312.
+ *   lcmx_count_nonfinite <- the per-period NaN/Inf diagnostics,
+ *                           backward_induction.py:205-236.
+ *
+ * Conventions: every pointer argument that names array data is a DEVICE
+ * pointer; sizes are element counts; `stream` is a cudaStream_t (NULL = the
+ * legacy default stream).  Every function returns an int status (LCMX_OK = 0)
+ * and never frees caller memory; the message of the last failure on a
+ * context is returned by lcmx_last_error.
+ */
+#ifndef LCMX_H
+#define LCMX_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  LCMX_OK = 0,
+  LCMX_ERR_ARGS = 1,      /* invalid argument (null pointer, bad size)     */
+  LCMX_ERR_COMPILE = 2,   /* NVRTC rejected the generated source           */
+  LCMX_ERR_MODULE = 3,    /* module load failed or kernel symbol missing   */
+  LCMX_ERR_LAUNCH = 4,    /* kernel launch failed                          */
+  LCMX_ERR_CUDA = 5,      /* other CUDA runtime / driver failure           */
+  LCMX_ERR_NOMEM = 6,     /* device memory exhausted                       */
+  LCMX_ERR_TIMEOUT = 7    /* a bounded device-side wait gave up            */
+};
+
+typedef struct lcmx_ctx lcmx_ctx;
+typedef struct lcmx_module lcmx_module;
+
+/* One launch of a generated kernel over a list of work items.
+ * `items` holds n_items records of 64-bit words whose layout is fixed by the
+ * code generator for that kernel; `tile_prefix[i]` is the first tile of item
+ * i and tile_prefix[n_items] the total tile count.  grid == 0 selects
+ * (SM count x resident CTAs per SM). */
+typedef struct {
+  const void* items;
+  const int* tile_prefix;
+  int n_items;
+  int n_tiles;
+  int grid;
+  int block;
+  int smem_bytes;
+} lcmx_launch_args;
+
+/* Create / destroy a context bound to CUDA device `device` (primary context). */
+int lcmx_ctx_create(int device, lcmx_ctx** out);
+int lcmx_ctx_destroy(lcmx_ctx* ctx);
+/* Message of the last failure on ctx (never NULL; "" after success). */
+const char* lcmx_last_error(const lcmx_ctx* ctx);
+/* Device facts used for grid sizing and HBM admission. */
+int lcmx_device_info(lcmx_ctx* ctx, int* sm_count, size_t* free_bytes, size_t* total_bytes);
+
+/* Compile CUDA C for sm_100a with NVRTC and load it.  `key` names the source
+ * in the in-process and on-disk cubin caches; `options` is a '\n'-separated
+ * list of extra NVRTC options (may be NULL). */
+int lcmx_module_compile(lcmx_ctx* ctx, const char* cuda_src, const char* key,
+                        const char* options, lcmx_module** out);
+int lcmx_module_destroy(lcmx_module* mod);
+/* Resident CTAs per SM of `kernel` at the given block size / dynamic smem. */
+int lcmx_occupancy(lcmx_module* mod, const char* kernel, int block, int smem_bytes,
+                   int* blocks_per_sm);
+
+/* Kernel (a): fused Q_and_F + max/argmax over actions for a batch of
+ * (solve instance, regime, period) items; writes V (double) and the flat
+ * argmax action index (int32) per state. */
+int lcmx_bellman_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
+                      void* stream);
+/* Kernel (b): EV[k, col] = sum_j W[k, j] V'[j, col] / sum_j W[k, j] for a batch
+ * of (instance, source regime, target regime) items. */
+int lcmx_expectation(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
+                     void* stream);
+/* Kernel (d): one simulated period for a batch of subjects (Philox-4x32-10
+ * counter RNG keyed by `seed`, subject and period). */
+int lcmx_simulate(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
+                  unsigned long long seed, void* stream);
+/* Kernel (c), part 1: DC-EGM Euler inversion and candidate generation. */
+int lcmx_egm_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
+                  void* stream);
+
+/* Count non-finite (and separately NaN) entries of a double array; the two
+ * counters are accumulated into counts_dev[0] (nan) and counts_dev[1]
+ * (+-inf), which the caller zeroes. */
+int lcmx_count_nonfinite(lcmx_ctx* ctx, const double* x, long long n,
+                         unsigned long long* counts_dev, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LCMX_H */

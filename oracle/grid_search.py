@@ -330,9 +330,22 @@ def bellman_step(
         V = np.where(has_nan, np.nan, V)
         mask = (Q == V[:, None]) & F
         pol = np.argmax(mask, axis=1).astype(np.int32)
+    # gap between the best and the second-best feasible action (inf if < 2)
+    Qg = np.where(F, np.nan_to_num(Q, nan=-np.inf), -np.inf)
+    if Qg.shape[1] >= 2:
+        top2 = np.partition(Qg, Qg.shape[1] - 2, axis=1)[:, -2:]
+        with np.errstate(invalid="ignore"):
+            gap = np.where(np.isfinite(top2[:, 0]), top2[:, 1] - top2[:, 0], np.inf)
+    else:
+        gap = np.full(Qg.shape[0], np.inf)
+    global LAST_GAP
+    LAST_GAP = gap
     if state_rows is None:
         return V.reshape(sshape), pol.reshape(sshape)
     return V, pol
+
+
+LAST_GAP = None
 
 
 def _lookup_table(deps, table, sidx_of, aidx_of, bshape, n_out):
@@ -444,9 +457,11 @@ def _expected_next_value(spec, tgt, resolver, ev, V_next, procs, sidx_of, aidx_o
         return num / np.where(den > 0.0, den, 1.0)
 
 
-def solve(model, params: dict) -> tuple[dict, dict]:
+def solve(model, params: dict, gaps: dict | None = None) -> tuple[dict, dict]:
     """Backward induction over all periods; returns (V, policy) dicts
-    ``{period: {regime: array}}`` like ``Model.solve``."""
+    ``{period: {regime: array}}`` like ``Model.solve``.  If `gaps` is a dict
+    it receives, per period and regime, the gap between the best and the
+    second-best feasible Q at every state (for argmax comparisons)."""
     specs = model.regime_specs
     resolver = ParamResolver(params, model.fixed_params, tuple(s.name for s in specs))
     T = model.n_periods
@@ -465,4 +480,6 @@ def solve(model, params: dict) -> tuple[dict, dict]:
             v, p = bellman_step(spec, specs, resolver, period, age, nxt)
             V[period][spec.name] = v
             pol[period][spec.name] = p
+            if gaps is not None:
+                gaps.setdefault(period, {})[spec.name] = LAST_GAP.reshape(spec.state_shape)
     return V, pol

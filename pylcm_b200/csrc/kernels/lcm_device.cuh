@@ -1,0 +1,188 @@
+// lcm_device.cuh -- hand-written device helpers shared by every generated
+// module (Bellman step, expectation contraction, simulation, DC-EGM).
+//
+// This header is prepended to the CUDA C that the Python code generator emits
+// for one model regime and the whole translation unit is compiled by NVRTC for
+// sm_100a.  It must stay free of host code and of any #include (NVRTC builds
+// it without the CUDA toolkit headers).
+//
+// Semantics follow the reference solve path:
+//   * zero-safe weighted term: w * v, with w == 0 annihilating +-inf / nan
+//     (src/_lcm/zero_safe.py:161-251);
+//   * linear interpolation with extrapolation, lower index clipped to
+//     [0, n-2] (src/_lcm/regime_building/ndimage.py:29-109);
+//   * grid coordinates for lin / log / irregular grids
+//     (src/_lcm/grids/coordinates.py:30-167);
+//   * argmax = first flat action index attaining the maximum over feasible
+//     actions, max initialised at -inf (max_Q_over_a.py:160, argmax.py:6-69).
+
+#pragma once
+
+typedef long long i64;
+typedef unsigned long long u64;
+typedef unsigned int u32;
+
+#define LCM_INF (__longlong_as_double(0x7ff0000000000000LL))
+#define LCM_NAN (__longlong_as_double(0x7ff8000000000000LL))
+
+template <typename T> struct lcm_lim;
+template <> struct lcm_lim<double> {
+  static __device__ __forceinline__ double inf() { return __longlong_as_double(0x7ff0000000000000LL); }
+  static __device__ __forceinline__ double nan() { return __longlong_as_double(0x7ff8000000000000LL); }
+};
+template <> struct lcm_lim<float> {
+  static __device__ __forceinline__ float inf() { return __int_as_float(0x7f800000); }
+  static __device__ __forceinline__ float nan() { return __int_as_float(0x7fc00000); }
+};
+
+__device__ __forceinline__ bool lcm_isfinite(double x) {
+  return (__double_as_longlong(x) & 0x7ff0000000000000LL) != 0x7ff0000000000000LL;
+}
+__device__ __forceinline__ bool lcm_isfinite(float x) {
+  return (__float_as_int(x) & 0x7f800000) != 0x7f800000;
+}
+__device__ __forceinline__ bool lcm_isnan(double x) { return x != x; }
+__device__ __forceinline__ bool lcm_isnan(float x) { return x != x; }
+
+// item-record word accessors (records are arrays of 64-bit words)
+__device__ __forceinline__ double lcm_wd(const i64* it, int k) { return __longlong_as_double(it[k]); }
+__device__ __forceinline__ int lcm_wi(const i64* it, int k) { return (int)it[k]; }
+template <typename P> __device__ __forceinline__ P* lcm_wp(const i64* it, int k) {
+  return reinterpret_cast<P*>(it[k]);
+}
+
+// w * v, exactly 0 where w == 0 whatever v is (zero_safe_weighted_term).
+template <typename T> __device__ __forceinline__ T lcm_zs(T w, T v) {
+  return (w == T(0) && !lcm_isfinite(v)) ? T(0) : w * v;
+}
+
+// Lower bracket index of a fractional coordinate: clip(floor(c), 0, n-2).
+template <typename T> __device__ __forceinline__ int lcm_lower(T c, int n) {
+  T f = floor(c);
+  T hi = (T)(n - 2);
+  f = f < T(0) ? T(0) : f;
+  f = f > hi ? hi : f;
+  return (f == f) ? (int)f : 0;
+}
+
+// Coordinate of x on a linearly spaced grid: (x - start) / step, computed as
+// a multiply by the host-supplied reciprocal of the step.
+template <typename T> __device__ __forceinline__ T lcm_coord_lin(T x, T start, T inv_step) {
+  return (x - start) * inv_step;
+}
+
+// Coordinate on a log-spaced grid (coordinates.py:73-114): rank in log space,
+// then the linear position between the two bracketing grid points.
+template <typename T>
+__device__ __forceinline__ T lcm_coord_log(T x, T log_start, T log_step) {
+  T lv = log(x);
+  T c = (lv - log_start) / log_step;
+  T lo = floor(c);
+  T lower = exp(log_start + log_step * lo);
+  T upper = exp(log_start + log_step * (lo + T(1)));
+  return lo + (x - lower) / (upper - lower);
+}
+
+// Coordinate on an irregular ascending grid (coordinates.py:117-167):
+// searchsorted(side="right") clipped to [1, n-1], then linear position.
+template <typename T>
+__device__ __forceinline__ T lcm_coord_irreg(T x, const double* __restrict__ pts, int n) {
+  if (n == 1) return T(0);
+  int lo = 0, hi = n;  // first index with pts[i] > x
+  double xd = (double)x;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (pts[mid] > xd) hi = mid; else lo = mid + 1;
+  }
+  int up = lo < 1 ? 1 : (lo > n - 1 ? n - 1 : lo);
+  int low = up - 1;
+  T pl = (T)pts[low], pu = (T)pts[up];
+  return (T)low + (x - pl) / (pu - pl);
+}
+
+// 1-D linear read with extrapolation; `row` is contiguous.
+template <typename T, typename S>
+__device__ __forceinline__ T lcm_interp1(const S* __restrict__ row, int n, T c) {
+  int lo = lcm_lower(c, n);
+  T wu = c - (T)lo;
+  T wl = T(1) - wu;
+  T v0 = (T)row[lo];
+  T v1 = (T)row[lo + 1];
+  return lcm_zs(wl, v0) + lcm_zs(wu, v1);
+}
+
+// 2-D bilinear read; `blk` is an (n0 x n1) row-major block.  Corner order and
+// left-to-right summation follow map_coordinates (ndimage.py:71-97).
+template <typename T, typename S>
+__device__ __forceinline__ T lcm_interp2(const S* __restrict__ blk, int n0, int n1, T c0, T c1) {
+  int l0 = lcm_lower(c0, n0), l1 = lcm_lower(c1, n1);
+  T u0 = c0 - (T)l0, u1 = c1 - (T)l1;
+  T d0 = T(1) - u0, d1 = T(1) - u1;
+  const S* r0 = blk + (i64)l0 * n1;
+  const S* r1 = r0 + n1;
+  T acc = lcm_zs(d0 * d1, (T)r0[l1]);
+  acc = acc + lcm_zs(d0 * u1, (T)r0[l1 + 1]);
+  acc = acc + lcm_zs(u0 * d1, (T)r1[l1]);
+  acc = acc + lcm_zs(u0 * u1, (T)r1[l1 + 1]);
+  return acc;
+}
+
+// Running (max, first argmax, nan) over feasible actions.
+template <typename T> struct LcmBest {
+  T v;
+  int idx;   // -1: no feasible action seen yet
+  int nan;   // a feasible action produced NaN
+  __device__ __forceinline__ void init() { v = -lcm_lim<T>::inf(); idx = -1; nan = 0; }
+  __device__ __forceinline__ void push(T q, int a) {
+    if (q != q) { nan = 1; return; }
+    if (idx < 0 || q > v) { v = q; idx = a; }
+  }
+  // merge with another partial result over a disjoint action set; ties go to
+  // the smaller flat index, so the result equals the sequential first argmax.
+  __device__ __forceinline__ void merge(T ov, int oidx, int onan) {
+    nan |= onan;
+    if (oidx < 0) return;
+    if (idx < 0 || ov > v || (ov == v && oidx < idx)) { v = ov; idx = oidx; }
+  }
+};
+
+// Combine LANES consecutive lanes (a power of two <= 32) holding partial
+// results for the same state, with warp shuffles.
+template <int LANES, typename T>
+__device__ __forceinline__ void lcm_group_reduce(LcmBest<T>& b) {
+#pragma unroll
+  for (int off = LANES >> 1; off > 0; off >>= 1) {
+    T ov = __shfl_xor_sync(0xffffffffu, b.v, off);
+    int oi = __shfl_xor_sync(0xffffffffu, b.idx, off);
+    int on = __shfl_xor_sync(0xffffffffu, b.nan, off);
+    b.merge(ov, oi, on);
+  }
+}
+
+// Tile -> item lookup: prefix[i] is the first tile of item i, prefix[n] = total.
+__device__ __forceinline__ int lcm_find_item(const int* __restrict__ prefix, int n_items, int tile) {
+  int lo = 0, hi = n_items - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Logsum over discrete choices with max shift (logsum.py:32-64).
+template <typename T, int ND>
+__device__ __forceinline__ T lcm_logsum(const T* vals, T scale) {
+  T vmax = -lcm_lim<T>::inf();
+#pragma unroll
+  for (int d = 0; d < ND; ++d) vmax = vals[d] > vmax ? vals[d] : vmax;
+  T fin = (vmax == -lcm_lim<T>::inf()) ? T(0) : vmax;
+  T m = -lcm_lim<T>::inf();
+  T sh[ND];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) { sh[d] = (vals[d] - fin) / scale; m = sh[d] > m ? sh[d] : m; }
+  if (!lcm_isfinite(m)) m = T(0);
+  T s = T(0);
+#pragma unroll
+  for (int d = 0; d < ND; ++d) s += exp(sh[d] - m);
+  return fin + scale * (log(s) + m);
+}

@@ -1,0 +1,366 @@
+"""Backward induction on the GPU.
+
+Restates the reference's solve loop (``src/_lcm/solution/backward_induction.py:44-302``)
+B200-first: for a batch of solve *instances* (parameter vectors of one model
+structure) every buffer is allocated once, the 64-bit item records of every
+launch of every period are packed on the host and uploaded in one copy, and
+the per-period work is a fixed list of kernel launches:
+
+    for period = T-1 .. 0:
+        kernel (b) for every (source regime, target regime) with stochastic
+                   target axes  -> EV buffers
+        kernel (a) for every regime active in the period -> V, policy
+
+Each launch covers all instances.  The launch list has no host
+synchronisation, so it can be replayed inside a CUDA graph
+(``SolvePlan.run_graph``).  V arrays stay on the device between periods.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import hashlib
+import math
+import struct
+from typing import Any, Sequence
+
+import numpy as np
+
+from pylcm_b200.codegen import LaunchConfig, RegimeKernels
+from pylcm_b200.exceptions import ModelInitializationError
+from pylcm_b200.spec import ParamResolver, RegimeSpec, TracedRegime, trace_regime
+
+
+def _f2w(x: float) -> int:
+    return struct.unpack("<q", struct.pack("<d", float(x)))[0]
+
+
+@dataclasses.dataclass
+class Launch:
+    kind: str  # 'bellman' | 'expect'
+    module: Any
+    kernel: str
+    item_off: int  # word offset into the item buffer
+    prefix_off: int  # int offset into the prefix buffer
+    n_items: int
+    n_tiles: int
+    block: int
+    smem: int
+    period: int
+
+
+def default_config(spec: RegimeSpec, precision: str) -> LaunchConfig:
+    """Heuristic launch shape: few actions per state -> more lanes per state."""
+    n_a = spec.n_actions
+    n_s = spec.n_states
+    if n_s <= 4096 and n_a >= 64:
+        lanes = 32
+    elif n_s <= 65536 and n_a >= 64:
+        lanes = 4
+    else:
+        lanes = 1
+    chunk = 512 if precision == "fp32" else 256
+    return LaunchConfig(block=256, lanes=lanes, chunk=chunk)
+
+
+class SolveEngine:
+    """Compiles and runs the per-period kernels of one model structure."""
+
+    def __init__(self, model, precision: str = "fp64", configs: dict | None = None, device: int = 0) -> None:
+        self.model = model
+        self.precision = precision
+        self.configs = dict(configs or {})
+        self.device = device
+        self.specs = model.regime_specs
+        self._kernels: dict[tuple, RegimeKernels] = {}
+        self._traces: dict[tuple, TracedRegime] = {}
+
+    # ------------------------------------------------------------ helpers
+    def targets_at(self, spec: RegimeSpec, period: int) -> tuple[str, ...]:
+        if spec.terminal:
+            return ()
+        return tuple(s.name for s in self.specs if (period + 1) in s.active_periods)
+
+    def resolver(self, params) -> ParamResolver:
+        return ParamResolver(params, self.model.fixed_params, tuple(s.name for s in self.specs))
+
+    def config_for(self, spec: RegimeSpec) -> LaunchConfig:
+        return self.configs.get(spec.name) or default_config(spec, self.precision)
+
+    def kernels(self, spec: RegimeSpec, targets: tuple[str, ...], params) -> RegimeKernels:
+        cfg = self.config_for(spec)
+        key = (spec.name, targets, cfg)
+        rk = self._kernels.get(key)
+        if rk is None:
+            tr = trace_regime(spec, self.specs, self.resolver(params), targets)
+            by = {s.name: s for s in self.specs}
+            rk = RegimeKernels(tr, [by[t] for t in targets], self.precision, cfg)
+            src = rk.source()
+            rk.src = src
+            rk.key = "lcm_" + hashlib.sha1(src.encode()).hexdigest()[:24]
+            self._kernels[key] = rk
+        return rk
+
+    def module(self, rk: RegimeKernels):
+        from pylcm_b200.runtime import get_context
+
+        mod = getattr(rk, "module", None)
+        if mod is None:
+            ctx = get_context(self.device)
+            mod = ctx.compile(rk.src, rk.key)
+            rk.module = mod
+        return mod
+
+    # --------------------------------------------------------------- plan
+    def plan(self, params_list: Sequence) -> "SolvePlan":
+        return SolvePlan(self, list(params_list))
+
+    def solve(self, params) -> tuple[dict, dict]:
+        plan = self.plan([params])
+        plan.run()
+        return plan.result(0)
+
+    def solve_batch(self, params_list: Sequence) -> list[tuple[dict, dict]]:
+        plan = self.plan(params_list)
+        plan.run()
+        return [plan.result(i) for i in range(len(params_list))]
+
+
+class SolvePlan:
+    """Buffers, item records and the launch list for a batch of instances."""
+
+    def __init__(self, eng: SolveEngine, params_list: list) -> None:
+        import torch
+
+        self.eng = eng
+        self.torch = torch
+        model = eng.model
+        specs = eng.specs
+        T = model.n_periods
+        n = len(params_list)
+        if n == 0:
+            raise ValueError("empty batch")
+        self.n = n
+        dev = torch.device("cuda", eng.device)
+        self.dev = dev
+        fp32 = eng.precision == "fp32"
+        resolvers = [eng.resolver(p) for p in params_list]
+
+        # ---- per regime: slots (active periods), V / policy buffers, grids
+        self.slot: dict[str, dict[int, int]] = {}
+        self.V: dict[str, Any] = {}
+        self.pol: dict[str, Any] = {}
+        self.sgrid: dict[str, list] = {}
+        self.agrid: dict[str, list] = {}
+        for s in specs:
+            per = list(s.active_periods)
+            self.slot[s.name] = {p: k for k, p in enumerate(per)}
+            ns = s.n_states
+            self.V[s.name] = torch.empty((n, max(len(per), 1), ns), dtype=torch.float64, device=dev)
+            self.pol[s.name] = torch.empty((n, max(len(per), 1), ns), dtype=torch.int32, device=dev)
+            self.sgrid[s.name] = [
+                torch.as_tensor(ax.grid.to_numpy(), dtype=torch.float64, device=dev) if ax.kind == "continuous" else None
+                for ax in s.states
+            ]
+            self.agrid[s.name] = [
+                torch.as_tensor(ax.grid.to_numpy(), dtype=torch.float64, device=dev) if ax.kind == "continuous" else None
+                for ax in s.actions
+            ]
+
+        # ---- kernels per (regime, target set); params per (regime, target set)
+        by = {s.name: s for s in specs}
+        self.params: dict[tuple, Any] = {}
+        self.ev: dict[tuple, tuple] = {}
+        step_list: list[tuple[int, RegimeSpec, tuple, RegimeKernels]] = []
+        for period in range(T - 1, -1, -1):
+            for s in specs:
+                if period not in s.active_periods:
+                    continue
+                if not s.terminal and period == T - 1:
+                    raise ModelInitializationError(f"non-terminal regime {s.name} active in the last period")
+                targets = eng.targets_at(s, period)
+                rk = eng.kernels(s, targets, params_list[0])
+                key = (s.name, targets)
+                if key not in self.params:
+                    vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in resolvers]
+                    self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                step_list.append((period, s, targets, rk))
+        # EV buffers per (source, target set, target)
+        for period, s, targets, rk in step_list:
+            for t in rk.targets:
+                if t.scalar:
+                    continue
+                if not (t.needs_contraction or fp32):
+                    continue
+                k = (s.name, targets, t.spec.name)
+                if k in self.ev:
+                    continue
+                cblk = int(np.prod([t.spec.states[p].size for p in t.cont_pos])) if t.cont_pos else 1
+                ncols = int(np.prod([t.spec.states[p].size for p in t.det_pos])) * cblk if t.det_pos else cblk
+                e64 = torch.empty((n, t.K, ncols), dtype=torch.float64, device=dev)
+                e32 = torch.empty((n, t.K, ncols), dtype=torch.float32, device=dev) if fp32 else None
+                self.ev[k] = (e64, e32, ncols, cblk)
+
+        # ---- item records
+        words: list[np.ndarray] = []
+        prefixes: list[np.ndarray] = []
+        self.launches: list[Launch] = []
+        w_off = 0
+        p_off = 0
+
+        def add_launch(kind, rk, kernel, recs, tiles_per_item, block, smem, period):
+            nonlocal w_off, p_off
+            arr = np.stack(recs).astype(np.int64)
+            pre = np.zeros(len(recs) + 1, dtype=np.int32)
+            pre[1:] = np.cumsum(tiles_per_item)
+            words.append(arr.ravel())
+            prefixes.append(pre)
+            self.launches.append(
+                Launch(kind, rk, kernel, w_off, p_off, len(recs), int(pre[-1]), block, smem, period)
+            )
+            w_off += arr.size
+            p_off += pre.size
+            # keep the prefix offsets 16-byte aligned for the device pointer math
+            pad = (-p_off) % 4
+            if pad:
+                prefixes.append(np.zeros(pad, dtype=np.int32))
+                p_off += pad
+
+        ages = model.ages.values
+        for period, s, targets, rk in step_list:
+            age = float(ages[period])
+            pbuf = self.params[(s.name, targets)]
+            plen = pbuf.shape[1]
+            # kernel (b) launches
+            for t in rk.targets:
+                if t.scalar:
+                    continue
+                if not (t.needs_contraction or fp32):
+                    continue
+                e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
+                Vt = self.V[t.spec.name]
+                tslot = self.slot[t.spec.name][period + 1]
+                recs = []
+                for i in range(n):
+                    r = np.zeros(rk.e_words_for(t), dtype=np.int64)
+                    r[0] = Vt[i, tslot].data_ptr()
+                    r[1] = e64[i].data_ptr()
+                    r[2] = e32[i].data_ptr() if e32 is not None else 0
+                    r[3] = pbuf[i].data_ptr()
+                    r[4] = period
+                    r[5] = _f2w(age)
+                    r[6] = cblk
+                    r[7] = ncols
+                    for k, ax in enumerate(t.spec.states):
+                        r[8 + k] = ax.size
+                    recs.append(r)
+                tiles = [math.ceil(ncols / 256)] * n
+                add_launch("expect", rk, rk.expect_name(t), recs, tiles, 256, 0, period)
+            # kernel (a)
+            slot = self.slot[s.name][period]
+            recs = []
+            for i in range(n):
+                r = np.zeros(rk.n_words, dtype=np.int64)
+                r[rk.W_P] = pbuf[i].data_ptr()
+                r[rk.W_V] = self.V[s.name][i, slot].data_ptr()
+                r[rk.W_POL] = self.pol[s.name][i, slot].data_ptr()
+                r[rk.W_PERIOD] = period
+                r[rk.W_AGE] = _f2w(age)
+                r[rk.W_NSTATES] = s.n_states
+                r[rk.W_NACT] = s.n_actions
+                for k, ax in enumerate(s.states):
+                    r[rk.W_SSIZE + k] = ax.size
+                    g = self.sgrid[s.name][k]
+                    r[rk.W_SGRID + k] = g.data_ptr() if g is not None else 0
+                for k, ax in enumerate(s.actions):
+                    r[rk.W_ASIZE + k] = ax.size
+                    g = self.agrid[s.name][k]
+                    r[rk.W_AGRID + k] = g.data_ptr() if g is not None else 0
+                r[rk.W_TASTE] = _f2w(rk.tr.taste_scale if rk.tr.taste_scale else 0.0)
+                if s.taste_shocks:
+                    r[rk.W_TASTE] = _f2w(resolvers[i].taste_scale(s.name))
+                for t in rk.targets:
+                    tV = self.V[t.spec.name]
+                    tslot = self.slot[t.spec.name][period + 1]
+                    if t.scalar:
+                        r[t.w_scalar] = tV[i, tslot].data_ptr()
+                        continue
+                    if t.needs_contraction or fp32:
+                        e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
+                        r[t.w_ev64] = e64[i].data_ptr()
+                        r[t.w_ev32] = e32[i].data_ptr() if e32 is not None else 0
+                    else:
+                        r[t.w_ev64] = tV[i, tslot].data_ptr()
+                        r[t.w_ev32] = 0
+                    for k, ax in enumerate(t.spec.states):
+                        r[t.w_sizes + k] = ax.size
+                    for ci, pos in enumerate(t.cont_pos):
+                        ax = t.spec.states[pos]
+                        kind, a, b, npts = ax.grid.coordinate_spec()
+                        base = t.w_coord + 3 * ci
+                        if kind == "lin":
+                            r[base] = _f2w(a)
+                            r[base + 1] = _f2w(1.0 / b if npts > 1 else 0.0)
+                        elif kind == "log":
+                            r[base] = _f2w(a)
+                            r[base + 1] = _f2w(b)
+                        else:
+                            r[base + 2] = self.sgrid[t.spec.name][pos].data_ptr()
+                recs.append(r)
+            spt = rk.cfg.states_per_tile
+            tiles = [math.ceil(s.n_states / spt)] * n
+            add_launch("bellman", rk, rk.bellman_name(), recs, tiles, rk.cfg.block, rk.smem_bytes, period)
+
+        self.items = torch.as_tensor(np.concatenate(words), dtype=torch.int64, device=dev)
+        self.prefix = torch.as_tensor(np.concatenate(prefixes), dtype=torch.int32, device=dev)
+        for rk in {id(l.module): l.module for l in self.launches}.values():
+            eng.module(rk)
+        self.graph = None
+
+    # ---------------------------------------------------------------- run
+    def run(self, stream: int | None = None) -> None:
+        torch = self.torch
+        if stream is None:
+            stream = torch.cuda.current_stream(self.dev).cuda_stream
+        ib = self.items.data_ptr()
+        pb = self.prefix.data_ptr()
+        for l in self.launches:
+            mod = l.module.module
+            ip = ib + 8 * l.item_off
+            pp = pb + 4 * l.prefix_off
+            if l.kind == "bellman":
+                mod.bellman_step(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
+            else:
+                mod.expectation(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
+
+    def capture(self) -> None:
+        """Capture the launch list in a CUDA graph (replayed by run_graph)."""
+        torch = self.torch
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(self.dev)
+        s.wait_stream(torch.cuda.current_stream(self.dev))
+        with torch.cuda.stream(s):
+            self.run(s.cuda_stream)  # warm-up (module attributes, caches)
+        torch.cuda.current_stream(self.dev).wait_stream(s)
+        with torch.cuda.graph(g):
+            self.run(torch.cuda.current_stream(self.dev).cuda_stream)
+        self.graph = g
+
+    def run_graph(self) -> None:
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    @property
+    def gpu_launches(self) -> int:
+        return len(self.launches)
+
+    def result(self, i: int) -> tuple[dict, dict]:
+        V: dict[int, dict[str, Any]] = {}
+        P: dict[int, dict[str, Any]] = {}
+        for s in self.eng.specs:
+            for period, k in self.slot[s.name].items():
+                shape = s.state_shape
+                V.setdefault(period, {})[s.name] = self.V[s.name][i, k].reshape(shape)
+                P.setdefault(period, {})[s.name] = self.pol[s.name][i, k].reshape(shape)
+        return dict(sorted(V.items())), dict(sorted(P.items()))

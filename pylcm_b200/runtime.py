@@ -1,0 +1,171 @@
+"""ctypes binding of liblcmx.so (the C ABI in include/lcmx.h).
+
+The library is built in-tree (``pylcm_b200/_lib/liblcmx.so``).  There is no
+fallback: if the library or a GPU is missing, solving raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import threading
+from pathlib import Path
+
+from pylcm_b200.exceptions import KernelError
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "liblcmx.so"
+
+EXPORTED = (
+    "lcmx_ctx_create",
+    "lcmx_ctx_destroy",
+    "lcmx_last_error",
+    "lcmx_device_info",
+    "lcmx_module_compile",
+    "lcmx_module_destroy",
+    "lcmx_occupancy",
+    "lcmx_bellman_step",
+    "lcmx_expectation",
+    "lcmx_simulate",
+    "lcmx_egm_step",
+    "lcmx_count_nonfinite",
+)
+
+
+class LaunchArgs(ctypes.Structure):
+    _fields_ = [
+        ("items", ctypes.c_void_p),
+        ("tile_prefix", ctypes.c_void_p),
+        ("n_items", ctypes.c_int),
+        ("n_tiles", ctypes.c_int),
+        ("grid", ctypes.c_int),
+        ("block", ctypes.c_int),
+        ("smem_bytes", ctypes.c_int),
+    ]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def load_library() -> ctypes.CDLL:
+    """Load liblcmx.so (building it first if the sources are newer)."""
+    global _lib
+    with _lib_lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            from pylcm_b200 import build as _build
+
+            try:
+                _build.build()
+            except Exception as e:  # noqa: BLE001
+                raise KernelError(-1, f"liblcmx.so is missing and could not be built: {e}") from e
+        lib = ctypes.CDLL(str(LIB_PATH))
+        vp, ip, cp = ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p
+        sig = {
+            "lcmx_ctx_create": ([ip, ctypes.POINTER(vp)], ip),
+            "lcmx_ctx_destroy": ([vp], ip),
+            "lcmx_last_error": ([vp], cp),
+            "lcmx_device_info": ([vp, ctypes.POINTER(ip), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)], ip),
+            "lcmx_module_compile": ([vp, cp, cp, cp, ctypes.POINTER(vp)], ip),
+            "lcmx_module_destroy": ([vp], ip),
+            "lcmx_occupancy": ([vp, cp, ip, ip, ctypes.POINTER(ip)], ip),
+            "lcmx_bellman_step": ([vp, cp, ctypes.POINTER(LaunchArgs), vp], ip),
+            "lcmx_expectation": ([vp, cp, ctypes.POINTER(LaunchArgs), vp], ip),
+            "lcmx_simulate": ([vp, cp, ctypes.POINTER(LaunchArgs), ctypes.c_ulonglong, vp], ip),
+            "lcmx_egm_step": ([vp, cp, ctypes.POINTER(LaunchArgs), vp], ip),
+            "lcmx_count_nonfinite": ([vp, vp, ctypes.c_longlong, vp, vp], ip),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = lib
+        return lib
+
+
+class Context:
+    """A liblcmx context on one CUDA device."""
+
+    def __init__(self, device: int = 0) -> None:
+        self.lib = load_library()
+        self.device = device
+        h = ctypes.c_void_p()
+        rc = self.lib.lcmx_ctx_create(device, ctypes.byref(h))
+        if rc != 0:
+            raise KernelError(rc, self.lib.lcmx_last_error(None).decode())
+        self.h = h
+        self._mods: dict[str, Module] = {}
+        self._lock = threading.Lock()
+
+    def check(self, rc: int) -> None:
+        if rc != 0:
+            raise KernelError(rc, self.lib.lcmx_last_error(self.h).decode())
+
+    def device_info(self) -> tuple[int, int, int]:
+        sm = ctypes.c_int()
+        free = ctypes.c_size_t()
+        total = ctypes.c_size_t()
+        self.check(self.lib.lcmx_device_info(self.h, ctypes.byref(sm), ctypes.byref(free), ctypes.byref(total)))
+        return sm.value, free.value, total.value
+
+    def compile(self, src: str, key: str, options: str = "") -> "Module":
+        with self._lock:
+            m = self._mods.get(key)
+            if m is not None:
+                return m
+            h = ctypes.c_void_p()
+            self.check(self.lib.lcmx_module_compile(self.h, src.encode(), key.encode(), options.encode(), ctypes.byref(h)))
+            m = Module(self, h, key)
+            self._mods[key] = m
+            return m
+
+    def count_nonfinite(self, ptr: int, n: int, counts_ptr: int, stream: int) -> None:
+        self.check(self.lib.lcmx_count_nonfinite(self.h, ptr, n, counts_ptr, stream))
+
+
+class Module:
+    def __init__(self, ctx: Context, h: ctypes.c_void_p, key: str) -> None:
+        self.ctx = ctx
+        self.h = h
+        self.key = key
+
+    def occupancy(self, kernel: str, block: int, smem: int) -> int:
+        n = ctypes.c_int()
+        self.ctx.check(self.ctx.lib.lcmx_occupancy(self.h, kernel.encode(), block, smem, ctypes.byref(n)))
+        return n.value
+
+    def _args(self, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid) -> LaunchArgs:
+        return LaunchArgs(items_ptr, prefix_ptr, n_items, n_tiles, grid, block, smem)
+
+    def bellman_step(self, kernel, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, stream, grid=0) -> None:
+        a = self._args(items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid)
+        self.ctx.check(self.ctx.lib.lcmx_bellman_step(self.h, kernel.encode(), ctypes.byref(a), stream))
+
+    def expectation(self, kernel, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, stream, grid=0) -> None:
+        a = self._args(items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid)
+        self.ctx.check(self.ctx.lib.lcmx_expectation(self.h, kernel.encode(), ctypes.byref(a), stream))
+
+    def simulate(self, kernel, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, seed, stream, grid=0) -> None:
+        a = self._args(items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid)
+        self.ctx.check(self.ctx.lib.lcmx_simulate(self.h, kernel.encode(), ctypes.byref(a), seed, stream))
+
+    def egm_step(self, kernel, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, stream, grid=0) -> None:
+        a = self._args(items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid)
+        self.ctx.check(self.ctx.lib.lcmx_egm_step(self.h, kernel.encode(), ctypes.byref(a), stream))
+
+
+_contexts: dict[int, Context] = {}
+_ctx_lock = threading.Lock()
+
+
+def get_context(device: int = 0) -> Context:
+    import torch
+
+    if not torch.cuda.is_available():
+        raise KernelError(-1, "no CUDA device is available; pylcm_b200 solves on the GPU only")
+    with _ctx_lock:
+        c = _contexts.get(device)
+        if c is None:
+            c = Context(device)
+            _contexts[device] = c
+        return c

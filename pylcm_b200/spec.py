@@ -275,6 +275,7 @@ class TracedRegime:
     next_states: dict[str, dict[str, NextState]]  # target -> state -> law
     param_values: dict[str, np.ndarray]  # flat name -> value (float64)
     param_order: list[str]
+    param_sources: dict[str, tuple]  # flat name -> how to look it up
     beta: ir.Expr | None
     taste_scale: float | None
     process_tables: dict[str, tuple[np.ndarray, np.ndarray]]  # state -> (nodes, P)
@@ -289,11 +290,40 @@ class TracedRegime:
             off += max(1, v.size)
         return out, off
 
-    def pack_params(self) -> np.ndarray:
+    def values_for(self, resolver: "ParamResolver") -> dict[str, np.ndarray]:
+        """Parameter values of another parameter set, same layout as the trace."""
+        out = {}
+        proc_cache: dict[str, tuple] = {}
+        for flat in self.param_order:
+            src = self.param_sources[flat]
+            if src[0] == "arg":
+                ok, val = resolver.find(self.spec.name, src[1], src[2])
+                if not ok:
+                    raise InvalidParamsError(f"regime {self.spec.name!r}: missing parameter {src[2]!r} of {src[1]!r}")
+                v = np.asarray(val, dtype=np.float64)
+            else:
+                state = src[1]
+                if state not in proc_cache:
+                    ax = self.spec.state(state)
+                    pp = resolver.process_params(self.spec.name, state, ax.grid)
+                    proc_cache[state] = (
+                        np.asarray(ax.grid.compute_gridpoints(**pp), dtype=np.float64),
+                        np.asarray(ax.grid.compute_transition_probs(**pp), dtype=np.float64),
+                    )
+                v = proc_cache[state][0 if src[0] == "proc_nodes" else 1]
+            if v.shape != self.param_values[flat].shape:
+                raise InvalidParamsError(
+                    f"parameter {flat} has shape {v.shape}, expected {self.param_values[flat].shape}"
+                )
+            out[flat] = v
+        return out
+
+    def pack_params(self, values: dict | None = None) -> np.ndarray:
+        values = self.param_values if values is None else values
         layout, total = self.param_layout()
         vec = np.zeros(max(total, 1), dtype=np.float64)
         for name, (off, shape) in layout.items():
-            v = np.asarray(self.param_values[name], dtype=np.float64).ravel()
+            v = np.asarray(values[name], dtype=np.float64).ravel()
             vec[off : off + max(1, v.size)] = v if v.size else 0.0
         return vec
 
@@ -314,6 +344,7 @@ class _Tracer:
         self.active: list[str] = []
         self.param_values: dict[str, np.ndarray] = {}
         self.param_order: list[str] = []
+        self.param_sources: dict[str, tuple] = {}
         self.env: dict[str, Any] = {}
         for ax in spec.states:
             if ax.kind == "continuous":
@@ -329,13 +360,14 @@ class _Tracer:
         self.env["period"] = ir.var("period", "period", "i")
         self.env["age"] = ir.var("age", "age", "f")
 
-    def add_param(self, flat: str, value: Any) -> Any:
+    def add_param(self, flat: str, value: Any, source: tuple) -> Any:
         arr = np.asarray(value)
         if arr.dtype == object:
             raise InvalidParamsError(f"parameter {flat} is not numeric")
         if flat not in self.param_values:
             self.param_values[flat] = np.asarray(arr, dtype=np.float64)
             self.param_order.append(flat)
+            self.param_sources[flat] = source
         if arr.ndim == 0:
             return ir.param(flat)
         return ir.ParamArray(flat, arr.shape)
@@ -347,7 +379,7 @@ class _Tracer:
             return self.env[arg]
         ok, val = self.resolver.find(self.spec.name, func, arg)
         if ok:
-            return self.add_param(f"{func}__{arg}", val)
+            return self.add_param(f"{func}__{arg}", val, ("arg", func, arg))
         if default is not inspect.Parameter.empty:
             return default
         raise InvalidParamsError(
@@ -445,8 +477,8 @@ def trace_regime(
             nodes = np.asarray(ax.grid.compute_gridpoints(**pp), dtype=np.float64)
             P = np.asarray(ax.grid.compute_transition_probs(**pp), dtype=np.float64)
             process_tables[ax.name] = (nodes, P)
-            t.add_param(proc_grid_name(ax.name), nodes)
-            t.add_param(proc_P_name(ax.name), P)
+            t.add_param(proc_grid_name(ax.name), nodes, ("proc_nodes", ax.name))
+            t.add_param(proc_P_name(ax.name), P, ("proc_P", ax.name))
     beta = None
     taste_scale = None
     regime_probs = None
@@ -455,7 +487,7 @@ def trace_regime(
         ok, bval = resolver.find(spec.name, BETA_FUNC, BETA_ARG)
         if not ok:
             raise InvalidParamsError(f"regime {spec.name!r}: missing discount_factor")
-        beta = t.add_param(f"{BETA_FUNC}__{BETA_ARG}", bval)
+        beta = t.add_param(f"{BETA_FUNC}__{BETA_ARG}", bval, ("arg", BETA_FUNC, BETA_ARG))
         raw = t.trace("next_regime")
         n_reg = len(all_specs)
         if isinstance(spec.user.transition, MarkovTransition):
@@ -524,6 +556,7 @@ def trace_regime(
         next_states=next_states,
         param_values=t.param_values,
         param_order=t.param_order,
+        param_sources=t.param_sources,
         beta=beta,
         taste_scale=taste_scale,
         process_tables=process_tables,

@@ -1,0 +1,49 @@
+"""The C-ABI library builds, loads and exports every declared entry point.
+
+No compute call is made here (no GPU needed)."""
+
+import ctypes
+import re
+from pathlib import Path
+
+from pylcm_b200 import build as B
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "lcmx.h"
+
+
+def declared_symbols() -> set[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(lcmx_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_exports_every_declared_symbol():
+    lib_path = B.build()
+    lib = ctypes.CDLL(str(lib_path))
+    syms = declared_symbols()
+    assert "lcmx_bellman_step" in syms and len(syms) >= 10
+    missing = [s for s in sorted(syms) if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_runtime_binding_matches_header():
+    from pylcm_b200 import runtime
+
+    assert declared_symbols() == set(runtime.EXPORTED)
+
+
+def test_last_error_without_context_is_a_string():
+    from pylcm_b200 import runtime
+
+    lib = runtime.load_library()
+    assert isinstance(lib.lcmx_last_error(None), bytes)
+
+
+def test_compile_rejects_null_arguments_without_gpu():
+    """Argument validation happens before any CUDA call."""
+    from pylcm_b200 import runtime
+
+    lib = runtime.load_library()
+    out = ctypes.c_void_p()
+    rc = lib.lcmx_module_compile(None, b"", b"k", None, ctypes.byref(out))
+    assert rc == 1  # LCMX_ERR_ARGS

@@ -1,0 +1,112 @@
+"""GPU solve vs the CPU oracle (parity tests proper; call through the C ABI).
+
+Bars: fp64 -- V within 1e-12 (|a-b| / max(1, |b|)), argmax identical wherever
+the oracle's best-to-second-best gap exceeds 1e-9; fp32 search with fp64
+re-evaluation -- V within 1e-6 and >= 99.9 % policy agreement.
+"""
+
+import numpy as np
+import pytest
+
+from oracle.grid_search import solve as oracle_solve
+from tests import models as M
+from tests.conftest import load_golden, rel_err
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "regression": (lambda: M.regression_model(4), lambda: M.regression_params(4)),
+    "proc_tauchen": (lambda: M.processes_model(4, "tauchen"), lambda: M.processes_params("tauchen")),
+    "proc_rouwenhorst": (lambda: M.processes_model(5, "rouwenhorst"), lambda: M.processes_params("rouwenhorst")),
+    "proc_uniform": (lambda: M.processes_model(4, "uniform"), lambda: M.processes_params("uniform")),
+    "retirement": (lambda: M.retirement_model(5, 100, 100), M.retirement_params),
+    "stochastic": (lambda: M.stochastic_model(6, 60, 80), M.stochastic_params),
+    "hc": (lambda: M.hc_model(4, 30, 6, 5, 25), lambda: M.hc_params(1, 5)),
+}
+
+
+def _compare(model, params, precision):
+    V, pol = model.solve(params=params, precision=precision, return_policy=True, log_level="off")
+    gaps: dict = {}
+    Vo, Po = oracle_solve(model, params, gaps=gaps)
+    worst = 0.0
+    n_pol = n_agree = 0
+    for p in Vo:
+        for r in Vo[p]:
+            worst = max(worst, rel_err(V[p][r], Vo[p][r]))
+            g = gaps[p][r]
+            sel = g > 1e-9
+            n_pol += int(sel.sum())
+            n_agree += int((np.asarray(pol[p][r])[sel] == Po[p][r][sel]).sum())
+    return worst, n_pol, n_agree
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_fp64_matches_oracle(case):
+    mk, mp = CASES[case]
+    worst, n_pol, n_agree = _compare(mk(), mp(), "fp64")
+    assert worst < 1e-12, worst
+    assert n_agree == n_pol, (n_agree, n_pol)
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_fp32_search_matches_oracle(case):
+    mk, mp = CASES[case]
+    worst, n_pol, n_agree = _compare(mk(), mp(), "fp32")
+    assert worst < 1e-6, worst
+    assert n_agree >= 0.999 * n_pol, (n_agree, n_pol)
+
+
+def test_gpu_matches_reference_golden_regression():
+    golden = load_golden("regression_solution.npz")
+    V = M.regression_model(4).solve(params=M.regression_params(4), log_level="off")
+    for p, regs in golden.items():
+        for r, ref in regs.items():
+            assert rel_err(V[p][r], ref) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["uniform", "normal", "lognormal", "tauchen", "rouwenhorst"])
+def test_gpu_matches_reference_golden_processes(kind):
+    golden = load_golden(f"processes_solution_{kind}.npz")
+    V = M.processes_model(4, kind).solve(params=M.processes_params(kind), log_level="off")
+    for p, regs in golden.items():
+        for r, ref in regs.items():
+            assert rel_err(V[p][r], ref) < 1e-12, (kind, p, r)
+
+
+def test_batch_equals_single():
+    model = M.stochastic_model(5, 40, 50)
+    ps = [M.stochastic_params(beta=b, crra=c) for b, c in ((0.95, 2.0), (0.9, 3.0), (0.97, 1.5))]
+    eng = model.engine("fp64")
+    batch = eng.solve_batch(ps)
+    for p, (Vb, _) in zip(ps, batch):
+        V1, _ = eng.solve(p)
+        for per in V1:
+            for r in V1[per]:
+                assert np.array_equal(V1[per][r].cpu().numpy(), Vb[per][r].cpu().numpy())
+
+
+def test_deterministic_replay():
+    model = M.stochastic_model(5, 40, 50)
+    p = M.stochastic_params()
+    a = model.solve(params=p, log_level="off")
+    b = model.solve(params=p, log_level="off")
+    for per in a:
+        for r in a[per]:
+            assert np.array_equal(a[per][r], b[per][r])
+
+
+def test_cuda_graph_replay_matches_eager():
+    model = M.stochastic_model(5, 40, 50)
+    eng = model.engine("fp64")
+    plan = eng.plan([M.stochastic_params()])
+    plan.run()
+    eager = {r: v.clone() for r, v in plan.V.items()}
+    for v in plan.V.values():
+        v.zero_()
+    plan.run_graph()
+    import torch
+
+    torch.cuda.synchronize()
+    for r in eager:
+        assert torch.equal(eager[r], plan.V[r])
