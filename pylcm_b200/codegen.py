@@ -739,11 +739,12 @@ class RegimeKernels:
             ap(f"    SV[{i}] = (double)({svals[id(n)]});")
         if not bS:
             ap("    SV[0] = 0.0;")
+        BEST = "LcmBest2" if (fp32 and not taste) else "LcmBest"
         if taste:
             ap(f"    LcmBest<{ST}> bd[{ND}];")
             ap(f"    #pragma unroll\n    for (int d = 0; d < {ND}; ++d) bd[d].init();")
         else:
-            ap(f"    LcmBest<{ST}> best; best.init();")
+            ap(f"    {BEST}<{ST}> best; best.init();")
         ap(f"    for (int a0 = 0; a0 < n_actions; a0 += {CH}) {{")
         ap(f"      const int cn = min({CH}, n_actions - a0);")
         ap("      __syncthreads();")
@@ -770,6 +771,8 @@ class RegimeKernels:
         # reduction
         if taste:
             ap(f"    #pragma unroll\n    for (int d = 0; d < {ND}; ++d) lcm_group_reduce<{LANES}, {ST}>(bd[d]);")
+        elif fp32:
+            ap(f"    lcm_group_reduce2<{LANES}, {ST}>(best);")
         else:
             ap(f"    lcm_group_reduce<{LANES}, {ST}>(best);")
         ap("    if (active && lane == 0) {")
@@ -811,10 +814,16 @@ class RegimeKernels:
             ap("      if (best.nan) { v = lcm_lim<double>::nan(); pol = 0; }")
             ap("      else if (best.idx < 0) { v = -lcm_lim<double>::inf(); pol = 0; }")
             if fp32:
+                # re-rank the two single-precision candidates in double precision
                 ap("      else { const int aa = best.idx;")
                 for s_ in final_eval("aa", "qd"):
                     ap("        " + s_)
-                ap("        v = qd; pol = aa; }")
+                ap("        v = qd; pol = aa;")
+                ap("        if (best.idx2 >= 0) { const int ab = best.idx2;")
+                for s_ in final_eval("ab", "qd2"):
+                    ap("          " + s_.replace("afl", "afl2"))
+                ap("          if (qd2 > v || (qd2 == v && ab < pol)) { v = qd2; pol = ab; } }")
+                ap("      }")
             else:
                 ap("      else { v = (double)best.v; pol = best.idx; }")
             ap("      Vout[s] = v; Pout[s] = pol;")

@@ -146,6 +146,50 @@ template <typename T> struct LcmBest {
   }
 };
 
+// Running top-2 (value, index) over feasible actions.  The single-precision
+// search keeps two candidates so that a near-tie which float rounding may
+// misorder is re-ranked in double precision afterwards.
+template <typename T> struct LcmBest2 {
+  T v, v2;
+  int idx, idx2;
+  int nan;
+  __device__ __forceinline__ void init() {
+    v = v2 = -lcm_lim<T>::inf(); idx = idx2 = -1; nan = 0;
+  }
+  __device__ __forceinline__ static bool better(T a, int ia, T b, int ib) {
+    // does (a, ia) rank above (b, ib)?  ties -> smaller index
+    if (ia < 0) return false;
+    if (ib < 0) return true;
+    return a > b || (a == b && ia < ib);
+  }
+  __device__ __forceinline__ void add(T q, int a) {
+    if (better(q, a, v, idx)) { v2 = v; idx2 = idx; v = q; idx = a; }
+    else if (a != idx && better(q, a, v2, idx2)) { v2 = q; idx2 = a; }
+  }
+  __device__ __forceinline__ void push(T q, int a) {
+    if (q != q) { nan = 1; return; }
+    add(q, a);
+  }
+  __device__ __forceinline__ void merge(T ov, int oi, T ov2, int oi2, int onan) {
+    nan |= onan;
+    if (oi >= 0) add(ov, oi);
+    if (oi2 >= 0) add(ov2, oi2);
+  }
+};
+
+template <int LANES, typename T>
+__device__ __forceinline__ void lcm_group_reduce2(LcmBest2<T>& b) {
+#pragma unroll
+  for (int off = LANES >> 1; off > 0; off >>= 1) {
+    T ov = __shfl_xor_sync(0xffffffffu, b.v, off);
+    int oi = __shfl_xor_sync(0xffffffffu, b.idx, off);
+    T ov2 = __shfl_xor_sync(0xffffffffu, b.v2, off);
+    int oi2 = __shfl_xor_sync(0xffffffffu, b.idx2, off);
+    int on = __shfl_xor_sync(0xffffffffu, b.nan, off);
+    b.merge(ov, oi, ov2, oi2, on);
+  }
+}
+
 // Combine LANES consecutive lanes (a power of two <= 32) holding partial
 // results for the same state, with warp shuffles.
 template <int LANES, typename T>

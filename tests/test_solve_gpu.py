@@ -25,26 +25,31 @@ CASES = {
 }
 
 
-def _compare(model, params, precision):
+def _compare(model, params, precision, gap_tol=1e-9):
+    """(worst V error, #states with gap > gap_tol, #agreeing among them,
+    #states, #agreeing overall)."""
     V, pol = model.solve(params=params, precision=precision, return_policy=True, log_level="off")
     gaps: dict = {}
     Vo, Po = oracle_solve(model, params, gaps=gaps)
     worst = 0.0
-    n_pol = n_agree = 0
+    n_pol = n_agree = n_all = n_all_agree = 0
     for p in Vo:
         for r in Vo[p]:
             worst = max(worst, rel_err(V[p][r], Vo[p][r]))
-            g = gaps[p][r]
-            sel = g > 1e-9
+            g = gaps[p][r] / np.maximum(1.0, np.abs(np.nan_to_num(Vo[p][r], neginf=0.0)))
+            sel = g > gap_tol
+            same = np.asarray(pol[p][r]) == Po[p][r]
             n_pol += int(sel.sum())
-            n_agree += int((np.asarray(pol[p][r])[sel] == Po[p][r][sel]).sum())
-    return worst, n_pol, n_agree
+            n_agree += int(same[sel].sum())
+            n_all += same.size
+            n_all_agree += int(same.sum())
+    return worst, n_pol, n_agree, n_all, n_all_agree
 
 
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_fp64_matches_oracle(case):
     mk, mp = CASES[case]
-    worst, n_pol, n_agree = _compare(mk(), mp(), "fp64")
+    worst, n_pol, n_agree, _, _ = _compare(mk(), mp(), "fp64")
     assert worst < 1e-12, worst
     assert n_agree == n_pol, (n_agree, n_pol)
 
@@ -52,9 +57,13 @@ def test_fp64_matches_oracle(case):
 @pytest.mark.parametrize("case", sorted(CASES))
 def test_fp32_search_matches_oracle(case):
     mk, mp = CASES[case]
-    worst, n_pol, n_agree = _compare(mk(), mp(), "fp32")
+    # single-precision search: exact agreement wherever the relative Q gap is
+    # above float resolution; >= 99 % agreement over all states of these
+    # small grids (the benchmark configurations report their own agreement)
+    worst, n_pol, n_agree, n_all, n_all_agree = _compare(mk(), mp(), "fp32", gap_tol=1e-5)
     assert worst < 1e-6, worst
-    assert n_agree >= 0.999 * n_pol, (n_agree, n_pol)
+    assert n_agree == n_pol, (n_agree, n_pol)
+    assert n_all_agree >= 0.99 * n_all, (n_all_agree, n_all)
 
 
 def test_gpu_matches_reference_golden_regression():
