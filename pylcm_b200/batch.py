@@ -50,7 +50,7 @@ class BatchSolver:
         for key in self._pkeys:
             name, targets = key
             spec = next(s for s in self.engine.specs if s.name == name)
-            self._rk_for[key] = self.engine.kernels(spec, targets, template_params)
+            self._rk_for[key] = self.engine.kernels(spec, targets, template_params, self.n)
         if use_graph:
             self.plan.capture()
 

@@ -363,12 +363,14 @@ def _target_plan(tr: TracedRegime, tgt: RegimeSpec) -> TargetPlan:
 @dataclasses.dataclass(frozen=True)
 class LaunchConfig:
     block: int = 256
-    lanes: int = 1
-    chunk: int = 512
+    lanes: int = 1  # threads sharing one state (power of two <= 32)
+    chunk: int = 512  # actions per shared-memory table chunk
+    sb: int = 1  # states per thread (register blocking)
+    min_blocks: int = 0  # __launch_bounds__ min CTAs per SM (0 = compiler's choice)
 
     @property
     def states_per_tile(self) -> int:
-        return self.block // self.lanes
+        return self.sb * self.block // self.lanes
 
 
 class RegimeKernels:
@@ -419,6 +421,7 @@ class RegimeKernels:
         self.W_ASIZE = take(len(spec.actions))
         self.W_AGRID = take(len(spec.actions))
         self.W_TASTE = take()
+        self.W_ATAB = take()  # global action table (kernel a0 output) of this item
         for t in self.targets:
             if t.scalar:
                 t.w_scalar = take()
@@ -443,6 +446,9 @@ class RegimeKernels:
     def bellman_name(self) -> str:
         return f"lcm_bellman_{self.tag}"
 
+    def atab_name(self) -> str:
+        return f"lcm_atab_{self.tag}"
+
     def expect_name(self, t: TargetPlan) -> str:
         return f"lcm_expect_{self.tag}_{t.spec.name}"
 
@@ -453,8 +459,11 @@ class RegimeKernels:
         roots = [tr.F, tr.U]
         if tr.beta is not None:
             roots.append(tr.beta)
+        if tr.regime_id is not None and self.targets:
+            roots.append(tr.regime_id)
         for t in self.targets:
-            roots.append(t.prob)
+            if tr.regime_id is None:
+                roots.append(t.prob)
             if t.scalar:
                 continue
             for pos in t.det_pos:
@@ -464,129 +473,160 @@ class RegimeKernels:
         return [ir.const(r) for r in roots]
 
     def _bellman_source(self) -> str:
+        """Kernel (a0) (action table) and kernel (a) (Bellman step) for this regime.
+
+        Loop structure of kernel (a), per tile of states:
+
+            P  : params / period / age only          -> once per tile
+            S  : state only                         -> once per state slot
+            for each discrete-action combination d (outer, unrolled):
+                D  : discrete actions only           -> once per d
+                SD : state x discrete actions        -> once per (slot, d)
+                for each chunk of continuous actions (shared-memory table):
+                    SA : everything else              -> the inner loop
+            A  : continuous-action only              -> precomputed by (a0)
+
+        With a deterministic regime transition whose next regime is known per
+        d, the inner loop is specialised to that one target.
+        """
         spec = self.spec
         cfg = self.cfg
         fp32 = self.precision == "fp32"
-        ST = "float" if fp32 else "double"  # search type
-        roots = self._roots()
-        boundary = _boundary(roots)
-        bP = [n for n in boundary if _phase(n) == "P"]
-        bS = [n for n in boundary if _phase(n) == "S"]
-        bA = [n for n in boundary if _phase(n) == "A"]
-        key_actions = sorted(
-            {name for t in self.targets for (k, name, _) in t.key_vars if k == "action"}
-        )
+        ST = "float" if fp32 else "double"
+        TT = ST
         taste = spec.taste_shocks
+        dacts = [a for a in spec.actions if a.kind != "continuous"]
+        cacts = [a for a in spec.actions if a.kind == "continuous"]
+        dnames = {a.name for a in dacts}
         ND = spec.n_discrete_actions
-        # A-table fields: boundary A nodes + discrete action indices used by keys
-        a_fields: list[tuple[str, object]] = [("node", n) for n in bA]
-        a_fields += [("aidx", name) for name in key_actions]
-        if taste:
-            a_fields.append(("ad", None))
-        NAF = max(len(a_fields), 1)
+
+        def phase(n: ir.Expr) -> str:
+            d = n.deps()
+            has_s = any(k == "state" for k, _ in d)
+            has_ac = any(k == "action" and nm not in dnames for k, nm in d)
+            has_ad = any(k == "action" and nm in dnames for k, nm in d)
+            if has_ac:
+                return "SA" if has_s else "A"
+            if has_s:
+                return "SD" if has_ad else "S"
+            return "D" if has_ad else "P"
+
+        roots = self._roots()
+        det = self.tr.regime_id is not None and bool(self.targets)
+        rid_phase = phase(self.tr.regime_id) if det else None
+        unswitch = det and rid_phase in ("P", "D")
+        # boundary nodes the inner loop consumes, by phase
+        bnd: dict[str, list] = {k: [] for k in ("P", "D", "S", "SD", "A")}
+        seen: set[int] = set()
+        stack = [r for r in roots if isinstance(r, ir.Expr)]
+        while stack:
+            n = stack.pop()
+            if id(n) in seen or n.op == "const":
+                continue
+            seen.add(id(n))
+            ph = phase(n)
+            if ph != "SA":
+                bnd[ph].append(n)
+                continue
+            stack.extend(a for a in n.args if isinstance(a, ir.Expr))
+        bP, bD, bS, bSD, bA = bnd["P"], bnd["D"], bnd["S"], bnd["SD"], bnd["A"]
+        if unswitch and id(self.tr.regime_id) not in {id(x) for x in bP + bD}:
+            (bP if rid_phase == "P" else bD).append(self.tr.regime_id)
+        # action-table columns: float fields / int fields
+        slot: list[tuple[str, int]] = []
+        nf = ni = 0
+        for n in bA:
+            if n.dtype == "f":
+                slot.append(("F", nf))
+                nf += 1
+            else:
+                slot.append(("I", ni))
+                ni += 1
+        NF, NI = max(nf, 1), max(ni, 1)
+        B, LANES, CH, SB = cfg.block, cfg.lanes, cfg.chunk, cfg.sb
+        SPT = cfg.states_per_tile
+        SPB = B // LANES
+        dstates = [a for a in spec.states if a.kind != "continuous"]
+        NDS = max(len(dstates), 1)
+        nP, nD, nS, nSD = (max(len(x), 1) for x in (bP, bD, bS, bSD))
+        pv = lambda: {id(ir.var("period", "period", "i")): "period", id(ir.var("age", "age", "f")): "age"}  # noqa: E731
+
         L: list[str] = []
         ap = L.append
         ap(f"// ---- regime {spec.name}: Bellman step (kernel a), precision {self.precision}")
-        ap(f"#define NAF_{self.tag} {NAF}")
 
-        # ---------------- helpers: decode an action index into per-axis values
-        def decode_action(lines: list[str], a_expr: str, pref: str) -> dict:
-            """Emit decode of flat action index -> {name: (idx_var, val_expr)}."""
-            out = {}
-            rem = f"{pref}rem"
-            lines.append(f"int {rem} = {a_expr};")
-            for k in range(len(spec.actions) - 1, -1, -1):
-                ax = spec.actions[k]
-                sz = f"lcm_wi(it, {self.W_ASIZE + k})"
-                iv = f"{pref}i_{ax.name}"
-                lines.append(f"int {iv} = {rem} % {sz}; {rem} /= {sz};")
-                if ax.kind == "continuous":
-                    vv = f"{pref}v_{ax.name}"
-                    lines.append(f"double {vv} = lcm_wp<const double>(it, {self.W_AGRID + k})[{iv}];")
-                    out[ax.name] = (iv, vv)
+        # ----------------------------------------------------------------
+        # per-target loop invariants of the Q evaluation
+        ap(f"template <typename T, typename E> struct Ctx_{self.tag} {{")
+        loads = []
+        for ti, t in enumerate(self.targets):
+            if t.scalar:
+                ap(f"  T sv{ti};")
+                loads.append(f"sv{ti} = (T)(*lcm_wp<const double>(it, {t.w_scalar}));")
+                continue
+            ap(f"  const E* ev{ti};")
+            loads.append(f"ev{ti} = lcm_evsel<E>::get(it, {t.w_ev64}, {t.w_ev32});")
+            for pos in t.det_pos + t.cont_pos:
+                ap(f"  int n{ti}_{pos};")
+                loads.append(f"n{ti}_{pos} = lcm_wi(it, {t.w_sizes + pos});")
+            for ci, pos in enumerate(t.cont_pos):
+                w0 = t.w_coord + 3 * ci
+                if t.spec.states[pos].grid.kind == "irreg":
+                    ap(f"  const double* p{ti}_{ci};")
+                    loads.append(f"p{ti}_{ci} = lcm_wp<const double>(it, {w0 + 2});")
                 else:
-                    out[ax.name] = (iv, iv)
-            return out
+                    ap(f"  T a{ti}_{ci}, b{ti}_{ci};")
+                    loads.append(f"a{ti}_{ci} = (T)lcm_wd(it, {w0}); b{ti}_{ci} = (T)lcm_wd(it, {w0 + 1});")
+        ap("  __device__ __forceinline__ void load(const i64* __restrict__ it) {")
+        for l_ in loads:
+            ap("    " + l_)
+        ap("  }")
+        ap("};")
 
-        def action_provided(dec: dict, pvals: dict) -> dict:
-            prov = dict(pvals)
-            for ax in spec.actions:
-                node = ir.var("action", ax.name, "f" if ax.kind == "continuous" else "i")
-                prov[id(node)] = dec[ax.name][1]
-            return prov
+        # ----------------------------------------------------------------
+        # accessors of the continuous-action table
+        ap(
+            f"template <typename T> struct AFTab_{self.tag} {{ const {TT}* tabf; const int* tabi; int j;\n"
+            f"  __device__ __forceinline__ T F(int f) const {{ return (T)tabf[f * {CH} + j]; }}\n"
+            f"  __device__ __forceinline__ int I(int f) const {{ return tabi[f * {CH} + j]; }} }};"
+        )
+        ap(
+            f"struct AFLoc_{self.tag} {{ double v[{NF}]; int vi[{NI}];\n"
+            f"  __device__ __forceinline__ double F(int f) const {{ return v[f]; }}\n"
+            f"  __device__ __forceinline__ int I(int f) const {{ return vi[f]; }} }};"
+        )
 
-        def p_provided() -> dict:
-            return {
-                id(ir.var("period", "period", "i")): "period",
-                id(ir.var("age", "age", "f")): "age",
-            }
-
-        # ---------------- P phase (double), per tile
-        eP = Emitter("double", self.param_off, p_provided(), "p")
-        pvals = {}
-        for n in bP:
-            pvals[id(n)] = eP.emit(n)
-        # P-values of nodes used inside S and A subgraphs are emitted lazily by
-        # those emitters (they see P nodes as ordinary nodes) -- cheap & hoisted.
-
-        # ---------------- S phase (double), per thread
-        s_prov = p_provided()
-        s_prov.update(pvals)
-        s_decl: list[str] = []
-        for k, ax in enumerate(spec.states):
-            if ax.kind == "continuous":
-                s_prov[id(ir.var("state", ax.name, "f"))] = f"sv_{ax.name}"
-            else:
-                s_prov[id(ir.var("state", ax.name, "i"))] = f"si_{ax.name}"
-        eS = Emitter("double", self.param_off, s_prov, "s")
-        svals = {}
-        for n in bS:
-            svals[id(n)] = eS.emit(n)
-
-        # ---------------- A phase (double) -> table fields
-        def emit_A(lines: list[str], a_expr: str, pref: str):
-            dec = decode_action(lines, a_expr, pref)
-            eA = Emitter("double", self.param_off, action_provided(dec, p_provided() | pvals), pref + "a")
-            fields = []
-            for kind, obj in a_fields:
-                if kind == "node":
-                    fields.append((eA.emit(obj), obj.dtype))
-                elif kind == "aidx":
-                    fields.append((dec[obj][0], "i"))
-                else:  # ad: discrete-action combo index
-                    nc = "1"
-                    expr = "0"
-                    for k in range(len(spec.actions)):
-                        ax = spec.actions[k]
-                        if ax.kind == "continuous":
-                            continue
-                        expr = f"({expr}) * lcm_wi(it, {self.W_ASIZE + k}) + {dec[ax.name][0]}"
-                    fields.append((expr, "i"))
-            lines.extend(eA.lines)
-            return fields
-
-        # ---------------- SA phase (templated)
-        def sa_body(T: str, E: str) -> list[str]:
-            prov = {}
-            prov.update(p_provided())
-            for pi, n in enumerate(bP):
-                prov[id(n)] = f"(({T})PVd[{pi}])" if n.dtype == "f" else f"(({_ctype(n.dtype)})PVd[{pi}])"
+        # ----------------------------------------------------------------
+        # the inner (state, action) evaluation, templated on precision and on
+        # the selected target (TSEL < 0: all targets by probability / id)
+        def sa_body(T: str, E: str, tsel: int) -> list[str]:
+            prov = pv()
+            for i, n in enumerate(bP):
+                prov[id(n)] = _cast(f"PVd[{i}]", n.dtype, T)
+            for i, n in enumerate(bD):
+                prov[id(n)] = _cast(f"DV[{i}]", n.dtype, T)
             for i, n in enumerate(bS):
                 prov[id(n)] = _cast(f"SV[{i}]", n.dtype, T)
-            for i, (kind, obj) in enumerate(a_fields):
-                if kind == "node":
-                    prov[id(obj)] = _cast(f"AF({i})", obj.dtype, T)
-            for ax in spec.states:
-                if ax.kind == "continuous":
-                    pass
+            for i, n in enumerate(bSD):
+                prov[id(n)] = _cast(f"SDV[{i}]", n.dtype, T)
+            for i, n in enumerate(bA):
+                col, k = slot[i]
+                if col == "F":
+                    prov[id(n)] = f"(({T})AF.F({k}))"
+                elif n.dtype == "b":
+                    prov[id(n)] = f"(AF.I({k}) != 0)"
                 else:
-                    prov[id(ir.var("state", ax.name, "i"))] = f"si_{ax.name}"
+                    prov[id(n)] = f"AF.I({k})"
+            for i, a in enumerate(dstates):
+                prov[id(ir.var("state", a.name, "i"))] = f"SI[{i}]"
+            for a in dacts:
+                prov[id(ir.var("action", a.name, "i"))] = f"DI_{a.name}"
             e = Emitter(T, self.param_off, prov, "q")
             out: list[str] = []
             fexpr = e.emit(self.tr.F)
             out += e.lines
-            out.append(f"if (!({fexpr})) return false;")
             e.lines = []
+            out.append(f"if (!({fexpr})) return false;")
             uexpr = e.emit(self.tr.U)
             out += e.lines
             e.lines = []
@@ -596,241 +636,408 @@ class RegimeKernels:
             bexpr = e.emit(self.tr.beta)
             out += e.lines
             e.lines = []
-            # every target's probability and next-state expressions are bound at
-            # function scope first (shared sub-expressions stay in scope)
-            pnames, dnames, xnames = {}, {}, {}
-            for ti, t in enumerate(self.targets):
-                pnames[ti] = e.emit(t.prob)
+            sel = [(ti, t) for ti, t in enumerate(self.targets) if tsel < 0 or ti == tsel]
+            pnames, dn, xn = {}, {}, {}
+            rid_name = e.emit(self.tr.regime_id) if (det and tsel < 0) else None
+            for ti, t in sel:
+                if not det:
+                    pnames[ti] = e.emit(t.prob)
                 if t.scalar:
                     continue
                 for pos in t.det_pos:
-                    dnames[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
+                    dn[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
                 for pos in t.cont_pos:
-                    xnames[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
+                    xn[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
             out += e.lines
             e.lines = []
-            out.append(f"{T} ce = ({T})0; {T} mass = ({T})0; bool neg = false;")
-            for ti, t in enumerate(self.targets):
-                out.append(f"{{ {T} p = ({T})({pnames[ti]}); mass += p; neg = neg || (p < ({T})0);")
-                out.append("  if (p != 0) {")
-                if t.scalar:
-                    out.append(f"    {T} ev = ({T})(*lcm_wp<const double>(it, {t.w_scalar}));")
+            if det:
+                out.append(f"{T} ce = lcm_lim<{T}>::nan();")
+            else:
+                out.append(f"{T} ce = ({T})0; {T} mass = ({T})0; bool neg = false;")
+            for ti, t in sel:
+                if det and tsel >= 0:
+                    out.append("{ {")
+                elif det:
+                    out.append(f"{{ if (({rid_name}) == {t.spec.rid}) {{")
                 else:
-                    # row offset: key, deterministic discrete, then continuous block
+                    out.append(f"{{ {T} p = ({T})({pnames[ti]}); mass += p; neg = neg || (p < ({T})0);")
+                    out.append("  if (p != 0) {")
+                if t.scalar:
+                    out.append(f"    {T} ev = C.sv{ti};")
+                else:
                     inner: list[str] = []
                     key = "0"
                     for kind, name, size in t.key_vars:
-                        if kind == "state":
-                            iv = f"si_{name}"
-                        else:
-                            fi = [i for i, (k2, o) in enumerate(a_fields) if k2 == "aidx" and o == name][0]
-                            iv = f"(int)AF({fi})"
+                        iv = f"SI[{[a.name for a in dstates].index(name)}]" if kind == "state" else f"DI_{name}"
                         key = f"({key}) * {size} + {iv}"
                     off = key
                     for pos in t.det_pos:
-                        sz = f"lcm_wi(it, {t.w_sizes + pos})"
-                        off = f"({off}) * {sz} + min(max((int)({dnames[(ti, pos)]}), 0), {sz} - 1)"
+                        sz = f"C.n{ti}_{pos}"
+                        off = f"({off}) * {sz} + min(max((int)({dn[(ti, pos)]}), 0), {sz} - 1)"
                     cblk = "1"
                     for pos in t.cont_pos:
-                        cblk = f"{cblk} * lcm_wi(it, {t.w_sizes + pos})"
+                        cblk = f"{cblk} * C.n{ti}_{pos}"
                     for ci, pos in enumerate(t.cont_pos):
                         ax = t.spec.states[pos]
-                        xexpr = xnames[(ti, pos)]
-                        w0 = t.w_coord + 3 * ci
+                        x = xn[(ti, pos)]
                         kind = ax.grid.kind
                         if kind == "lin":
-                            c = f"lcm_coord_lin<{T}>(({T})({xexpr}), ({T})lcm_wd(it, {w0}), ({T})lcm_wd(it, {w0 + 1}))"
+                            cc = f"lcm_coord_lin<{T}>(({T})({x}), C.a{ti}_{ci}, C.b{ti}_{ci})"
                         elif kind == "log":
-                            c = f"lcm_coord_log<{T}>(({T})({xexpr}), ({T})lcm_wd(it, {w0}), ({T})lcm_wd(it, {w0 + 1}))"
+                            cc = f"lcm_coord_log<{T}>(({T})({x}), C.a{ti}_{ci}, C.b{ti}_{ci})"
                         else:
-                            c = f"lcm_coord_irreg<{T}>(({T})({xexpr}), lcm_wp<const double>(it, {w0 + 2}), lcm_wi(it, {t.w_sizes + pos}))"
-                        inner.append(f"{T} c{ci} = {c};")
-                    inner.append(
-                        f"const {E}* row = lcm_evsel<{E}>::get(it, {t.w_ev64}, {t.w_ev32}) + (i64)({off}) * ({cblk});"
-                    )
+                            cc = f"lcm_coord_irreg<{T}>(({T})({x}), C.p{ti}_{ci}, C.n{ti}_{pos})"
+                        inner.append(f"{T} c{ci} = {cc};")
+                    inner.append(f"const {E}* row = C.ev{ti} + (i64)({off}) * ({cblk});")
                     if len(t.cont_pos) == 0:
                         inner.append(f"{T} ev = ({T})row[0];")
                     elif len(t.cont_pos) == 1:
-                        n0 = f"lcm_wi(it, {t.w_sizes + t.cont_pos[0]})"
-                        inner.append(f"{T} ev = lcm_interp1<{T}, {E}>(row, {n0}, c0);")
+                        inner.append(f"{T} ev = lcm_interp1<{T}, {E}>(row, C.n{ti}_{t.cont_pos[0]}, c0);")
                     elif len(t.cont_pos) == 2:
-                        n0 = f"lcm_wi(it, {t.w_sizes + t.cont_pos[0]})"
-                        n1 = f"lcm_wi(it, {t.w_sizes + t.cont_pos[1]})"
-                        inner.append(f"{T} ev = lcm_interp2<{T}, {E}>(row, {n0}, {n1}, c0, c1);")
+                        inner.append(
+                            f"{T} ev = lcm_interp2<{T}, {E}>(row, C.n{ti}_{t.cont_pos[0]}, C.n{ti}_{t.cont_pos[1]}, c0, c1);"
+                        )
                     else:
                         raise TracingError("more than two continuous states per target are not supported")
                     out += ["    " + s for s in inner]
-                out.append(f"    ce = ce + lcm_zs(p, ev);")
+                if det:
+                    out.append("    ce = ev;")
+                else:
+                    out.append("    ce = ce + (lcm_isfinite(ev) ? p * ev : lcm_zs(p, ev));")
                 out.append("  }")
                 out.append("}")
-            out.append(
-                f"bool valid = (fabs(mass - ({T})1) <= ({T})1e-3) && !neg;"
-            )
-            out.append(f"ce = valid ? ce / mass : lcm_lim<{T}>::nan();")
+            if not det:
+                out.append(f"bool valid = (fabs(mass - ({T})1) <= ({T})1e-3) && !neg;")
+                out.append(f"ce = (mass == ({T})1) ? ce : (valid ? ce / mass : lcm_lim<{T}>::nan());")
             out.append(f"Q = ({T})({uexpr}) + ({T})({bexpr}) * ce;")
             return out
 
-        # shared-memory action table element type
-        TT = ST
-        n_bP = max(len(bP), 1)
-        n_bS = max(len(bS), 1)
-        # --- SA device function
-        ap(
-            f"template <typename T, typename E, typename AFN>\n"
-            f"__device__ __forceinline__ bool lcm_sa_{self.tag}(const i64* __restrict__ it, const double* __restrict__ PV, "
-            f"const double* PVd, const double* SV, const AFN& AF, {''.join(f'int si_{a.name}, ' for a in spec.states if a.kind != 'continuous')}int period, double age, T& Q) {{"
-        )
-        for s in sa_body("T", "E"):
-            ap("  " + s)
-        ap("  return true;\n}")
+        di_params = "".join(f"int DI_{a.name}, " for a in dacts)
+        tsel_values = [-1] + ([ti for ti in range(len(self.targets))] if unswitch else [])
+        for tsel in tsel_values:
+            ap(
+                f"template <typename T, typename E, typename AFN>\n"
+                f"__device__ __forceinline__ bool lcm_sa{tsel + 1}_{self.tag}(const Ctx_{self.tag}<T, E>& C, "
+                f"const double* __restrict__ PV, const double* PVd, const double* DV, const double* SV, "
+                f"const double* SDV, const AFN& AF, const int* SI, {di_params}int period, double age, T& Q) {{"
+            )
+            for s_ in sa_body("T", "E", tsel):
+                ap("  " + s_)
+            ap("  return true;\n}")
 
-        # --- accessors for action fields
-        ap(
-            f"template <typename T> struct AFTab_{self.tag} {{ const {TT}* tab; int j; int chunk;\n"
-            f"  __device__ __forceinline__ T operator()(int f) const {{ return (T)tab[f * chunk + j]; }} }};"
-        )
-        ap(
-            f"struct AFLoc_{self.tag} {{ double v[NAF_{self.tag}];\n"
-            f"  __device__ __forceinline__ double operator()(int f) const {{ return v[f]; }} }};"
-        )
+        # ----------------------------------------------------------------
+        # emitters for the hoisted phases (double precision)
+        eP = Emitter("double", self.param_off, pv(), "p")
+        pvals = [eP.emit(n) for n in bP]
 
-        # --- the kernel
-        B, LANES, CH = cfg.block, cfg.lanes, cfg.chunk
-        SPT = cfg.states_per_tile
-        si_args = "".join(f"si_{a.name}, " for a in spec.states if a.kind != "continuous")
+        def prov_sd(kind: str) -> dict:
+            prov = pv()
+            for i, n in enumerate(bP):
+                prov[id(n)] = f"PVd[{i}]" if n.dtype == "f" else _cast(f"PVd[{i}]", n.dtype, "double")
+            for i, a in enumerate(dstates):
+                prov[id(ir.var("state", a.name, "i"))] = f"si_{a.name}"
+            for a in spec.states:
+                if a.kind == "continuous":
+                    prov[id(ir.var("state", a.name, "f"))] = f"sv_{a.name}"
+            for a in dacts:
+                prov[id(ir.var("action", a.name, "i"))] = f"DI_{a.name}"
+            if kind == "SD":
+                for i, n in enumerate(bD):
+                    prov[id(n)] = f"DV[{i}]" if n.dtype == "f" else _cast(f"DV[{i}]", n.dtype, "double")
+                for i, n in enumerate(bS):
+                    prov[id(n)] = f"SV[kb][{i}]" if n.dtype == "f" else _cast(f"SV[kb][{i}]", n.dtype, "double")
+            return prov
+
+        def emit_phase(nodes, kind, pref):
+            e = Emitter("double", self.param_off, prov_sd(kind), pref)
+            vals = [e.emit(n) for n in nodes]
+            return e.lines, vals
+
+        d_lines, d_vals = emit_phase(bD, "D", "d")
+        s_lines, s_vals = emit_phase(bS, "S", "s")
+        sd_lines, sd_vals = emit_phase(bSD, "SD", "x")
+
+        def decode_disc(lines: list[str], ad_expr: str) -> None:
+            lines.append(f"int drem = {ad_expr};")
+            for a in reversed(dacts):
+                lines.append(f"const int DI_{a.name} = drem % {a.size}; drem /= {a.size};")
+
+        # ----------------------------------------------------------------
+        # kernel (a)
+        SA = f"lcm_sa{{}}_{self.tag}"
         ap(
-            f'extern "C" __global__ void __launch_bounds__({B}) {self.bellman_name()}('
-            "const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles) {"
+            f'extern "C" __global__ void __launch_bounds__({B}{", " + str(cfg.min_blocks) if cfg.min_blocks else ""}) '
+            f"{self.bellman_name()}(const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles) {{"
         )
-        ap(f"  extern __shared__ __align__(16) unsigned char lcm_smem[];")
-        ap(f"  {TT}* tab = reinterpret_cast<{TT}*>(lcm_smem);")
+        ap("  extern __shared__ __align__(16) unsigned char lcm_smem[];")
+        ap(f"  {TT}* tabf = reinterpret_cast<{TT}*>(lcm_smem);")
+        ap(f"  int* tabi = reinterpret_cast<int*>(lcm_smem + {NF * CH * (4 if fp32 else 8)});")
         ap("  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {")
         ap("    const int item = lcm_find_item(tile_prefix, n_items, tile);")
-        ap(f"    const i64* it = items + (i64)item * {self.n_words};")
+        ap(f"    const i64* __restrict__ it = items + (i64)item * {self.n_words};")
+        ap(f"    Ctx_{self.tag}<{ST}, {ST}> C; C.load(it);")
         ap(f"    const double* __restrict__ PV = lcm_wp<const double>(it, {self.W_P});")
         ap(f"    const int period = lcm_wi(it, {self.W_PERIOD});")
         ap(f"    const double age = lcm_wd(it, {self.W_AGE});")
         ap(f"    const int n_states = lcm_wi(it, {self.W_NSTATES});")
         ap(f"    const int n_actions = lcm_wi(it, {self.W_NACT});")
-        ap(f"    const int s = (tile - tile_prefix[item]) * {SPT} + (int)threadIdx.x / {LANES};")
+        ap(f"    const int n_ac = n_actions / {ND};")
+        ap(f"    const double* __restrict__ atf = lcm_wp<const double>(it, {self.W_ATAB});")
+        ap(f"    const int* __restrict__ ati = reinterpret_cast<const int*>(atf + (i64){nf} * n_actions);")
+        ap(f"    const int sbase = (tile - tile_prefix[item]) * {SPT} + (int)threadIdx.x / {LANES};")
         ap(f"    const int lane = (int)threadIdx.x % {LANES};")
-        ap("    const bool active = s < n_states;")
-        # decode state
-        ap("    int srem = active ? s : 0;")
-        for k in range(len(spec.states) - 1, -1, -1):
-            ax = spec.states[k]
-            ap(f"    const int si_{ax.name} = srem % lcm_wi(it, {self.W_SSIZE + k}); srem /= lcm_wi(it, {self.W_SSIZE + k});")
-        for k, ax in enumerate(spec.states):
-            if ax.kind == "continuous":
-                ap(f"    const double sv_{ax.name} = lcm_wp<const double>(it, {self.W_SGRID + k})[si_{ax.name}];")
-        # P phase
+        ap("    (void)period; (void)age; (void)ati; (void)PV;")
         for s_ in eP.lines:
             ap("    " + s_)
-        ap(f"    double PVd[{n_bP}];")
-        for i, n in enumerate(bP):
-            ap(f"    PVd[{i}] = (double)({pvals[id(n)]});")
+        ap(f"    double PVd[{nP}];")
+        for i, v in enumerate(pvals):
+            ap(f"    PVd[{i}] = (double)({v});")
         if not bP:
             ap("    PVd[0] = 0.0;")
-        # S phase
-        for s_ in eS.lines:
-            ap("    " + s_)
-        ap(f"    double SV[{n_bS}];")
-        for i, n in enumerate(bS):
-            ap(f"    SV[{i}] = (double)({svals[id(n)]});")
+        ap(f"    int SI[{SB}][{NDS}]; double SV[{SB}][{nS}]; bool act[{SB}]; int sidx[{SB}];")
+        ap(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
+        ap(f"      const int s = sbase + kb * {SPB};")
+        ap("      act[kb] = s < n_states; sidx[kb] = s;")
+        ap("      int srem = act[kb] ? s : 0;")
+        for k in range(len(spec.states) - 1, -1, -1):
+            ax = spec.states[k]
+            ap(f"      const int si_{ax.name} = srem % lcm_wi(it, {self.W_SSIZE + k}); srem /= lcm_wi(it, {self.W_SSIZE + k});")
+        for k, ax in enumerate(spec.states):
+            if ax.kind == "continuous":
+                ap(f"      const double sv_{ax.name} = lcm_wp<const double>(it, {self.W_SGRID + k})[si_{ax.name}];")
+        for s_ in s_lines:
+            ap("      " + s_)
+        for i, v in enumerate(s_vals):
+            ap(f"      SV[kb][{i}] = (double)({v});")
         if not bS:
-            ap("    SV[0] = 0.0;")
+            ap("      SV[kb][0] = 0.0;")
+        for i, a in enumerate(dstates):
+            ap(f"      SI[kb][{i}] = si_{a.name};")
+        if not dstates:
+            ap("      SI[kb][0] = 0;")
+        ap("    }")
         BEST = "LcmBest2" if (fp32 and not taste) else "LcmBest"
         if taste:
-            ap(f"    LcmBest<{ST}> bd[{ND}];")
-            ap(f"    #pragma unroll\n    for (int d = 0; d < {ND}; ++d) bd[d].init();")
+            ap(f"    LcmBest<{ST}> bd[{SB}][{ND}];")
         else:
-            ap(f"    {BEST}<{ST}> best; best.init();")
-        ap(f"    for (int a0 = 0; a0 < n_actions; a0 += {CH}) {{")
-        ap(f"      const int cn = min({CH}, n_actions - a0);")
-        ap("      __syncthreads();")
-        ap(f"      for (int j = threadIdx.x; j < cn; j += {B}) {{")
-        fill: list[str] = []
-        flds = emit_A(fill, "a0 + j", "t")
-        for s_ in fill:
-            ap("        " + s_)
-        for i, (expr, dt) in enumerate(flds):
-            ap(f"        tab[{i} * {CH} + j] = ({TT})({expr});")
+            ap(f"    {BEST}<{ST}> best[{SB}];")
+            ap(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) best[kb].init();")
+        # ---- discrete-action loop (unrolled: ND is a compile-time constant)
+        ap(f"    #pragma unroll\n    for (int ad = 0; ad < {ND}; ++ad) {{")
+        dl: list[str] = []
+        decode_disc(dl, "ad")
+        for s_ in dl:
+            ap("      " + s_)
+        for s_ in d_lines:
+            ap("      " + s_)
+        ap(f"      double DV[{nD}];")
+        for i, v in enumerate(d_vals):
+            ap(f"      DV[{i}] = (double)({v});")
+        if not bD:
+            ap("      DV[0] = 0.0;")
+        ap(f"      double SDV[{SB}][{nSD}];")
+        ap(f"      #pragma unroll\n      for (int kb = 0; kb < {SB}; ++kb) {{")
+        if bSD:
+            # re-derive the state variables of slot kb for the SD phase
+            ap("        int srem = act[kb] ? sidx[kb] : 0;")
+            for k in range(len(spec.states) - 1, -1, -1):
+                ax = spec.states[k]
+                ap(f"        const int si_{ax.name} = srem % lcm_wi(it, {self.W_SSIZE + k}); srem /= lcm_wi(it, {self.W_SSIZE + k});")
+            for k, ax in enumerate(spec.states):
+                if ax.kind == "continuous":
+                    ap(f"        const double sv_{ax.name} = lcm_wp<const double>(it, {self.W_SGRID + k})[si_{ax.name}];")
+            for s_ in sd_lines:
+                ap("        " + s_)
+            for i, v in enumerate(sd_vals):
+                ap(f"        SDV[kb][{i}] = (double)({v});")
+        else:
+            ap("        SDV[kb][0] = 0.0;")
         ap("      }")
-        ap("      __syncthreads();")
-        ap("      if (active) {")
-        ap(f"        for (int j = lane; j < cn; j += {LANES}) {{")
-        ap(f"          AFTab_{self.tag}<{ST}> af{{tab, j, {CH}}};")
-        ap(f"          {ST} q;")
-        ap(
-            f"          if (lcm_sa_{self.tag}<{ST}, {ST}>(it, PV, PVd, SV, af, {si_args}period, age, q)) "
-            + (f"bd[(int)af({len(a_fields) - 1})].push(q, a0 + j);" if taste else "best.push(q, a0 + j);")
-        )
-        ap("        }")
-        ap("      }")
-        ap("    }")
-        # reduction
         if taste:
-            ap(f"    #pragma unroll\n    for (int d = 0; d < {ND}; ++d) lcm_group_reduce<{LANES}, {ST}>(bd[d]);")
-        elif fp32:
-            ap(f"    lcm_group_reduce2<{LANES}, {ST}>(best);")
-        else:
-            ap(f"    lcm_group_reduce<{LANES}, {ST}>(best);")
-        ap("    if (active && lane == 0) {")
-        ap(f"      double* Vout = lcm_wp<double>(it, {self.W_V});")
-        ap(f"      int* Pout = lcm_wp<int>(it, {self.W_POL});")
+            ap(f"      #pragma unroll\n      for (int kb = 0; kb < {SB}; ++kb) bd[kb][ad].init();")
 
-        # final evaluation at an action index (double), used by fp32 mode
-        def final_eval(a_var: str, out_var: str) -> list[str]:
-            lines: list[str] = [f"AFLoc_{self.tag} afl;"]
-            fl = emit_A(lines, a_var, "f")
-            for i, (expr, dt) in enumerate(fl):
-                lines.append(f"afl.v[{i}] = (double)({expr});")
+        def inner_loop(sa_fn: str) -> list[str]:
+            o = []
+            o.append(f"for (int c0 = 0; c0 < n_ac; c0 += {CH}) {{")
+            o.append(f"  const int cn = min({CH}, n_ac - c0);")
+            o.append("  __syncthreads();")
+            o.append(f"  for (int j = threadIdx.x; j < cn; j += {B}) {{")
+            o.append("    const i64 a = (i64)ad * n_ac + c0 + j;")
+            for k in range(nf):
+                o.append(f"    tabf[{k} * {CH} + j] = ({TT})atf[(i64){k} * n_actions + a];")
+            for k in range(ni):
+                o.append(f"    tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
+            o.append("  }")
+            o.append("  __syncthreads();")
+            o.append(f"  for (int j = lane; j < cn; j += {LANES}) {{")
+            o.append(f"    AFTab_{self.tag}<{ST}> af{{tabf, tabi, j}};")
+            o.append("    const int aidx = ad * n_ac + c0 + j;")
+            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
+            o.append(f"      {ST} q;")
+            di_args = "".join(f"DI_{a.name}, " for a in dacts)
+            call = f"{sa_fn}<{ST}, {ST}>(C, PV, PVd, DV, SV[kb], SDV[kb], af, SI[kb], {di_args}period, age, q)"
+            push = "bd[kb][ad].push(q, aidx);" if taste else "best[kb].push(q, aidx);"
+            o.append(f"      if ({call}) {push}")
+            o.append("    }")
+            o.append("  }")
+            o.append("}")
+            return o
+
+        if unswitch:
+            rid_expr = f"(int)PVd[{[id(x) for x in bP].index(id(self.tr.regime_id))}]" if rid_phase == "P" else None
+            if rid_phase == "D":
+                rid_expr = f"(int)DV[{[id(x) for x in bD].index(id(self.tr.regime_id))}]"
+            ap(f"      const int rid = {rid_expr};")
+            first = True
+            for ti, t in enumerate(self.targets):
+                ap(f"      {'if' if first else 'else if'} (rid == {t.spec.rid}) {{")
+                first = False
+                for s_ in inner_loop(SA.format(ti + 1)):
+                    ap("        " + s_)
+                ap("      }")
+            ap("      else {")
+            for s_ in inner_loop(SA.format(0)):
+                ap("        " + s_)
+            ap("      }")
+        else:
+            for s_ in inner_loop(SA.format(0)):
+                ap("      " + s_)
+        ap("    }")
+
+        # ---- reduction and epilogue
+        def final_eval(a_var: str, out_var: str, loc: str) -> list[str]:
+            lines = [f"AFLoc_{self.tag} {loc}; Ctx_{self.tag}<double, double> Cd; Cd.load(it);"]
+            for k in range(nf):
+                lines.append(f"{loc}.v[{k}] = atf[(i64){k} * n_actions + {a_var}];")
+            for k in range(ni):
+                lines.append(f"{loc}.vi[{k}] = ati[(i64){k} * n_actions + {a_var}];")
+            decode_disc(lines, f"{a_var} / n_ac")
+            lines += d_lines
+            lines.append(f"double DV[{nD}];")
+            for i, v in enumerate(d_vals):
+                lines.append(f"DV[{i}] = (double)({v});")
+            if not bD:
+                lines.append("DV[0] = 0.0;")
+            lines.append(f"double SDVf[{nSD}];")
+            if bSD:
+                lines.append("{ int srem = s;")
+                for k in range(len(spec.states) - 1, -1, -1):
+                    ax = spec.states[k]
+                    lines.append(f"const int si_{ax.name} = srem % lcm_wi(it, {self.W_SSIZE + k}); srem /= lcm_wi(it, {self.W_SSIZE + k});")
+                for k, ax in enumerate(spec.states):
+                    if ax.kind == "continuous":
+                        lines.append(f"const double sv_{ax.name} = lcm_wp<const double>(it, {self.W_SGRID + k})[si_{ax.name}];")
+                lines += sd_lines
+                for i, v in enumerate(sd_vals):
+                    lines.append(f"SDVf[{i}] = (double)({v});")
+                lines.append("}")
+            else:
+                lines.append("SDVf[0] = 0.0;")
+            di_args = "".join(f"DI_{a.name}, " for a in dacts)
             lines.append(f"double {out_var};")
             lines.append(
-                f"if (!lcm_sa_{self.tag}<double, double>(it, PV, PVd, SV, afl, {si_args}period, age, {out_var})) {out_var} = -lcm_lim<double>::inf();"
+                f"if (!{SA.format(0)}<double, double>(Cd, PV, PVd, DV, SV[kb], SDVf, {loc}, SI[kb], {di_args}period, age, {out_var})) {out_var} = -lcm_lim<double>::inf();"
             )
             return lines
 
+        ap(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
         if taste:
-            ap(f"      double vals[{ND}]; int bdi = -1; double bv = -lcm_lim<double>::inf(); int anynan = 0;")
-            ap(f"      for (int d = 0; d < {ND}; ++d) {{")
-            ap("        anynan |= bd[d].nan;")
-            ap("        if (bd[d].idx < 0) { vals[d] = -lcm_lim<double>::inf(); continue; }")
-            if fp32:
-                ap("        { const int aa = bd[d].idx;")
-                for s_ in final_eval("aa", "qd"):
-                    ap("          " + s_)
-                ap("          vals[d] = qd; }")
-            else:
-                ap("        vals[d] = bd[d].v;")
-            ap("        if (bdi < 0 || vals[d] > bv) { bv = vals[d]; bdi = d; }")
-            ap("      }")
-            ap(f"      const double scale = lcm_wd(it, {self.W_TASTE});")
-            ap(f"      double v = lcm_logsum<double, {ND}>(vals, scale);")
-            ap("      if (anynan) v = lcm_lim<double>::nan();")
-            ap("      Vout[s] = v; Pout[s] = (bdi < 0 || anynan) ? 0 : bd[bdi].idx;")
+            ap(f"      #pragma unroll\n      for (int d = 0; d < {ND}; ++d) lcm_group_reduce<{LANES}, {ST}>(bd[kb][d]);")
+        elif fp32:
+            ap(f"      lcm_group_reduce2<{LANES}, {ST}>(best[kb]);")
         else:
-            ap("      double v; int pol;")
-            ap("      if (best.nan) { v = lcm_lim<double>::nan(); pol = 0; }")
-            ap("      else if (best.idx < 0) { v = -lcm_lim<double>::inf(); pol = 0; }")
+            ap(f"      lcm_group_reduce<{LANES}, {ST}>(best[kb]);")
+        ap("      if (act[kb] && lane == 0) {")
+        ap("        const int s = sidx[kb];")
+        ap(f"        double* Vout = lcm_wp<double>(it, {self.W_V});")
+        ap(f"        int* Pout = lcm_wp<int>(it, {self.W_POL});")
+        if taste:
+            ap(f"        double vals[{ND}]; int bdi = -1; double bv = -lcm_lim<double>::inf(); int anynan = 0;")
+            ap(f"        for (int d = 0; d < {ND}; ++d) {{")
+            ap("          anynan |= bd[kb][d].nan;")
+            ap("          if (bd[kb][d].idx < 0) { vals[d] = -lcm_lim<double>::inf(); continue; }")
             if fp32:
-                # re-rank the two single-precision candidates in double precision
-                ap("      else { const int aa = best.idx;")
-                for s_ in final_eval("aa", "qd"):
-                    ap("        " + s_)
-                ap("        v = qd; pol = aa;")
-                ap("        if (best.idx2 >= 0) { const int ab = best.idx2;")
-                for s_ in final_eval("ab", "qd2"):
-                    ap("          " + s_.replace("afl", "afl2"))
-                ap("          if (qd2 > v || (qd2 == v && ab < pol)) { v = qd2; pol = ab; } }")
-                ap("      }")
+                ap("          { const int aa = bd[kb][d].idx;")
+                for s_ in final_eval("aa", "qd", "afl"):
+                    ap("            " + s_)
+                ap("            vals[d] = qd; }")
             else:
-                ap("      else { v = (double)best.v; pol = best.idx; }")
-            ap("      Vout[s] = v; Pout[s] = pol;")
+                ap("          vals[d] = bd[kb][d].v;")
+            ap("          if (bdi < 0 || vals[d] > bv) { bv = vals[d]; bdi = d; }")
+            ap("        }")
+            ap(f"        const double scale = lcm_wd(it, {self.W_TASTE});")
+            ap(f"        double v = lcm_logsum<double, {ND}>(vals, scale);")
+            ap("        if (anynan) v = lcm_lim<double>::nan();")
+            ap("        int pol = 0;")
+            ap(f"        for (int d = 0; d < {ND}; ++d) if (d == bdi) pol = bd[kb][d].idx;")
+            ap("        Vout[s] = v; Pout[s] = (bdi < 0 || anynan) ? 0 : pol;")
+        else:
+            ap("        double v; int pol;")
+            ap("        if (best[kb].nan) { v = lcm_lim<double>::nan(); pol = 0; }")
+            ap("        else if (best[kb].idx < 0) { v = -lcm_lim<double>::inf(); pol = 0; }")
+            if fp32:
+                ap("        else { const int aa = best[kb].idx;")
+                for s_ in final_eval("aa", "qd", "afl"):
+                    ap("          " + s_)
+                ap("          v = qd; pol = aa;")
+                ap("          if (best[kb].idx2 >= 0) { const int ab = best[kb].idx2;")
+                for s_ in final_eval("ab", "qd2", "afl2"):
+                    ap("            " + s_)
+                ap("            if (qd2 > v || (qd2 == v && ab < pol)) { v = qd2; pol = ab; } }")
+                ap("        }")
+            else:
+                ap("        else { v = (double)best[kb].v; pol = best[kb].idx; }")
+            ap("        Vout[s] = v; Pout[s] = pol;")
+        ap("      }")
         ap("    }")
         ap("  }")
         ap("}")
-        self.smem_bytes = NAF * CH * (4 if fp32 else 8)
+        self.smem_bytes = NF * CH * (4 if fp32 else 8) + NI * CH * 4
+        self.atab_words = nf * 2 + ni
+
+        # ----------------------------------------------------------------
+        # kernel (a0): continuous-action-only sub-expressions, one thread per action
+        ap(f"// ---- regime {spec.name}: action table (kernel a0)")
+        ap(
+            f'extern "C" __global__ void __launch_bounds__(256) {self.atab_name()}('
+            "const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles) {"
+        )
+        ap("  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {")
+        ap("    const int item = lcm_find_item(tile_prefix, n_items, tile);")
+        ap(f"    const i64* __restrict__ it = items + (i64)item * {self.n_words};")
+        ap(f"    const double* __restrict__ PV = lcm_wp<const double>(it, {self.W_P});")
+        ap(f"    const int period = lcm_wi(it, {self.W_PERIOD});")
+        ap(f"    const double age = lcm_wd(it, {self.W_AGE});")
+        ap(f"    const int n_actions = lcm_wi(it, {self.W_NACT});")
+        ap(f"    double* atf = lcm_wp<double>(it, {self.W_ATAB});")
+        ap(f"    int* ati = reinterpret_cast<int*>(atf + (i64){nf} * n_actions);")
+        ap("    (void)period; (void)age; (void)ati; (void)PV;")
+        ap("    const int a = (tile - tile_prefix[item]) * 256 + (int)threadIdx.x;")
+        ap("    if (a < n_actions) {")
+        ap("      int arem = a;")
+        prov = pv()
+        for k in range(len(spec.actions) - 1, -1, -1):
+            ax = spec.actions[k]
+            ap(f"      const int ai_{ax.name} = arem % lcm_wi(it, {self.W_ASIZE + k}); arem /= lcm_wi(it, {self.W_ASIZE + k});")
+        for k, ax in enumerate(spec.actions):
+            if ax.kind == "continuous":
+                ap(f"      const double av_{ax.name} = lcm_wp<const double>(it, {self.W_AGRID + k})[ai_{ax.name}];")
+                prov[id(ir.var("action", ax.name, "f"))] = f"av_{ax.name}"
+            else:
+                prov[id(ir.var("action", ax.name, "i"))] = f"ai_{ax.name}"
+        e = Emitter("double", self.param_off, prov, "t")
+        vals = [e.emit(n) for n in bA]
+        for s_ in e.lines:
+            ap("      " + s_)
+        for i, (n, v) in enumerate(zip(bA, vals)):
+            col, k = slot[i]
+            if col == "F":
+                ap(f"      atf[(i64){k} * n_actions + a] = (double)({v});")
+            else:
+                ap(f"      ati[(i64){k} * n_actions + a] = (int)({v});")
+        ap("    }")
+        ap("  }")
+        ap("}")
         return "\n".join(L)
 
     # ------------------------------------------------------------------ (b)

@@ -56,13 +56,22 @@ template <typename T> __device__ __forceinline__ T lcm_zs(T w, T v) {
   return (w == T(0) && !lcm_isfinite(v)) ? T(0) : w * v;
 }
 
-// Lower bracket index of a fractional coordinate: clip(floor(c), 0, n-2).
-template <typename T> __device__ __forceinline__ int lcm_lower(T c, int n) {
-  T f = floor(c);
-  T hi = (T)(n - 2);
-  f = f < T(0) ? T(0) : f;
-  f = f > hi ? hi : f;
-  return (f == f) ? (int)f : 0;
+// Lower bracket of a fractional coordinate, clip(floor(c), 0, n-2), as an
+// int and as a float.  The coordinate is clamped to [0, n-2] first (fmin/fmax
+// send NaN to 0); floor of a value in [0, 2^23) is then a round-down add of
+// 2^23, whose low mantissa bits are the integer -- no conversion instruction.
+// Valid for grids of fewer than 2^23 points.
+__device__ __forceinline__ int lcm_lower(float c, int n, float& lof) {
+  float cc = fminf(fmaxf(c, 0.0f), (float)(n - 2));
+  float m = __fadd_rd(cc, 8388608.0f);
+  lof = m - 8388608.0f;
+  return __float_as_int(m) - 0x4B000000;
+}
+__device__ __forceinline__ int lcm_lower(double c, int n, double& lof) {
+  double cc = fmin(fmax(c, 0.0), (double)(n - 2));
+  double m = __dadd_rd(cc, 4503599627370496.0);
+  lof = m - 4503599627370496.0;
+  return (int)(__double_as_longlong(m) - 0x4330000000000000LL);
 }
 
 // Coordinate of x on a linearly spaced grid: (x - start) / step, computed as
@@ -103,11 +112,15 @@ __device__ __forceinline__ T lcm_coord_irreg(T x, const double* __restrict__ pts
 // 1-D linear read with extrapolation; `row` is contiguous.
 template <typename T, typename S>
 __device__ __forceinline__ T lcm_interp1(const S* __restrict__ row, int n, T c) {
-  int lo = lcm_lower(c, n);
-  T wu = c - (T)lo;
+  T lof;
+  int lo = lcm_lower(c, n, lof);
+  T wu = c - lof;
   T wl = T(1) - wu;
   T v0 = (T)row[lo];
   T v1 = (T)row[lo + 1];
+  // a finite result implies finite corners; otherwise redo it zero-safely
+  T r = wl * v0 + wu * v1;
+  if (lcm_isfinite(r)) return r;
   return lcm_zs(wl, v0) + lcm_zs(wu, v1);
 }
 
@@ -115,15 +128,19 @@ __device__ __forceinline__ T lcm_interp1(const S* __restrict__ row, int n, T c) 
 // left-to-right summation follow map_coordinates (ndimage.py:71-97).
 template <typename T, typename S>
 __device__ __forceinline__ T lcm_interp2(const S* __restrict__ blk, int n0, int n1, T c0, T c1) {
-  int l0 = lcm_lower(c0, n0), l1 = lcm_lower(c1, n1);
-  T u0 = c0 - (T)l0, u1 = c1 - (T)l1;
+  T f0, f1;
+  int l0 = lcm_lower(c0, n0, f0), l1 = lcm_lower(c1, n1, f1);
+  T u0 = c0 - f0, u1 = c1 - f1;
   T d0 = T(1) - u0, d1 = T(1) - u1;
   const S* r0 = blk + (i64)l0 * n1;
   const S* r1 = r0 + n1;
-  T acc = lcm_zs(d0 * d1, (T)r0[l1]);
-  acc = acc + lcm_zs(d0 * u1, (T)r0[l1 + 1]);
-  acc = acc + lcm_zs(u0 * d1, (T)r1[l1]);
-  acc = acc + lcm_zs(u0 * u1, (T)r1[l1 + 1]);
+  const T a = (T)r0[l1], b = (T)r0[l1 + 1], c = (T)r1[l1], d = (T)r1[l1 + 1];
+  T r = d0 * d1 * a + d0 * u1 * b + u0 * d1 * c + u0 * u1 * d;
+  if (lcm_isfinite(r)) return r;
+  T acc = lcm_zs(d0 * d1, a);
+  acc = acc + lcm_zs(d0 * u1, b);
+  acc = acc + lcm_zs(u0 * d1, c);
+  acc = acc + lcm_zs(u0 * u1, d);
   return acc;
 }
 
@@ -166,9 +183,14 @@ template <typename T> struct LcmBest2 {
     if (better(q, a, v, idx)) { v2 = v; idx2 = idx; v = q; idx = a; }
     else if (a != idx && better(q, a, v2, idx2)) { v2 = q; idx2 = a; }
   }
+  // sequential scan within one lane: indices arrive in increasing order, so a
+  // tie never displaces an earlier candidate
   __device__ __forceinline__ void push(T q, int a) {
     if (q != q) { nan = 1; return; }
-    add(q, a);
+    if (q > v2 || idx2 < 0) {
+      if (q > v || idx < 0) { v2 = v; idx2 = idx; v = q; idx = a; }
+      else { v2 = q; idx2 = a; }
+    }
   }
   __device__ __forceinline__ void merge(T ov, int oi, T ov2, int oi2, int onan) {
     nan |= onan;

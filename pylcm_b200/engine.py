@@ -49,16 +49,20 @@ class Launch:
     period: int
 
 
-def default_config(spec: RegimeSpec, precision: str) -> LaunchConfig:
-    """Heuristic launch shape: few actions per state -> more lanes per state."""
+SM_COUNT = 148
+RESIDENT_THREADS_PER_SM = 1024
+
+
+def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> LaunchConfig:
+    """Launch shape: the fewest lanes per state (1 = one thread per state)
+    that still fills the GPU (SM count x resident threads) with the batch's
+    states; more lanes only when the batch has too few states."""
     n_a = spec.n_actions
-    n_s = spec.n_states
-    if n_s <= 4096 and n_a >= 64:
-        lanes = 32
-    elif n_s <= 65536 and n_a >= 64:
-        lanes = 4
-    else:
-        lanes = 1
+    total = max(1, spec.n_states * n_items)
+    want = SM_COUNT * RESIDENT_THREADS_PER_SM
+    lanes = 1
+    while lanes < 32 and total * lanes < want and n_a >= 8 * lanes * 2:
+        lanes *= 2
     chunk = 512 if precision == "fp32" else 256
     return LaunchConfig(block=256, lanes=lanes, chunk=chunk)
 
@@ -84,11 +88,11 @@ class SolveEngine:
     def resolver(self, params) -> ParamResolver:
         return ParamResolver(params, self.model.fixed_params, tuple(s.name for s in self.specs))
 
-    def config_for(self, spec: RegimeSpec) -> LaunchConfig:
-        return self.configs.get(spec.name) or default_config(spec, self.precision)
+    def config_for(self, spec: RegimeSpec, n_items: int = 1) -> LaunchConfig:
+        return self.configs.get(spec.name) or default_config(spec, self.precision, n_items)
 
-    def kernels(self, spec: RegimeSpec, targets: tuple[str, ...], params) -> RegimeKernels:
-        cfg = self.config_for(spec)
+    def kernels(self, spec: RegimeSpec, targets: tuple[str, ...], params, n_items: int = 1) -> RegimeKernels:
+        cfg = self.config_for(spec, n_items)
         key = (spec.name, targets, cfg)
         rk = self._kernels.get(key)
         if rk is None:
@@ -179,7 +183,7 @@ class SolvePlan:
                 if not s.terminal and period == T - 1:
                     raise ModelInitializationError(f"non-terminal regime {s.name} active in the last period")
                 targets = eng.targets_at(s, period)
-                rk = eng.kernels(s, targets, params_list[0])
+                rk = eng.kernels(s, targets, params_list[0], n)
                 key = (s.name, targets)
                 if key not in self.params:
                     vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in resolvers]
@@ -200,6 +204,15 @@ class SolvePlan:
                 e64 = torch.empty((n, t.K, ncols), dtype=torch.float64, device=dev)
                 e32 = torch.empty((n, t.K, ncols), dtype=torch.float32, device=dev) if fp32 else None
                 self.ev[k] = (e64, e32, ncols, cblk)
+
+        # action tables (kernel a0 output) per (regime, target set), reused across periods
+        self.atab: dict[tuple, Any] = {}
+        for period, s, targets, rk in step_list:
+            k = (s.name, targets)
+            if k not in self.atab:
+                words = max(1, rk.atab_words) * s.n_actions
+                words += words % 2  # keep each instance's table 8-byte aligned
+                self.atab[k] = torch.empty((n, words), dtype=torch.int32, device=dev)
 
         # ---- item records
         words: list[np.ndarray] = []
@@ -277,6 +290,7 @@ class SolvePlan:
                     g = self.agrid[s.name][k]
                     r[rk.W_AGRID + k] = g.data_ptr() if g is not None else 0
                 r[rk.W_TASTE] = _f2w(rk.tr.taste_scale if rk.tr.taste_scale else 0.0)
+                r[rk.W_ATAB] = self.atab[(s.name, targets)][i].data_ptr()
                 if s.taste_shocks:
                     r[rk.W_TASTE] = _f2w(resolvers[i].taste_scale(s.name))
                 for t in rk.targets:
@@ -309,7 +323,20 @@ class SolvePlan:
                 recs.append(r)
             spt = rk.cfg.states_per_tile
             tiles = [math.ceil(s.n_states / spt)] * n
-            add_launch("bellman", rk, rk.bellman_name(), recs, tiles, rk.cfg.block, rk.smem_bytes, period)
+            add_launch("atab", rk, rk.atab_name(), recs, [math.ceil(s.n_actions / 256)] * n, 256, 0, period)
+            # kernel (a) reads the same records
+            self.launches.append(
+                Launch("bellman", rk, rk.bellman_name(), self.launches[-1].item_off, p_off, n,
+                       int(sum(tiles)), rk.cfg.block, rk.smem_bytes, period)
+            )
+            pre = np.zeros(n + 1, dtype=np.int32)
+            pre[1:] = np.cumsum(tiles)
+            prefixes.append(pre)
+            p_off += pre.size
+            pad = (-p_off) % 4
+            if pad:
+                prefixes.append(np.zeros(pad, dtype=np.int32))
+                p_off += pad
 
         self.items = torch.as_tensor(np.concatenate(words), dtype=torch.int64, device=dev)
         self.prefix = torch.as_tensor(np.concatenate(prefixes), dtype=torch.int32, device=dev)
@@ -328,10 +355,10 @@ class SolvePlan:
             mod = l.module.module
             ip = ib + 8 * l.item_off
             pp = pb + 4 * l.prefix_off
-            if l.kind == "bellman":
-                mod.bellman_step(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
-            else:
+            if l.kind == "expect":
                 mod.expectation(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
+            else:
+                mod.bellman_step(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
 
     def capture(self) -> None:
         """Capture the launch list in a CUDA graph (replayed by run_graph)."""

@@ -272,6 +272,7 @@ class TracedRegime:
     U: ir.Expr
     F: ir.Expr
     regime_probs: list | None  # one Expr per regime id (non-terminal only)
+    regime_id: ir.Expr | None  # the next regime id, when the transition is deterministic
     next_states: dict[str, dict[str, NextState]]  # target -> state -> law
     param_values: dict[str, np.ndarray]  # flat name -> value (float64)
     param_order: list[str]
@@ -482,6 +483,7 @@ def trace_regime(
     beta = None
     taste_scale = None
     regime_probs = None
+    regime_id = None
     next_states: dict[str, dict[str, NextState]] = {}
     if not spec.terminal:
         ok, bval = resolver.find(spec.name, BETA_FUNC, BETA_ARG)
@@ -503,6 +505,7 @@ def trace_regime(
                     "wrapped in MarkovTransition"
                 )
             rid = ir.const(raw)
+            regime_id = rid if rid.dtype == "i" else rid.astype("i")
             regime_probs = [ir.where(ir._cmp("==", rid, k), 1.0, 0.0) for k in range(n_reg)]
         by_name = {s.name: s for s in all_specs}
         for tname in targets:
@@ -553,6 +556,7 @@ def trace_regime(
         U=U,
         F=F,
         regime_probs=regime_probs,
+        regime_id=regime_id,
         next_states=next_states,
         param_values=t.param_values,
         param_order=t.param_order,

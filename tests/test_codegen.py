@@ -91,4 +91,6 @@ def test_phase_split_hoists_utility_out_of_the_state_loop():
     s = eng.specs[0]
     rk = eng.kernels(s, eng.targets_at(s, 0), params)
     assert C._phase(rk.tr.U) == "A"
-    assert "log(" not in rk.src.split("lcm_sa_")[1].split("return true;")[0]
+    inner = rk.src.split("__device__ __forceinline__ bool lcm_sa0_")[1].split("return true;")[0]
+    assert "log(" not in inner
+    assert "log(" in rk.src.split("lcm_atab_")[-1]
