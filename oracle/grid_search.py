@@ -73,6 +73,13 @@ def grid_coordinate(grid, values: np.ndarray) -> np.ndarray:
     raise ValueError(kind)
 
 
+def _irreg_coordinate(pts: np.ndarray, v: np.ndarray) -> np.ndarray:
+    n = len(pts)
+    up = np.clip(np.searchsorted(pts, v, side="right"), 1, n - 1)
+    lo = up - 1
+    return lo + (v - pts[lo]) / (pts[up] - pts[lo])
+
+
 def zero_safe(w: np.ndarray, v: np.ndarray) -> np.ndarray:
     """w * v with w == 0 annihilating +-inf/nan (``zero_safe.py:161-251``)."""
     w = np.asarray(w, dtype=np.float64)
@@ -229,17 +236,28 @@ def bellman_step(
     age: float,
     next_V: dict[str, np.ndarray],
     state_rows: np.ndarray | None = None,
-) -> tuple[np.ndarray, np.ndarray]:
+    state_values: dict | None = None,
+    return_qf: bool = False,
+):
     """V and policy (flat action index) of `spec` at `period`.
 
     `next_V` maps each regime active next period to its value array.
     `state_rows` optionally restricts the computation to a subset of flat
-    state indices (used for bounded CPU timing samples).
+    state indices (used for bounded CPU timing samples).  `state_values`
+    (name -> array) evaluates at arbitrary, off-grid states instead (the
+    simulation): a process state's transition weights are then the
+    transition-matrix rows interpolated at the value's node coordinate
+    (``processing.py:2780-2839``).  With `return_qf` the (Q, F) matrices are
+    returned instead of (V, policy).
     """
     sshape = spec.state_shape
     n_s = spec.n_states
-    rows = np.arange(n_s) if state_rows is None else np.asarray(state_rows)
-    s_idx = np.unravel_index(rows, sshape) if spec.states else ()
+    if state_values is not None:
+        n_rows = len(next(iter(state_values.values()))) if state_values else 1
+        rows = np.arange(n_rows)
+    else:
+        rows = np.arange(n_s) if state_rows is None else np.asarray(state_rows)
+    s_idx = np.unravel_index(rows, sshape) if (spec.states and state_values is None) else ()
     ashape = tuple(a.size for a in spec.actions)
     n_a = spec.n_actions
     a_idx = np.unravel_index(np.arange(n_a), ashape) if spec.actions else ()
@@ -247,7 +265,23 @@ def bellman_step(
 
     env: dict[str, Any] = {"period": period, "age": age}
     sidx_of: dict[str, np.ndarray] = {}
+    blend: dict[str, tuple] = {}
     for k, ax in enumerate(spec.states):
+        if state_values is not None:
+            x = np.asarray(state_values[ax.name], dtype=np.float64)[:, None]
+            if ax.kind == "process":
+                nodes = procs[ax.name][0]
+                c = _irreg_coordinate(nodes, x)
+                lo = np.clip(np.floor(c), 0, len(nodes) - 2).astype(np.int64)
+                blend[ax.name] = (lo, c - lo)
+                sidx_of[ax.name] = lo
+                env[ax.name] = x
+            elif ax.kind == "discrete":
+                sidx_of[ax.name] = x.astype(np.int64)
+                env[ax.name] = x.astype(np.int64)
+            else:
+                env[ax.name] = x
+            continue
         i = s_idx[k][:, None]
         sidx_of[ax.name] = i
         if ax.kind == "process":
@@ -297,7 +331,7 @@ def bellman_step(
                 E = np.broadcast_to(np.asarray(next_V[tgt.name], dtype=np.float64), bshape)
             else:
                 E = _expected_next_value(
-                    spec, tgt, resolver, ev, next_V[tgt.name], procs, sidx_of, aidx_of, bshape, period, age
+                    spec, tgt, resolver, ev, next_V[tgt.name], procs, sidx_of, aidx_of, bshape, period, age, blend
                 )
             CE = CE + zero_safe(p, E)
         valid = (np.abs(mass - 1.0) <= 1e-3) & ~neg
@@ -305,6 +339,8 @@ def bellman_step(
             CE = CE / np.where(valid, mass, np.nan)
         Q = U + beta * CE
 
+    if return_qf:
+        return Q, F
     if spec.taste_shocks:
         scale = resolver.taste_scale(spec.name)
         nd = spec.n_discrete_actions
@@ -377,17 +413,22 @@ def _lookup_table(deps, table, sidx_of, aidx_of, bshape, n_out):
     return out
 
 
-def _expected_next_value(spec, tgt, resolver, ev, V_next, procs, sidx_of, aidx_of, bshape, period, age):
+def _expected_next_value(spec, tgt, resolver, ev, V_next, procs, sidx_of, aidx_of, bshape, period, age, blend=None):
     """E[V'_tgt] at every (state, action): node-by-node interpolation."""
     laws = {}
     stoch_axes = []  # (axis position in tgt, list of weight arrays per node)
     det_idx = {}
     cont_vals = {}
+    blend = blend or {}
     for pos, ax in enumerate(tgt.states):
         if ax.kind == "process":
             P = procs[ax.name][1]
-            cur = sidx_of[ax.name]
-            ws = [np.broadcast_to(P[cur, j], bshape) for j in range(ax.size)]
+            if ax.name in blend:
+                lo, t = blend[ax.name]
+                ws = [np.broadcast_to(zero_safe(1 - t, P[lo, j]) + zero_safe(t, P[lo + 1, j]), bshape) for j in range(ax.size)]
+            else:
+                cur = sidx_of[ax.name]
+                ws = [np.broadcast_to(P[cur, j], bshape) for j in range(ax.size)]
             stoch_axes.append((pos, ws))
             continue
         fname = f"next_{ax.name}"

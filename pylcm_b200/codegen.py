@@ -599,7 +599,9 @@ class RegimeKernels:
         # ----------------------------------------------------------------
         # the inner (state, action) evaluation, templated on precision and on
         # the selected target (TSEL < 0: all targets by probability / id)
-        def sa_body(T: str, E: str, tsel: int) -> list[str]:
+        proc_names = [a.name for a in spec.states if a.kind == "process"]
+
+        def sa_body(T: str, E: str, tsel: int, sim: bool = False) -> list[str]:
             prov = pv()
             for i, n in enumerate(bP):
                 prov[id(n)] = _cast(f"PVd[{i}]", n.dtype, T)
@@ -667,13 +669,27 @@ class RegimeKernels:
                 else:
                     inner: list[str] = []
                     key = "0"
+                    key_hi = None
                     for kind, name, size in t.key_vars:
+                        if sim and kind == "state" and name in proc_names:
+                            if key_hi is not None:
+                                raise TracingError("simulation supports one process key per target")
+                            pi = proc_names.index(name)
+                            key_hi = f"({key}) * {size} + PLO[{pi}] + 1"
+                            key = f"({key}) * {size} + PLO[{pi}]"
+                            blend = pi
+                            continue
                         iv = f"SI[{[a.name for a in dstates].index(name)}]" if kind == "state" else f"DI_{name}"
                         key = f"({key}) * {size} + {iv}"
+                        if key_hi is not None:
+                            key_hi = f"({key_hi}) * {size} + {iv}"
                     off = key
+                    off_hi = key_hi
                     for pos in t.det_pos:
                         sz = f"C.n{ti}_{pos}"
                         off = f"({off}) * {sz} + min(max((int)({dn[(ti, pos)]}), 0), {sz} - 1)"
+                        if off_hi is not None:
+                            off_hi = f"({off_hi}) * {sz} + min(max((int)({dn[(ti, pos)]}), 0), {sz} - 1)"
                     cblk = "1"
                     for pos in t.cont_pos:
                         cblk = f"{cblk} * C.n{ti}_{pos}"
@@ -688,17 +704,24 @@ class RegimeKernels:
                         else:
                             cc = f"lcm_coord_irreg<{T}>(({T})({x}), C.p{ti}_{ci}, C.n{ti}_{pos})"
                         inner.append(f"{T} c{ci} = {cc};")
-                    inner.append(f"const {E}* row = C.ev{ti} + (i64)({off}) * ({cblk});")
-                    if len(t.cont_pos) == 0:
-                        inner.append(f"{T} ev = ({T})row[0];")
-                    elif len(t.cont_pos) == 1:
-                        inner.append(f"{T} ev = lcm_interp1<{T}, {E}>(row, C.n{ti}_{t.cont_pos[0]}, c0);")
-                    elif len(t.cont_pos) == 2:
-                        inner.append(
-                            f"{T} ev = lcm_interp2<{T}, {E}>(row, C.n{ti}_{t.cont_pos[0]}, C.n{ti}_{t.cont_pos[1]}, c0, c1);"
-                        )
-                    else:
-                        raise TracingError("more than two continuous states per target are not supported")
+                    rows = [("row", off)] + ([("rowh", off_hi)] if off_hi is not None else [])
+                    for rname, roff in rows:
+                        ev_name = "ev" if rname == "row" else "evh"
+                        inner.append(f"const {E}* {rname} = C.ev{ti} + (i64)({roff}) * ({cblk});")
+                        if len(t.cont_pos) == 0:
+                            inner.append(f"{T} {ev_name} = ({T}){rname}[0];")
+                        elif len(t.cont_pos) == 1:
+                            inner.append(f"{T} {ev_name} = lcm_interp1<{T}, {E}>({rname}, C.n{ti}_{t.cont_pos[0]}, c0);")
+                        elif len(t.cont_pos) == 2:
+                            inner.append(
+                                f"{T} {ev_name} = lcm_interp2<{T}, {E}>({rname}, C.n{ti}_{t.cont_pos[0]}, C.n{ti}_{t.cont_pos[1]}, c0, c1);"
+                            )
+                        else:
+                            raise TracingError("more than two continuous states per target are not supported")
+                    if off_hi is not None:
+                        # off-grid process value: blend the two bracketing node rows
+                        # (the reference interpolates the transition-matrix rows)
+                        inner.append(f"ev = lcm_zs(({T})1 - ({T})PT[{blend}], ev) + lcm_zs(({T})PT[{blend}], evh);")
                     out += ["    " + s for s in inner]
                 if det:
                     out.append("    ce = ev;")
@@ -724,6 +747,18 @@ class RegimeKernels:
             for s_ in sa_body("T", "E", tsel):
                 ap("  " + s_)
             ap("  return true;\n}")
+
+        ap(
+            f"template <typename T, typename E, typename AFN>\n"
+            f"__device__ __forceinline__ bool lcm_simsa_{self.tag}(const Ctx_{self.tag}<T, E>& C, "
+            f"const double* __restrict__ PV, const double* PVd, const double* DV, const double* SV, "
+            f"const double* SDV, const AFN& AF, const int* SI, const int* PLO, const double* PT, "
+            f"{di_params}int period, double age, T& Q) {{"
+        )
+        ap("  (void)PLO; (void)PT;")
+        for s_ in sa_body("T", "E", -1, sim=True):
+            ap("  " + s_)
+        ap("  return true;\n}")
 
         # ----------------------------------------------------------------
         # emitters for the hoisted phases (double precision)
@@ -1038,7 +1073,268 @@ class RegimeKernels:
         ap("    }")
         ap("  }")
         ap("}")
+        L += self._sim_kernel(locals())
         return "\n".join(L)
+
+    # ------------------------------------------------------------------ (d)
+    def _sim_layout(self) -> None:
+        spec = self.spec
+        w = self.n_words
+        self.SW_N, self.SW_RID_IN, self.SW_RID_OUT, self.SW_VAL, self.SW_AIDX = w, w + 1, w + 2, w + 3, w + 4
+        w += 5
+        self.SW_ACT = w
+        w += len(spec.actions)
+        self.SW_SIN = w
+        w += len(spec.states)
+        names: list[str] = []
+        if self.targets:
+            for t in self.targets:
+                for ax in t.spec.states:
+                    if ax.name not in names:
+                        names.append(ax.name)
+        else:
+            names = [ax.name for ax in spec.states]
+        self.sim_out_names = names
+        self.SW_SOUT = w
+        w += len(names)
+        self.sim_words = w
+
+    def sim_name(self) -> str:
+        return f"lcm_sim_{self.tag}"
+
+    def _sim_kernel(self, env: dict) -> list[str]:
+        """Kernel (d): one simulated period of this regime for every subject in it.
+
+        One warp per subject: the 32 lanes stride over the actions (double
+        precision), the first lane records value and action and draws the next
+        regime and next states with the Philox stream of (seed, subject,
+        period, stream id).  Stream ids: 0 regime draw, 1 + k the k-th state of
+        the drawn target, 64 + d the taste shock of discrete choice d.
+        """
+        from pylcm_b200.spec import proc_field_name, proc_grid_name
+
+        self._sim_layout()
+        spec = self.spec
+        tag = self.tag
+        bP, bD, bS, bSD = env["bP"], env["bD"], env["bS"], env["bSD"]
+        nf, nP, nD, nS, nSD = env["nf"], env["nP"], env["nD"], env["nS"], env["nSD"]
+        dstates, dacts = env["dstates"], env["dacts"]
+        ND, taste = env["ND"], env["taste"]
+        pv, decode_disc = env["pv"], env["decode_disc"]
+        eP, pvals = env["eP"], env["pvals"]
+        d_lines, d_vals = env["d_lines"], env["d_vals"]
+        proc_names = env["proc_names"]
+        NDS = max(len(dstates), 1)
+        NPROC = max(len(proc_names), 1)
+        L: list[str] = []
+        ap = L.append
+
+        def sim_prov(kind: str) -> dict:
+            prov = pv()
+            for i, n in enumerate(bP):
+                prov[id(n)] = f"PVd[{i}]" if n.dtype == "f" else _cast(f"PVd[{i}]", n.dtype, "double")
+            for a in spec.states:
+                if a.kind == "continuous":
+                    prov[id(ir.var("state", a.name, "f"))] = f"sv_{a.name}"
+                else:
+                    prov[id(ir.var("state", a.name, "i"))] = f"si_{a.name}"
+                if a.kind == "process":
+                    node = ir.Expr("pidx", (proc_grid_name(a.name), ir.var("state", a.name, "i")), "f")
+                    prov[id(node)] = f"pv_{a.name}"
+            for a in dacts:
+                prov[id(ir.var("action", a.name, "i"))] = f"DI_{a.name}"
+            if kind == "SD":
+                for i, n in enumerate(bD):
+                    prov[id(n)] = f"DV[{i}]" if n.dtype == "f" else _cast(f"DV[{i}]", n.dtype, "double")
+                for i, n in enumerate(bS):
+                    prov[id(n)] = f"SV[{i}]" if n.dtype == "f" else _cast(f"SV[{i}]", n.dtype, "double")
+            return prov
+
+        eS = Emitter("double", self.param_off, sim_prov("S"), "s")
+        s_vals = [eS.emit(n) for n in bS]
+        eSD = Emitter("double", self.param_off, sim_prov("SD"), "x")
+        sdv = [eSD.emit(n) for n in bSD]
+
+        ap(f"struct AFG_{tag} {{ const double* atf; const int* ati; int n; int a;")
+        ap("  __device__ __forceinline__ double F(int f) const { return __ldg(atf + (i64)f * n + a); }")
+        ap("  __device__ __forceinline__ int I(int f) const { return __ldg(ati + (i64)f * n + a); } };")
+        ap(
+            f'extern "C" __global__ void __launch_bounds__(256) {self.sim_name()}('
+            "const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles, u64 seed) {"
+        )
+        ap("  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {")
+        ap("    const int item = lcm_find_item(tile_prefix, n_items, tile);")
+        ap(f"    const i64* __restrict__ it = items + (i64)item * {self.sim_words};")
+        ap("    const int s = (tile - tile_prefix[item]) * 8 + (int)threadIdx.x / 32;")
+        ap("    const int lane = (int)threadIdx.x % 32;")
+        ap(f"    if (s >= lcm_wi(it, {self.SW_N})) continue;")
+        ap(f"    const int* rid_in = lcm_wp<const int>(it, {self.SW_RID_IN});")
+        ap(f"    if (rid_in[s] != {spec.rid}) continue;  // warp-uniform: one subject per warp")
+        ap(f"    Ctx_{tag}<double, double> C; C.load(it);")
+        ap(f"    const double* __restrict__ PV = lcm_wp<const double>(it, {self.W_P});")
+        ap(f"    const int period = lcm_wi(it, {self.W_PERIOD});")
+        ap(f"    const double age = lcm_wd(it, {self.W_AGE});")
+        ap(f"    const int n_actions = lcm_wi(it, {self.W_NACT});")
+        ap(f"    const int n_ac = n_actions / {ND};")
+        ap(f"    const double* __restrict__ atf = lcm_wp<const double>(it, {self.W_ATAB});")
+        ap(f"    const int* __restrict__ ati = reinterpret_cast<const int*>(atf + (i64){nf} * n_actions);")
+        ap("    (void)period; (void)age; (void)ati; (void)PV;")
+        ap("    LcmRng rng; rng.k0 = (u32)seed; rng.k1 = (u32)(seed >> 32); rng.subject = (u32)s; rng.period = (u32)period;")
+        for s_ in eP.lines:
+            ap("    " + s_)
+        ap(f"    double PVd[{nP}]; PVd[0] = 0.0;")
+        for i, v in enumerate(pvals):
+            ap(f"    PVd[{i}] = (double)({v});")
+        ap(f"    int SI[{NDS}]; int PLO[{NPROC}]; double PT[{NPROC}]; SI[0] = 0; PLO[0] = 0; PT[0] = 0.0;")
+        for k, a in enumerate(spec.states):
+            ap(f"    const double x_{a.name} = lcm_wp<const double>(it, {self.SW_SIN + k})[s];")
+            if a.kind == "continuous":
+                ap(f"    const double sv_{a.name} = x_{a.name};")
+            elif a.kind == "discrete":
+                ap(f"    const int si_{a.name} = (int)x_{a.name};")
+            else:
+                off, shape = self.param_off[proc_grid_name(a.name)]
+                pi = proc_names.index(a.name)
+                ap(f"    const double pv_{a.name} = x_{a.name};")
+                ap(f"    const double pc_{a.name} = lcm_coord_irreg<double>(pv_{a.name}, PV + {off}, {shape[0]});")
+                ap(f"    double pf_{a.name}; PLO[{pi}] = lcm_lower(pc_{a.name}, {shape[0]}, pf_{a.name}); PT[{pi}] = pc_{a.name} - pf_{a.name};")
+                ap(f"    const int si_{a.name} = PLO[{pi}];")
+        for i, a in enumerate(dstates):
+            ap(f"    SI[{i}] = si_{a.name};")
+        for s_ in eS.lines:
+            ap("    " + s_)
+        ap(f"    double SV[{nS}]; SV[0] = 0.0;")
+        for i, v in enumerate(s_vals):
+            ap(f"    SV[{i}] = (double)({v});")
+        if taste:
+            ap(f"    LcmBest<double> bd[{ND}];")
+            ap(f"    #pragma unroll\n    for (int d = 0; d < {ND}; ++d) bd[d].init();")
+        else:
+            ap("    LcmBest<double> best; best.init();")
+        ap(f"    #pragma unroll\n    for (int ad = 0; ad < {ND}; ++ad) {{")
+        dl: list[str] = []
+        decode_disc(dl, "ad")
+        for s_ in dl + d_lines:
+            ap("      " + s_)
+        ap(f"      double DV[{nD}]; DV[0] = 0.0;")
+        for i, v in enumerate(d_vals):
+            ap(f"      DV[{i}] = (double)({v});")
+        for s_ in eSD.lines:
+            ap("      " + s_)
+        ap(f"      double SDV[{nSD}]; SDV[0] = 0.0;")
+        for i, v in enumerate(sdv):
+            ap(f"      SDV[{i}] = (double)({v});")
+        di_args = "".join(f"DI_{a.name}, " for a in dacts)
+        push = "bd[ad].push(q, aidx);" if taste else "best.push(q, aidx);"
+        ap("      for (int j = lane; j < n_ac; j += 32) {")
+        ap("        const int aidx = ad * n_ac + j;")
+        ap(f"        AFG_{tag} af{{atf, ati, n_actions, aidx}};")
+        ap("        double q;")
+        ap(f"        if (lcm_simsa_{tag}<double, double>(C, PV, PVd, DV, SV, SDV, af, SI, PLO, PT, {di_args}period, age, q)) {push}")
+        ap("      }")
+        ap("    }")
+        if taste:
+            ap(f"    #pragma unroll\n    for (int d = 0; d < {ND}; ++d) lcm_group_reduce<32, double>(bd[d]);")
+        else:
+            ap("    lcm_group_reduce<32, double>(best);")
+        ap("    if (lane != 0) continue;")
+        if taste:
+            ap(f"    const double scale = lcm_wd(it, {self.W_TASTE});")
+            ap("    int dstar = -1; double bn = -lcm_lim<double>::inf(); double vstar = -lcm_lim<double>::inf();")
+            ap(f"    for (int d = 0; d < {ND}; ++d) {{")
+            ap("      if (bd[d].idx < 0) continue;")
+            ap("      const double noisy = bd[d].v + scale * (rng.gumbel(64u + (u32)d) - 0.5772156649015329);")
+            ap("      if (dstar < 0 || noisy > bn) { bn = noisy; dstar = d; vstar = bd[d].v; }")
+            ap("    }")
+            ap("    int aa = 0;")
+            ap(f"    for (int d = 0; d < {ND}; ++d) if (d == dstar) aa = bd[d].idx;")
+            ap("    const double value = dstar < 0 ? -lcm_lim<double>::inf() : vstar;")
+        else:
+            ap("    const int aa = best.idx < 0 ? 0 : best.idx;")
+            ap("    const double value = best.nan ? lcm_lim<double>::nan() : (best.idx < 0 ? -lcm_lim<double>::inf() : best.v);")
+        ap(f"    lcm_wp<double>(it, {self.SW_VAL})[s] = value;")
+        ap(f"    lcm_wp<int>(it, {self.SW_AIDX})[s] = aa;")
+        ap("    int arem = aa;")
+        prov = sim_prov("S")
+        for k in range(len(spec.actions) - 1, -1, -1):
+            ax = spec.actions[k]
+            ap(f"    const int ai_{ax.name} = arem % lcm_wi(it, {self.W_ASIZE + k}); arem /= lcm_wi(it, {self.W_ASIZE + k});")
+        for k, ax in enumerate(spec.actions):
+            if ax.kind == "continuous":
+                ap(f"    const double av_{ax.name} = lcm_wp<const double>(it, {self.W_AGRID + k})[ai_{ax.name}];")
+                prov[id(ir.var("action", ax.name, "f"))] = f"av_{ax.name}"
+                ap(f"    lcm_wp<double>(it, {self.SW_ACT + k})[s] = av_{ax.name};")
+            else:
+                prov[id(ir.var("action", ax.name, "i"))] = f"ai_{ax.name}"
+                ap(f"    lcm_wp<double>(it, {self.SW_ACT + k})[s] = (double)ai_{ax.name};")
+        e = Emitter("double", self.param_off, prov, "n")
+        out_idx = {name: self.SW_SOUT + i for i, name in enumerate(self.sim_out_names)}
+        rid_out = f"lcm_wp<int>(it, {self.SW_RID_OUT})[s]"
+        if spec.terminal:
+            ap(f"    {rid_out} = {spec.rid};")
+            for a in spec.states:
+                ap(f"    lcm_wp<double>(it, {out_idx[a.name]})[s] = x_{a.name};")
+        else:
+            tr = self.tr
+            if tr.regime_id is not None:
+                r_expr = e.emit(tr.regime_id)
+                for s_ in e.lines:
+                    ap("    " + s_)
+                e.lines = []
+                ap(f"    const int rid = (int)({r_expr});")
+            else:
+                probs = [e.emit(p) for p in tr.regime_probs]
+                for s_ in e.lines:
+                    ap("    " + s_)
+                e.lines = []
+                ap(f"    double rp[{len(probs)}];")
+                for i, p_ in enumerate(probs):
+                    ap(f"    rp[{i}] = (double)({p_});")
+                ap(f"    const int rid = lcm_categorical<{len(probs)}>(rp, rng.uniform(0u));")
+            ap(f"    {rid_out} = rid;")
+            for t in self.targets:
+                ap(f"    if (rid == {t.spec.rid}) {{")
+                # scoped emitter: expressions bound inside this branch stay in it
+                et = Emitter("double", self.param_off, dict(e.vals), f"n{t.spec.rid}_")
+                for k, ax in enumerate(t.spec.states):
+                    law = t.laws[ax.name]
+                    dst = f"lcm_wp<double>(it, {out_idx[ax.name]})[s]"
+                    stream = f"{1 + k}u"
+                    if law.kind in ("cont", "det"):
+                        v = et.emit(law.expr)
+                        for s_ in et.lines:
+                            ap("      " + s_)
+                        et.lines = []
+                        ap(f"      {dst} = (double)({v});")
+                    elif law.kind == "markov":
+                        vs = [et.emit(x) for x in law.expr.items]
+                        for s_ in et.lines:
+                            ap("      " + s_)
+                        et.lines = []
+                        ap(f"      {{ double mp[{len(vs)}];")
+                        for i, v in enumerate(vs):
+                            ap(f"        mp[{i}] = (double)({v});")
+                        ap(f"        {dst} = (double)lcm_categorical<{len(vs)}>(mp, rng.uniform({stream})); }}")
+                    else:  # process: draw from the source process's law
+                        src = law.source_process
+                        grid = spec.state(src).grid
+                        fld = lambda f, src=src: f"PV[{self.param_off[proc_field_name(src, f)][0]}]"  # noqa: E731
+                        cls = type(grid).__name__
+                        if cls in ("TauchenAR1Process", "RouwenhorstAR1Process"):
+                            ap(f"      {dst} = {fld('mu')} + {fld('rho')} * pv_{src} + {fld('sigma')} * rng.normal({stream});")
+                        elif cls == "NormalIIDProcess":
+                            ap(f"      {dst} = {fld('mu')} + {fld('sigma')} * rng.normal({stream});")
+                        elif cls == "LogNormalIIDProcess":
+                            ap(f"      {dst} = exp({fld('mu')} + {fld('sigma')} * rng.normal({stream}));")
+                        elif cls == "UniformIIDProcess":
+                            ap(f"      {dst} = {fld('start')} + ({fld('stop')} - {fld('start')}) * rng.uniform({stream});")
+                        else:
+                            raise TracingError(f"no simulation draw for process {cls}")
+                ap("    }")
+        ap("  }")
+        ap("}")
+        return L
+
 
     # ------------------------------------------------------------------ (b)
     def _expect_source(self, t: TargetPlan) -> str:

@@ -116,8 +116,8 @@ __device__ __forceinline__ T lcm_interp1(const S* __restrict__ row, int n, T c) 
   int lo = lcm_lower(c, n, lof);
   T wu = c - lof;
   T wl = T(1) - wu;
-  T v0 = (T)row[lo];
-  T v1 = (T)row[lo + 1];
+  T v0 = (T)__ldg(row + lo);
+  T v1 = (T)__ldg(row + lo + 1);
   // a finite result implies finite corners; otherwise redo it zero-safely
   T r = wl * v0 + wu * v1;
   if (lcm_isfinite(r)) return r;
@@ -134,7 +134,7 @@ __device__ __forceinline__ T lcm_interp2(const S* __restrict__ blk, int n0, int 
   T d0 = T(1) - u0, d1 = T(1) - u1;
   const S* r0 = blk + (i64)l0 * n1;
   const S* r1 = r0 + n1;
-  const T a = (T)r0[l1], b = (T)r0[l1 + 1], c = (T)r1[l1], d = (T)r1[l1 + 1];
+  const T a = (T)__ldg(r0 + l1), b = (T)__ldg(r0 + l1 + 1), c = (T)__ldg(r1 + l1), d = (T)__ldg(r1 + l1 + 1);
   T r = d0 * d1 * a + d0 * u1 * b + u0 * d1 * c + u0 * u1 * d;
   if (lcm_isfinite(r)) return r;
   T acc = lcm_zs(d0 * d1, a);
@@ -251,4 +251,60 @@ __device__ __forceinline__ T lcm_logsum(const T* vals, T scale) {
 #pragma unroll
   for (int d = 0; d < ND; ++d) s += exp(sh[d] - m);
   return fin + scale * (log(s) + m);
+}
+
+// ---------------------------------------------------------------------------
+// Counter-based RNG: Philox-4x32 with 10 rounds (Salmon, Moraes, Dror & Shaw,
+// "Parallel random numbers: as easy as 1, 2, 3", SC 2011).  A draw is a pure
+// function of (counter, key): the simulation uses counter = (subject, period,
+// stream, 0) and key = the 64-bit seed, so results do not depend on launch
+// shape or on which thread draws.
+struct LcmU4 { u32 x, y, z, w; };
+
+__device__ __forceinline__ LcmU4 lcm_philox4x32(u32 c0, u32 c1, u32 c2, u32 c3, u32 k0, u32 k1) {
+  const u32 M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const u32 W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    if (r > 0) { k0 += W0; k1 += W1; }
+    const u32 hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
+    const u32 hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+    const u32 n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  LcmU4 o; o.x = c0; o.y = c1; o.z = c2; o.w = c3;
+  return o;
+}
+
+// uniform double in (0, 1) from 53 random bits
+__device__ __forceinline__ double lcm_u53(u32 a, u32 b) {
+  const u64 m = ((u64)(a >> 5) << 26) | (u64)(b >> 6);
+  return ((double)m + 0.5) * 1.1102230246251565404e-16;  // 2^-53
+}
+
+struct LcmRng {
+  u32 k0, k1, subject, period;
+  __device__ __forceinline__ LcmU4 raw(u32 stream) const { return lcm_philox4x32(subject, period, stream, 0u, k0, k1); }
+  __device__ __forceinline__ double uniform(u32 stream) const { LcmU4 r = raw(stream); return lcm_u53(r.x, r.y); }
+  // standard normal by Box-Muller on two uniforms of the same counter
+  __device__ __forceinline__ double normal(u32 stream) const {
+    LcmU4 r = raw(stream);
+    const double u1 = lcm_u53(r.x, r.y), u2 = lcm_u53(r.z, r.w);
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
+  // standard Gumbel: -log(-log(u))
+  __device__ __forceinline__ double gumbel(u32 stream) const { return -log(-log(uniform(stream))); }
+};
+
+// categorical draw: first index whose cumulative weight exceeds u * total
+template <int N>
+__device__ __forceinline__ int lcm_categorical(const double* p, double u) {
+  double tot = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) tot += p[i];
+  const double thr = u * tot;
+  double acc = 0.0;
+  int pick = N - 1;
+  for (int i = 0; i < N; ++i) { acc += p[i]; if (thr < acc) { pick = i; break; } }
+  return pick;
 }

@@ -218,6 +218,9 @@ class SolvePlan:
         words: list[np.ndarray] = []
         prefixes: list[np.ndarray] = []
         self.launches: list[Launch] = []
+        # host copies of the Bellman item records per (period, regime), reused
+        # by the simulation (same layout, extended with simulation words)
+        self.records: dict[tuple, tuple] = {}
         w_off = 0
         p_off = 0
 
@@ -323,6 +326,7 @@ class SolvePlan:
                 recs.append(r)
             spt = rk.cfg.states_per_tile
             tiles = [math.ceil(s.n_states / spt)] * n
+            self.records[(period, s.name)] = (rk, np.stack(recs).astype(np.int64))
             add_launch("atab", rk, rk.atab_name(), recs, [math.ceil(s.n_actions / 256)] * n, 256, 0, period)
             # kernel (a) reads the same records
             self.launches.append(
@@ -343,22 +347,36 @@ class SolvePlan:
         for rk in {id(l.module): l.module for l in self.launches}.values():
             eng.module(rk)
         self.graph = None
+        self._prepared = None
 
     # ---------------------------------------------------------------- run
-    def run(self, stream: int | None = None) -> None:
-        torch = self.torch
-        if stream is None:
-            stream = torch.cuda.current_stream(self.dev).cuda_stream
+    def _prepare(self) -> list:
         ib = self.items.data_ptr()
         pb = self.prefix.data_ptr()
-        for l in self.launches:
-            mod = l.module.module
-            ip = ib + 8 * l.item_off
-            pp = pb + 4 * l.prefix_off
-            if l.kind == "expect":
-                mod.expectation(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
-            else:
-                mod.bellman_step(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream)
+        return [
+            l.module.module.prepared(
+                l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem
+            )
+            for l in self.launches
+        ]
+
+    def run(self, stream: int | None = None) -> None:
+        """Issue every launch of the plan (all periods) on `stream`."""
+        if stream is None:
+            stream = self.torch.cuda.current_stream(self.dev).cuda_stream
+        if self._prepared is None:
+            self._prepared = self._prepare()
+        for launch in self._prepared:
+            launch(stream)
+
+    def run_period_inputs(self, period: int, stream: int) -> None:
+        """Re-issue the expectation and action-table launches of one period
+        (the simulation reads EV and the action table of that period)."""
+        if self._prepared is None:
+            self._prepared = self._prepare()
+        for l, launch in zip(self.launches, self._prepared):
+            if l.period == period and l.kind in ("expect", "atab"):
+                launch(stream)
 
     def capture(self) -> None:
         """Capture the launch list in a CUDA graph (replayed by run_graph)."""

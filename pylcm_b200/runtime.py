@@ -129,6 +129,28 @@ class Module:
         self.h = h
         self.key = key
 
+    def prepared(self, kind: str, kernel: str, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid=0):
+        """A launch with its ctypes arguments built once (cheap to replay)."""
+        fn = {
+            "bellman": self.ctx.lib.lcmx_bellman_step,
+            "atab": self.ctx.lib.lcmx_bellman_step,
+            "expect": self.ctx.lib.lcmx_expectation,
+            "egm": self.ctx.lib.lcmx_egm_step,
+        }[kind]
+        args = LaunchArgs(items_ptr, prefix_ptr, n_items, n_tiles, grid, block, smem)
+        name = kernel.encode()
+        h = self.h
+        ref = ctypes.byref(args)
+        ctx = self.ctx
+
+        def launch(stream):
+            rc = fn(h, name, ref, stream)
+            if rc:
+                ctx.check(rc)
+
+        launch.keepalive = (args, name)
+        return launch
+
     def occupancy(self, kernel: str, block: int, smem: int) -> int:
         n = ctypes.c_int()
         self.ctx.check(self.ctx.lib.lcmx_occupancy(self.h, kernel.encode(), block, smem, ctypes.byref(n)))

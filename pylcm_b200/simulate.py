@@ -1,0 +1,218 @@
+"""Forward simulation on the GPU (kernel (d)).
+
+Restates the reference's simulation loop (``src/_lcm/simulation/simulate.py:74-668``):
+for each period, for each regime active in it, every subject currently in
+that regime takes the argmax of Q at its own (off-grid) state -- the same
+Q evaluation as the solve, reading next period's value function -- and then
+draws its next regime and next states.
+
+Draws use a counter-based Philox-4x32-10 stream keyed by the seed and
+indexed by (subject, period, stream id), so a subject's path does not depend
+on the batch it is simulated in.  The reference draws with JAX's threefry
+keys, so paths with stochastic draws agree with it in distribution, not
+bitwise; paths without draws agree exactly.
+"""
+
+from __future__ import annotations
+
+import math
+from typing import Any, Mapping
+
+import numpy as np
+
+from pylcm_b200.exceptions import InvalidParamsError
+from pylcm_b200.grids import DiscreteGrid
+
+
+class SimulationResult:
+    """Raw simulated arrays plus ``to_dataframe()`` (``src/lcm/result.py``)."""
+
+    def __init__(self, model, periods: dict) -> None:
+        self.model = model
+        self.periods = periods  # period -> dict of arrays
+
+    @property
+    def n_subjects(self) -> int:
+        return len(next(iter(self.periods.values()))["regime_id"])
+
+    def to_dataframe(self, terminal_rows: str = "all"):
+        import pandas as pd
+
+        specs = self.model.regime_specs
+        by_id = {s.rid: s for s in specs}
+        state_names = sorted({a.name for s in specs for a in s.states})
+        action_names = sorted({a.name for s in specs for a in s.actions})
+        grids = {}
+        for s in specs:
+            for a in s.states + s.actions:
+                grids.setdefault(a.name, a.grid)
+        cols: dict[str, list] = {k: [] for k in ["subject_id", "period", "regime_name", "value", *state_names, *action_names, "age"]}
+        ages = self.model.ages.values
+        for p in sorted(self.periods):
+            d = self.periods[p]
+            rid = d["regime_id"]
+            for i in range(len(rid)):
+                r = int(rid[i])
+                if r < 0:
+                    continue
+                spec = by_id[r]
+                if spec.terminal and terminal_rows == "none":
+                    continue
+                cols["subject_id"].append(i)
+                cols["period"].append(p)
+                cols["regime_name"].append(spec.name)
+                cols["value"].append(float(d["value"][i]))
+                own_s = {a.name for a in spec.states}
+                own_a = {a.name for a in spec.actions}
+                for n in state_names:
+                    cols[n].append(float(d["states"][n][i]) if n in own_s else np.nan)
+                for n in action_names:
+                    cols[n].append(float(d["actions"][n][i]) if n in own_a else np.nan)
+                cols["age"].append(float(ages[p]))
+        df = pd.DataFrame(cols)
+        df["regime_name"] = pd.Categorical(df["regime_name"], categories=[s.name for s in specs])
+        for n in state_names + action_names:
+            g = grids[n]
+            if isinstance(g, DiscreteGrid):
+                codes = df[n].to_numpy()
+                labels = np.array([g.categories[int(c)] if np.isfinite(c) else None for c in codes], dtype=object)
+                df[n] = pd.Categorical(labels, categories=list(g.categories))
+        return df
+
+
+def _initial_arrays(model, initial_conditions: Mapping) -> tuple[np.ndarray, dict]:
+    ic = dict(initial_conditions)
+    rid = ic.pop("regime_id", ic.pop("regime", None))
+    if rid is None:
+        raise InvalidParamsError("initial_conditions needs 'regime_id'")
+    rid = np.asarray(rid).astype(np.int64)
+    n = rid.shape[0]
+    if "age" in ic:
+        ages = np.asarray(ic.pop("age"), dtype=np.float64)
+        if not np.all(ages == model.ages.values[0]):
+            raise InvalidParamsError("all subjects must start at the first age of the age grid")
+    states = {}
+    for k, v in ic.items():
+        a = np.asarray(v, dtype=np.float64)
+        if a.shape != (n,):
+            raise InvalidParamsError(f"initial condition {k!r} must have shape ({n},)")
+        states[k] = a
+    return rid, states
+
+
+class SimPlan:
+    """Device buffers and launches of one simulation (one solve instance)."""
+
+    def __init__(self, solve_plan, initial_conditions: Mapping, seed: int) -> None:
+        import torch
+
+        self.torch = torch
+        self.plan = solve_plan
+        eng = solve_plan.eng
+        model = eng.model
+        specs = eng.specs
+        T = model.n_periods
+        dev = solve_plan.dev
+        rid0, states0 = _initial_arrays(model, initial_conditions)
+        N = rid0.shape[0]
+        self.N, self.T, self.seed = N, T, int(seed) & 0xFFFFFFFFFFFFFFFF
+        names = sorted({a.name for s in specs for a in s.states})
+        anames = sorted({a.name for s in specs for a in s.actions})
+        for s in specs:
+            for a in s.states:
+                if a.name not in states0 and (rid0 == s.rid).any():
+                    raise InvalidParamsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
+        nan = float("nan")
+        self.S = {n: torch.full((T + 1, N), nan, dtype=torch.float64, device=dev) for n in names}
+        for n, v in states0.items():
+            if n in self.S:
+                self.S[n][0] = torch.as_tensor(v, device=dev)
+        self.R = torch.full((T + 1, N), -1, dtype=torch.int32, device=dev)
+        self.R[0] = torch.as_tensor(rid0, dtype=torch.int32, device=dev)
+        self.val = torch.full((T, N), nan, dtype=torch.float64, device=dev)
+        self.aidx = torch.zeros((T, N), dtype=torch.int32, device=dev)
+        self.A = {n: torch.full((T, N), nan, dtype=torch.float64, device=dev) for n in anames}
+        # item records: the Bellman record of (period, regime) + simulation words
+        recs = []
+        self.launches = []
+        off = 0
+        for period in range(T):
+            for s in specs:
+                if period not in s.active_periods:
+                    continue
+                rk, base = solve_plan.records[(period, s.name)]
+                eng.module(rk)
+                r = np.zeros(rk.sim_words, dtype=np.int64)
+                r[: rk.n_words] = base[0]
+                r[rk.SW_N] = N
+                r[rk.SW_RID_IN] = self.R[period].data_ptr()
+                r[rk.SW_RID_OUT] = self.R[period + 1].data_ptr()
+                r[rk.SW_VAL] = self.val[period].data_ptr()
+                r[rk.SW_AIDX] = self.aidx[period].data_ptr()
+                for k, a in enumerate(s.actions):
+                    r[rk.SW_ACT + k] = self.A[a.name][period].data_ptr()
+                for k, a in enumerate(s.states):
+                    r[rk.SW_SIN + k] = self.S[a.name][period].data_ptr()
+                for k, name in enumerate(rk.sim_out_names):
+                    r[rk.SW_SOUT + k] = self.S[name][period + 1].data_ptr()
+                recs.append(r)
+                self.launches.append((period, rk, off, math.ceil(N / 8)))
+                off += r.size
+        self.items = torch.as_tensor(np.concatenate(recs), dtype=torch.int64, device=dev)
+        pref = []
+        for _, _, _, tiles in self.launches:
+            pref.append(np.array([0, tiles, 0, 0], dtype=np.int32))
+        self.prefix = torch.as_tensor(np.concatenate(pref), dtype=torch.int32, device=dev)
+
+    def run(self, stream: int | None = None) -> None:
+        torch = self.torch
+        if stream is None:
+            stream = torch.cuda.current_stream(self.plan.dev).cuda_stream
+        ib, pb = self.items.data_ptr(), self.prefix.data_ptr()
+        done_inputs = set()
+        for k, (period, rk, off, tiles) in enumerate(self.launches):
+            if period not in done_inputs:
+                self.plan.run_period_inputs(period, stream)
+                done_inputs.add(period)
+            rk.module.simulate(rk.sim_name(), ib + 8 * off, pb + 16 * k, 1, tiles, 256, 0, self.seed, stream)
+
+    @property
+    def gpu_launches(self) -> int:
+        return len(self.launches)
+
+    def result(self, model) -> SimulationResult:
+        torch = self.torch
+        torch.cuda.current_stream(self.plan.dev).synchronize()
+        periods = {}
+        R = self.R.cpu().numpy()
+        V = self.val.cpu().numpy()
+        S = {n: v.cpu().numpy() for n, v in self.S.items()}
+        A = {n: v.cpu().numpy() for n, v in self.A.items()}
+        for p in range(self.T):
+            periods[p] = {
+                "regime_id": R[p],
+                "value": V[p],
+                "states": {n: S[n][p] for n in S},
+                "actions": {n: A[n][p] for n in A},
+            }
+        return SimulationResult(model, periods)
+
+
+def simulate(model, *, params, initial_conditions, V_arr=None, seed: int = 0, precision: str = "fp64",
+             log_level: str = "progress") -> SimulationResult:
+    """Solve (unless `V_arr` is given) and simulate `initial_conditions`."""
+    import torch
+
+    eng = model.engine(precision)
+    plan = eng.plan([params])
+    if V_arr is None:
+        plan.run()
+    else:
+        for p, regs in V_arr.items():
+            for r, v in regs.items():
+                k = plan.slot[r].get(int(p))
+                if k is not None:
+                    plan.V[r][0, k].copy_(torch.as_tensor(np.asarray(v, dtype=np.float64).reshape(-1)))
+    sim = SimPlan(plan, initial_conditions, seed)
+    sim.run()
+    return sim.result(model)

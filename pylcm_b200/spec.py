@@ -302,6 +302,10 @@ class TracedRegime:
                 if not ok:
                     raise InvalidParamsError(f"regime {self.spec.name!r}: missing parameter {src[2]!r} of {src[1]!r}")
                 v = np.asarray(val, dtype=np.float64)
+            elif src[0] == "proc_field":
+                ax = self.spec.state(src[1])
+                pp = resolver.process_params(self.spec.name, src[1], ax.grid)
+                v = np.asarray(float(pp[src[2]]), dtype=np.float64)
             else:
                 state = src[1]
                 if state not in proc_cache:
@@ -335,6 +339,10 @@ def proc_grid_name(state: str) -> str:
 
 def proc_P_name(state: str) -> str:
     return f"__proc__{state}__P"
+
+
+def proc_field_name(state: str, field: str) -> str:
+    return f"__proc__{state}__{field}"
 
 
 class _Tracer:
@@ -480,6 +488,9 @@ def trace_regime(
             process_tables[ax.name] = (nodes, P)
             t.add_param(proc_grid_name(ax.name), nodes, ("proc_nodes", ax.name))
             t.add_param(proc_P_name(ax.name), P, ("proc_P", ax.name))
+            # the process's own parameters (used by the simulation's draws)
+            for field in sorted(pp):
+                t.add_param(proc_field_name(ax.name, field), float(pp[field]), ("proc_field", ax.name, field))
     beta = None
     taste_scale = None
     regime_probs = None
