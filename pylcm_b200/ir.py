@@ -603,3 +603,97 @@ def _erf(x):
 
 
 _NP_UNARY["erf"] = _erf
+
+
+def diff(expr: Any, wrt: Expr) -> Expr:
+    """Symbolic derivative of a scalar expression with respect to a variable.
+
+    Used where the reference differentiates with ``jax.grad``: the marginal
+    utility u'(c) of the EGM carry rows and the savings derivative dR'/dA of
+    the law of motion.  Non-differentiable pieces (comparisons, floor, integer
+    arithmetic) have derivative zero; ``where`` differentiates its branches.
+    """
+    memo: dict[int, Expr] = {}
+    zero, one = const(0.0), const(1.0)
+
+    def d(e: Expr) -> Expr:
+        if id(e) in memo:
+            return memo[id(e)]
+        r = _d(e)
+        memo[id(e)] = r
+        return r
+
+    def _d(e: Expr) -> Expr:
+        if e is wrt:
+            return one
+        if e.dtype != _FLOAT or e.op in ("const", "param", "pidx", "var", "pgrid"):
+            return zero
+        if not any(x is wrt or (isinstance(x, Expr) and wrt in _leaves(x)) for x in e.args if isinstance(x, Expr)):
+            return zero
+        if e.op == "bin":
+            o, a, b = e.args
+            da, db = d(a), d(b)
+            if o == "+":
+                return da + db
+            if o == "-":
+                return da - db
+            if o == "*":
+                return da * b + a * db
+            if o == "/":
+                return (da * b - a * db) / (b * b)
+            if o == "pow":
+                # a**b: b * a**(b-1) * da + log(a) * a**b * db
+                out = zero
+                if not (isinstance(db, Expr) and db.op == "const" and db.args[0] == 0.0):
+                    out = out + un("log", a) * e * db
+                if not (isinstance(da, Expr) and da.op == "const" and da.args[0] == 0.0):
+                    out = out + b * _bin("pow", a, b - 1.0) * da
+                return out
+            if o == "min":
+                return where(_cmp("<=", a, b), da, db)
+            if o == "max":
+                return where(_cmp(">=", a, b), da, db)
+            return zero
+        if e.op == "un":
+            f, a = e.args
+            da = d(a)
+            table = {
+                "neg": lambda: -da,
+                "log": lambda: da / a,
+                "log1p": lambda: da / (1.0 + a),
+                "exp": lambda: e * da,
+                "expm1": lambda: un("exp", a) * da,
+                "sqrt": lambda: da / (2.0 * e),
+                "abs": lambda: where(_cmp(">=", a, 0.0), da, -da),
+                "sin": lambda: un("cos", a) * da,
+                "cos": lambda: -un("sin", a) * da,
+                "tanh": lambda: (1.0 - e * e) * da,
+            }
+            if f in table:
+                return table[f]()
+            return zero
+        if e.op == "where":
+            c, a, b = e.args
+            return where(c, d(a), d(b))
+        if e.op == "cast":
+            return d(e.args[1]) if e.args[0] == _FLOAT else zero
+        return zero
+
+    return const(d(const(expr)))
+
+
+def _leaves(e: Expr) -> set:
+    out = getattr(e, "_leaf_cache", None)
+    if out is None:
+        out = {id(n) for n in topo_order([e])}
+    return _IdSet(out)
+
+
+class _IdSet:
+    __slots__ = ("ids",)
+
+    def __init__(self, ids: set) -> None:
+        self.ids = ids
+
+    def __contains__(self, x: Any) -> bool:
+        return id(x) in self.ids

@@ -346,9 +346,10 @@ def proc_field_name(state: str, field: str) -> str:
 
 
 class _Tracer:
-    def __init__(self, spec: RegimeSpec, resolver: ParamResolver) -> None:
+    def __init__(self, spec: RegimeSpec, resolver: ParamResolver, overrides: dict | None = None) -> None:
         self.spec = spec
         self.resolver = resolver
+        self.overrides = dict(overrides or {})
         self.cache: dict[str, Any] = {}
         self.active: list[str] = []
         self.param_values: dict[str, np.ndarray] = {}
@@ -382,6 +383,8 @@ class _Tracer:
         return ir.ParamArray(flat, arr.shape)
 
     def resolve_arg(self, func: str, arg: str, default: Any) -> Any:
+        if arg in self.overrides:
+            return self.overrides[arg]
         if arg in self.spec.functions:
             return self.trace(arg)
         if arg in self.env:

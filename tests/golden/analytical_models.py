@@ -103,3 +103,62 @@ CASES = {
 def model_and_params(case: str):
     kw = CASES[case]
     return get_model(kw["n_periods"]), get_params(**kw)
+
+
+# ---------------------------------------------------------------------------
+# the same model solved by DC-EGM with the FUES envelope
+def _savings(wealth, consumption):
+    return wealth - consumption
+
+
+def _next_wealth_from_savings(savings, labor_income, interest_rate):
+    return (1 + interest_rate) * savings + labor_income
+
+
+def _inv_mu_log(marginal_continuation):
+    return 1.0 / marginal_continuation
+
+
+def get_dcegm_model(n_periods: int, n_savings: int = 200, n_constrained: int = 64) -> Model:
+    from pylcm_b200 import DCEGM, ConsumptionSavingsRegime, FUESEnvelope, IrregSpacedGrid, LiquidMargin
+
+    wealth = LinSpacedGrid(start=1, stop=400, n_points=100)
+    cons = LinSpacedGrid(start=1, stop=400, n_points=500)
+    ages = AgeGrid(start=40, stop=40 + (n_periods - 1) * 10, step="10Y")
+    last = ages.exact_values[-1]
+    sav = IrregSpacedGrid(points=tuple(400.0 * (i / (n_savings - 1)) ** 3 for i in range(n_savings)))
+    solver = DCEGM(savings_grid=sav, n_constrained_points=n_constrained, envelope=FUESEnvelope())
+    margin = LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings")
+    work = ConsumptionSavingsRegime(
+        actions={"labor_supply": DiscreteGrid(Labor), "consumption": cons},
+        states={"wealth": wealth},
+        state_transitions={"wealth": _next_wealth_from_savings},
+        transition=_nr_work,
+        functions={
+            "utility": _u_work,
+            "labor_income": _income,
+            "is_working": _is_working,
+            "savings": _savings,
+            "inverse_marginal_utility": _inv_mu_log,
+        },
+        solver=solver,
+        liquid=margin,
+        active=lambda age, la=last: age < la,
+    )
+    ret = ConsumptionSavingsRegime(
+        actions={"consumption": cons},
+        states={"wealth": wealth},
+        state_transitions={"wealth": _next_wealth_from_savings},
+        transition=_nr_ret,
+        functions={"utility": _u_ret, "savings": _savings, "inverse_marginal_utility": _inv_mu_log},
+        solver=solver,
+        liquid=margin,
+        active=lambda age, la=last: age < la,
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(regimes={"working_life": work, "retirement": ret, "dead": dead}, ages=ages, regime_id_class=Rid)
+
+
+def dcegm_model_and_params(case: str):
+    kw = CASES[case]
+    return get_dcegm_model(kw["n_periods"]), get_params(**kw)
