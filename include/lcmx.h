@@ -19,6 +19,8 @@
  *                           src/_lcm/simulation/simulate.py:465-668.
  *   lcmx_egm_step        <- the DC-EGM per-period core,
  *                           src/_lcm/egm/step_core.py:156-312.
+ *   lcmx_fues_scan       <- the FUES upper envelope of DC-EGM candidates,
+ *                           src/_lcm/egm/upper_envelope/fues.py:151-338.
  *   lcmx_count_nonfinite <- the per-period NaN/Inf diagnostics,
  *                           backward_induction.py:205-236.
  *
@@ -100,6 +102,19 @@ int lcmx_simulate(lcmx_module* mod, const char* kernel, const lcmx_launch_args* 
 /* Kernel (c), part 1: DC-EGM Euler inversion and candidate generation. */
 int lcmx_egm_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
                   void* stream);
+
+/* Kernel (c), part 2: FUES upper envelope of `n_rows` candidate rows of
+ * length n_in (row-major; any order within a row, NaN entries are absent
+ * candidates).  `savings` (may be NULL) is each candidate's exogenous savings
+ * source.  Outputs are (n_rows x n_out) NaN-padded refined rows in ascending
+ * grid order; n_kept[row] > n_out signals overflow (the row holds a valid
+ * prefix).  `workspace` must hold lcmx_fues_workspace_bytes(n_rows, n_in)
+ * bytes of device memory.  Rows of up to 8192 candidates. */
+size_t lcmx_fues_workspace_bytes(int n_rows, int n_in);
+int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
+                   const double* savings, int n_rows, int n_in, double jump_thresh,
+                   double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
+                   void* workspace, size_t workspace_bytes, void* stream);
 
 /* Count non-finite (and separately NaN) entries of a double array; the two
  * counters are accumulated into counts_dev[0] (nan) and counts_dev[1]

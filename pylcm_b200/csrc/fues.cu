@@ -1,0 +1,342 @@
+// fues.cu -- FUES upper envelope of DC-EGM candidate rows (kernel c, part 2).
+//
+// Restates the Fast Upper-Envelope Scan (Dobrescu & Shanker 2022) with the
+// reference's rules (src/_lcm/egm/upper_envelope/fues.py:151-1189):
+//   1. sort each row by (grid asc, value desc, policy desc), NaN grid last,
+//      ties by input position (a stable lexsort);
+//   2. reduce every run of equal grid values to its maximisers, keeping one
+//      copy per exogenous savings source;
+//   3. scan the sorted row keeping the last two envelope points (k, j); drop a
+//      candidate below j on the same segment, one with falling savings and a
+//      secant below the previous gradient, or one below the continuation of
+//      j's segment; insert segment crossings twice (left / right policy);
+//      "same segment" means |d(R - c)/dR| <= jump_thresh.
+//
+// GPU mapping: one CTA per row.  The CTA sorts an index array in shared
+// memory (bitonic), gathers the sorted row into the workspace, reduces the
+// coincident groups in parallel, and then warp 0 runs the scan: the scan
+// state is held redundantly by all 32 lanes, and each exhaustive look-ahead
+// for the next same-segment candidate inspects 32 candidates per step with
+// a warp ballot.  Lane 0 writes the emissions.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/lcmx.h"
+
+namespace {
+
+constexpr int kBlock = 256;
+constexpr int kMaxSort = 8192;  // largest row the shared-memory sort handles
+
+__device__ __forceinline__ bool isnan_(double x) { return x != x; }
+
+__device__ __forceinline__ double slope(double xa, double ya, double xb, double yb) {
+  const double dx = xb - xa;
+  return dx == 0.0 ? 0.0 : (yb - ya) / dx;
+}
+
+// different segments iff the implied savings (R - c) jump
+__device__ __forceinline__ bool policy_jump(double ga, double pa, double gb, double pb, double thr,
+                                            bool use_sav, double sa, double sb) {
+  const double ia = ga - pa, ib = gb - pb;
+  if (ga == gb) return use_sav ? (sa != sb) : (ia != ib);
+  return fabs(slope(ga, ia, gb, ib)) > thr;
+}
+
+__device__ __forceinline__ void intersect(double xa, double ya, double sa, double xb, double yb, double sb,
+                                          double& x, double& y) {
+  const double den = sa - sb;
+  if (den == 0.0) {
+    x = __longlong_as_double(0x7ff8000000000000LL);
+    y = ya;
+    return;
+  }
+  x = (yb - ya + sa * xa - sb * xb) / den;
+  y = ya + sa * (x - xa);
+}
+
+struct Key {
+  double g, v, p;
+  int i;
+};
+
+__device__ __forceinline__ Key load_key(const double* g, const double* v, const double* p, int i, int n) {
+  Key k;
+  k.i = i;
+  if (i >= n) {
+    k.g = __longlong_as_double(0x7ff0000000000000LL);  // padding sorts last
+    k.v = -k.g;
+    k.p = -k.g;
+    k.i = 0x7fffffff;
+    return k;
+  }
+  const double gi = g[i], vi = v[i], pi = p[i];
+  k.g = isnan_(gi) ? __longlong_as_double(0x7ff0000000000000LL) : gi;
+  k.v = isnan_(vi) ? -__longlong_as_double(0x7ff0000000000000LL) : vi;
+  k.p = isnan_(pi) ? -__longlong_as_double(0x7ff0000000000000LL) : pi;
+  return k;
+}
+
+// a before b ?
+__device__ __forceinline__ bool key_less(const Key& a, const Key& b) {
+  if (a.g != b.g) return a.g < b.g;
+  if (a.v != b.v) return a.v > b.v;
+  if (a.p != b.p) return a.p > b.p;
+  return a.i < b.i;
+}
+
+// first same-segment candidate from idx in direction dir (warp-cooperative)
+__device__ __forceinline__ bool find_same_segment(const double* g, const double* p, const double* v, int n,
+                                                  double ag, double ap, int idx, int dir, double thr,
+                                                  double& fg, double& fp, double& fv) {
+  const int lane = threadIdx.x & 31;
+  for (int base = idx + dir;; base += 32 * dir) {
+    if (dir > 0 ? base >= n : base < 0) break;
+    const int k = base + dir * lane;
+    bool ok = false;
+    double gk = 0.0, pk = 0.0, vk = 0.0;
+    if (k >= 0 && k < n) {
+      gk = g[k];
+      pk = p[k];
+      vk = v[k];
+      ok = !isnan_(gk) && !isnan_(vk) && !policy_jump(ag, ap, gk, pk, thr, false, 0.0, 0.0);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (m) {
+      const int src = __ffs(m) - 1;  // nearest candidate
+      fg = __shfl_sync(0xffffffffu, gk, src);
+      fp = __shfl_sync(0xffffffffu, pk, src);
+      fv = __shfl_sync(0xffffffffu, vk, src);
+      return true;
+    }
+  }
+  fg = fp = fv = __longlong_as_double(0x7ff8000000000000LL);
+  return false;
+}
+
+__global__ void __launch_bounds__(kBlock) fues_kernel(const double* __restrict__ grid, const double* __restrict__ policy,
+                                                      const double* __restrict__ value,
+                                                      const double* __restrict__ savings, int n_rows, int n_in,
+                                                      double thr, double* __restrict__ grid_out,
+                                                      double* __restrict__ policy_out, double* __restrict__ value_out,
+                                                      int n_out, int* __restrict__ n_kept, double* __restrict__ work) {
+  __shared__ int sidx[kMaxSort];
+  int np2 = 1;
+  while (np2 < n_in) np2 <<= 1;
+  const bool use_sav = savings != nullptr;
+  for (int row = blockIdx.x; row < n_rows; row += gridDim.x) {
+    const double* G = grid + (int64_t)row * n_in;
+    const double* P = policy + (int64_t)row * n_in;
+    const double* V = value + (int64_t)row * n_in;
+    const double* S = use_sav ? savings + (int64_t)row * n_in : nullptr;
+    double* g = work + (int64_t)row * 4 * n_in;
+    double* p = g + n_in;
+    double* v = p + n_in;
+    double* s = v + n_in;
+    // ---- 1. bitonic sort of indices by the lexsort key
+    __syncthreads();
+    for (int t = threadIdx.x; t < np2; t += kBlock) sidx[t] = t;
+    __syncthreads();
+    for (int size = 2; size <= np2; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = threadIdx.x; t < np2; t += kBlock) {
+          const int partner = t ^ stride;
+          if (partner > t) {
+            const bool ascending = (t & size) == 0;
+            const Key a = load_key(G, V, P, sidx[t], n_in);
+            const Key b = load_key(G, V, P, sidx[partner], n_in);
+            const bool swap = ascending ? key_less(b, a) : key_less(a, b);
+            if (swap) {
+              const int tmp = sidx[t];
+              sidx[t] = sidx[partner];
+              sidx[partner] = tmp;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int t = threadIdx.x; t < n_in; t += kBlock) {
+      const int i = sidx[t];
+      g[t] = G[i];
+      p[t] = P[i];
+      v[t] = V[i];
+      s[t] = use_sav ? S[i] : G[i] - P[i];
+    }
+    __syncthreads();
+    // ---- 2. coincident groups: keep the maximisers, one per savings source
+    for (int t = threadIdx.x; t < n_in; t += kBlock) {
+      const double gt = g[t];
+      bool keep = !isnan_(gt);
+      if (keep) {
+        int lo = t, hi = t;
+        while (lo > 0 && g[lo - 1] == gt) --lo;
+        while (hi + 1 < n_in && g[hi + 1] == gt) ++hi;
+        if (hi > lo) {
+          double vmax = -__longlong_as_double(0x7ff0000000000000LL);
+          for (int k = lo; k <= hi; ++k) {
+            const double vk = v[k];
+            if (!isnan_(vk) && vk > vmax) vmax = vk;
+          }
+          keep = v[t] == vmax;
+          if (keep) {
+            for (int k = lo; k < t; ++k)
+              if (v[k] == vmax && s[k] == s[t]) keep = false;
+          }
+        }
+      }
+      sidx[t] = keep ? 1 : 0;  // reuse shared memory as the keep mask
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n_in; t += kBlock) {
+      if (!sidx[t]) {
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+        g[t] = p[t] = v[t] = s[t] = nan;
+      }
+    }
+    __syncthreads();
+    // ---- 3. the scan (warp 0; all lanes hold the state, lane 0 writes)
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double* GO = grid_out + (int64_t)row * n_out;
+      double* PO = policy_out + (int64_t)row * n_out;
+      double* VO = value_out + (int64_t)row * n_out;
+      const double nan = __longlong_as_double(0x7ff8000000000000LL);
+      for (int t = lane; t < n_out; t += 32) GO[t] = PO[t] = VO[t] = nan;
+      __syncwarp();
+      int cnt = 0;
+      auto emit = [&](double eg, double ep, double ev) {
+        if (lane == 0 && cnt < n_out) {
+          GO[cnt] = eg;
+          PO[cnt] = ep;
+          VO[cnt] = ev;
+        }
+        ++cnt;
+      };
+      double gk = g[0], pk = p[0], vk = v[0];
+      double gj = g[0], pj = p[0], vj = v[0], sj = s[0];
+      const double near = 16.0 * 2.220446049250313e-16;
+      for (int idx = 1; idx < n_in; ++idx) {
+        const double gi = g[idx], pi = p[idx], vi = v[idx], si = s[idx];
+        const bool valid = !isnan_(gi) && !isnan_(vi);
+        const bool sw = valid && policy_jump(gj, pj, gi, pi, thr, true, sj, si);
+        const bool node_crossing = valid && sw && gi == gj && vi == vj;
+        const double secant = slope(gj, vj, gi, vi);
+        const double grad_before = slope(gk, vk, gj, vj);
+        double jg, jp, jv;
+        const bool jf = find_same_segment(g, p, v, n_in, gj, pj, idx, 1, thr, jg, jp, jv);
+        bool below_j = false;
+        if (sw && jf) below_j = (gi == jg) ? (vi < jv) : (secant < slope(gi, vi, jg, jv));
+        const bool sav_dec = si < sj;
+        bool dropped = !valid || ((vi < vj) && !sw) || (sav_dec && secant < grad_before) || below_j;
+        dropped = dropped && !node_crossing;
+        if (dropped) continue;
+        double fg, fp, fv, bg, bp, bv;
+        const bool ff = find_same_segment(g, p, v, n_in, gi, pi, idx, 1, thr, fg, fp, fv);
+        const bool bf = find_same_segment(g, p, v, n_in, gi, pi, idx, -1, thr, bg, bp, bv);
+        const bool found = ff || bf;
+        const double pg = ff ? fg : bg, pp = ff ? fp : bp, pv = ff ? fv : bv;
+        const double i_slope = slope(gi, vi, pg, pv);
+        const double i_pslope = slope(gi, pi, pg, pp);
+        const bool j_dom = sw && found && (secant > i_slope) && !node_crossing;
+        const double pslope_kj = slope(gk, pk, gj, pj);
+        double k6g, k6v;
+        intersect(gj, vj, grad_before, gi, vi, i_slope, k6g, k6v);
+        const double k6pl = pj + pslope_kj * (k6g - gj);
+        const double k6pr = pi + i_pslope * (k6g - gi);
+        const bool kink6 = j_dom && (k6g > gk) && (k6g < gj) && (k6g < gi);
+        const double j_slope = jf ? slope(gj, vj, jg, jv) : grad_before;
+        const double j_pslope = jf ? slope(gj, pj, jg, jp) : pslope_kj;
+        double k5g, k5v;
+        intersect(gj, vj, j_slope, gi, vi, i_slope, k5g, k5v);
+        const double k5pl = pj + j_pslope * (k5g - gj);
+        const double k5pr = pi + i_pslope * (k5g - gi);
+        const bool crossing = !j_dom && !node_crossing && sw && found;
+        const double tol = near * fmax(fmax(fabs(gj), fabs(gi)), 1.0);
+        const bool on_j = crossing && fabs(k5g - gj) <= tol;
+        const bool on_i = crossing && !on_j && fabs(k5g - gi) <= tol;
+        const bool kink5 = crossing && !on_j && !on_i && (k5g > gj) && (k5g < gi);
+        const bool plain = !j_dom && !kink5 && !on_j && !on_i;
+        if (kink6) {
+          emit(k6g, k6pl, k6v);
+          emit(k6g, k6pr, k6v);
+        } else if (plain || kink5 || on_j || on_i) {
+          emit(gj, pj, vj);
+          if (kink5) {
+            emit(k5g, k5pl, k5v);
+            emit(k5g, k5pr, k5v);
+          } else if (on_j) {
+            emit(gj, k5pr, k5v);
+          } else if (on_i) {
+            emit(gi, k5pl, k5v);
+          }
+        }
+        const bool keeps_k = j_dom && !kink6;
+        if (!keeps_k) {
+          if (kink5) {
+            gk = k5g; pk = k5pr; vk = k5v;
+          } else if (kink6) {
+            gk = k6g; pk = k6pr; vk = k6v;
+          } else {
+            gk = gj;
+            pk = on_j ? k5pr : pj;
+            vk = on_j ? k5v : vj;
+          }
+        }
+        gj = gi; pj = pi; vj = vi; sj = si;
+      }
+      if (!isnan_(gj) && !isnan_(vj)) emit(gj, pj, vj);
+      if (lane == 0) n_kept[row] = cnt;
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+extern "C" size_t lcmx_fues_workspace_bytes(int n_rows, int n_in) {
+  if (n_rows <= 0 || n_in <= 0) return 0;
+  return (size_t)n_rows * 4 * (size_t)n_in * sizeof(double);
+}
+
+static int launch_fues(const double* grid, const double* policy, const double* value, const double* savings,
+                       int n_rows, int n_in, double jump_thresh, double* grid_out, double* policy_out,
+                       double* value_out, int n_out, int* n_kept, double* work, cudaStream_t stream,
+                       std::string& err) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  int grid_n = n_rows < sms * 4 ? n_rows : sms * 4;
+  fues_kernel<<<grid_n, kBlock, 0, stream>>>(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out,
+                                             policy_out, value_out, n_out, n_kept, work);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    err = std::string("fues launch: ") + cudaGetErrorString(e);
+    return LCMX_ERR_LAUNCH;
+  }
+  return LCMX_OK;
+}
+
+int lcmx_set_error_from(lcmx_ctx* ctx, int code, const std::string& msg);
+
+extern "C" int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
+                              const double* savings, int n_rows, int n_in, double jump_thresh,
+                              double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+  if (!ctx || !grid || !policy || !value || !grid_out || !policy_out || !value_out || !n_kept || n_rows < 0 ||
+      n_in < 1 || n_out < 1 || !(jump_thresh > 0.0))
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan: bad arguments");
+  if (n_in > kMaxSort)
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan: rows longer than 8192 candidates");
+  if (n_rows == 0) return LCMX_OK;
+  if (!workspace || workspace_bytes < lcmx_fues_workspace_bytes(n_rows, n_in))
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan: workspace too small");
+  std::string err;
+  int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
+                       n_out, n_kept, static_cast<double*>(workspace), (cudaStream_t)stream, err);
+  if (rc) return lcmx_set_error_from(ctx, rc, err);
+  return LCMX_OK;
+}

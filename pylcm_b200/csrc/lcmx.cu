@@ -392,3 +392,6 @@ extern "C" int lcmx_count_nonfinite(lcmx_ctx* ctx, const double* x, long long n,
   if (e != cudaSuccess) return set_err(ctx, LCMX_ERR_LAUNCH, std::string("nonfinite: ") + cudaGetErrorString(e));
   return LCMX_OK;
 }
+
+// error helper shared with the other translation units of this library
+int lcmx_set_error_from(lcmx_ctx* ctx, int code, const std::string& msg) { return set_err(ctx, code, msg); }

@@ -27,6 +27,8 @@ EXPORTED = (
     "lcmx_simulate",
     "lcmx_egm_step",
     "lcmx_count_nonfinite",
+    "lcmx_fues_workspace_bytes",
+    "lcmx_fues_scan",
 )
 
 
@@ -74,6 +76,11 @@ def load_library() -> ctypes.CDLL:
             "lcmx_simulate": ([vp, cp, ctypes.POINTER(LaunchArgs), ctypes.c_ulonglong, vp], ip),
             "lcmx_egm_step": ([vp, cp, ctypes.POINTER(LaunchArgs), vp], ip),
             "lcmx_count_nonfinite": ([vp, vp, ctypes.c_longlong, vp, vp], ip),
+            "lcmx_fues_workspace_bytes": ([ip, ip], ctypes.c_size_t),
+            "lcmx_fues_scan": (
+                [vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp, ctypes.c_size_t, vp],
+                ip,
+            ),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
@@ -121,6 +128,18 @@ class Context:
 
     def count_nonfinite(self, ptr: int, n: int, counts_ptr: int, stream: int) -> None:
         self.check(self.lib.lcmx_count_nonfinite(self.h, ptr, n, counts_ptr, stream))
+
+    def fues_workspace_bytes(self, n_rows: int, n_in: int) -> int:
+        return int(self.lib.lcmx_fues_workspace_bytes(n_rows, n_in))
+
+    def fues_scan(self, grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out,
+                  value_out, n_out, n_kept, workspace, workspace_bytes, stream) -> None:
+        """FUES envelope of candidate rows (all arguments are device pointers)."""
+        self.check(
+            self.lib.lcmx_fues_scan(self.h, grid, policy, value, savings, n_rows, n_in, float(jump_thresh),
+                                    grid_out, policy_out, value_out, n_out, n_kept, workspace,
+                                    workspace_bytes, stream)
+        )
 
 
 class Module:

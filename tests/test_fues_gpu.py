@@ -1,0 +1,89 @@
+"""FUES kernel (liblcmx.so) vs the oracle restatement, row by row."""
+
+import numpy as np
+import pytest
+
+from oracle.fues import refine
+from tests.test_fues_oracle import _crossing
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_fues(rows_g, rows_c, rows_v, rows_s, n_out, thr=2.0):
+    import torch
+
+    from pylcm_b200.runtime import get_context
+
+    ctx = get_context(0)
+    n_rows, n_in = rows_g.shape
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    g, c, v, s = d(rows_g), d(rows_c), d(rows_v), d(rows_s)
+    go = torch.empty((n_rows, n_out), dtype=torch.float64, device="cuda")
+    co = torch.empty_like(go)
+    vo = torch.empty_like(go)
+    nk = torch.empty(n_rows, dtype=torch.int32, device="cuda")
+    wb = ctx.fues_workspace_bytes(n_rows, n_in)
+    ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    ctx.fues_scan(g.data_ptr(), c.data_ptr(), v.data_ptr(), s.data_ptr(), n_rows, n_in, thr,
+                  go.data_ptr(), co.data_ptr(), vo.data_ptr(), n_out, nk.data_ptr(), ws.data_ptr(), wb, stream)
+    torch.cuda.synchronize()
+    return go.cpu().numpy(), co.cpu().numpy(), vo.cpu().numpy(), nk.cpu().numpy()
+
+
+def _same(a, b):
+    """Same NaN pattern; values within 1e-12 (inserted crossings may differ by
+    an ulp: fused multiply-add on the GPU)."""
+    np.testing.assert_array_equal(np.isnan(a), np.isnan(b))
+    np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12, equal_nan=True)
+
+
+def _rows_nonconcave(n_rows, n, seed):
+    """Two interleaved concave branches with a jump in savings (a discrete-choice
+    kink), shuffled, with a few NaN (absent) candidates."""
+    rng = np.random.default_rng(seed)
+    G, C, V, S = [], [], [], []
+    for _ in range(n_rows):
+        a = np.sort(rng.uniform(0, 10, n))
+        half = n // 2
+        c = np.where(np.arange(n) < half, 0.5 + 0.3 * a, 1.5 + 0.6 * a)
+        shift = np.where(np.arange(n) < half, 0.0, rng.uniform(0.5, 2.0))
+        g = a + c
+        v = np.log(c) + 0.2 * np.sqrt(a + 1) + shift - 0.15 * np.arange(n) / n
+        perm = rng.permutation(n)
+        g, c, v, s = g[perm], c[perm], v[perm], a[perm]
+        drop = rng.random(n) < 0.02
+        g = np.where(drop, np.nan, g)
+        v = np.where(drop, np.nan, v)
+        G.append(g); C.append(c); V.append(v); S.append(s)
+    return np.array(G), np.array(C), np.array(V), np.array(S)
+
+
+def test_fues_kernel_matches_oracle_on_analytic_crossing():
+    g, c, v = _crossing()
+    go, co, vo, nk = _gpu_fues(g[None], c[None], v[None], (g - c)[None], 12)
+    rg, rc, rv, n = refine(g, c, v, g - c, 12)
+    assert nk[0] == n
+    _same(go[0], rg)
+    _same(co[0], rc)
+    _same(vo[0], rv)
+
+
+@pytest.mark.parametrize("n", [17, 300, 2020])
+def test_fues_kernel_matches_oracle_on_nonconcave_rows(n):
+    G, C, V, S = _rows_nonconcave(6, n, seed=n)
+    n_out = 2 * n + 2
+    go, co, vo, nk = _gpu_fues(G, C, V, S, n_out)
+    for r in range(G.shape[0]):
+        rg, rc, rv, k = refine(G[r], C[r], V[r], S[r], n_out)
+        assert nk[r] == k
+        _same(go[r], rg)
+        _same(co[r], rc)
+        _same(vo[r], rv)
+
+
+def test_fues_kernel_reports_overflow():
+    G, C, V, S = _rows_nonconcave(2, 64, seed=3)
+    go, co, vo, nk = _gpu_fues(G, C, V, S, 4)
+    assert np.all(nk > 4)
+    assert np.all(np.isfinite(go[:, :4]))
