@@ -116,6 +116,19 @@ int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* policy, cons
                    double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* lcmx_fues_scan without a caller workspace: for callers that cannot call
+ * cudaMalloc on this path (code running inside another runtime's execution,
+ * such as an XLA FFI custom-call handler).  No counterpart in the reference.
+ * Scratch is an 8 MiB file-scope device array per device, so
+ * lcmx_fues_workspace_bytes(n_rows, n_in) must not exceed 8 MiB (larger calls
+ * return LCMX_ERR_ARGS).  The first call on a device resolves the array's
+ * address (make it before any stream capture); all calls share the array, so
+ * calls that overlap on the GPU race.  Allocates nothing. */
+int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
+                          const double* savings, int n_rows, int n_in, double jump_thresh,
+                          double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
+                          void* stream);
+
 /* Count non-finite (and separately NaN) entries of a double array; the two
  * counters are accumulated into counts_dev[0] (nan) and counts_dev[1]
  * (+-inf), which the caller zeroes. */

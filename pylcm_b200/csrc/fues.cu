@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "../../include/lcmx.h"
@@ -337,6 +338,79 @@ extern "C" int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* p
   std::string err;
   int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
                        n_out, n_kept, static_cast<double*>(workspace), (cudaStream_t)stream, err);
+  if (rc) return lcmx_set_error_from(ctx, rc, err);
+  return LCMX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Variant that allocates nothing.
+//
+// Some callers cannot call cudaMalloc on this path: code running inside
+// another runtime's execution -- for example an XLA FFI custom-call handler,
+// which is how the reference runs its native kernels -- must not allocate
+// there (cudaMalloc synchronises the device and bypasses the runtime's
+// allocator).  For them lcmx_fues_scan_static takes its workspace from the
+// file-scope device array below instead of a caller pointer.
+//
+// * Size: kStaticScratchBytes (8 MiB) per device, held by every GPU that
+//   loads this library until the process exits.  A call needs
+//   lcmx_fues_workspace_bytes(n_rows, n_in) <= 8 MiB, i.e. at most
+//   262144 / n_in rows (129 rows of 2020 candidates); larger calls are
+//   rejected with LCMX_ERR_ARGS.
+// * Set-up: the first call on a device, with that device current, looks up
+//   the array's device address with cudaGetSymbolAddress (in host code the
+//   symbol is only a host-side stand-in, not a device address) and caches it
+//   for that device.  Make that first call before any stream capture.
+// * Sharing: every call uses the same array, which keeps the last call's
+//   contents.  Nothing in it has to start at zero (each row's sorted copy is
+//   written in full before it is read), but calls that overlap on the GPU
+//   race on it: serialise them (one stream, or events).
+namespace {
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;
+__device__ __align__(256) double g_fues_static_scratch[kStaticScratchBytes / sizeof(double)];
+std::mutex g_static_mu;
+double* g_static_ptr[64] = {};
+}  // namespace
+
+int lcmx_ctx_device_of(const lcmx_ctx* ctx);
+
+extern "C" int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
+                                     const double* savings, int n_rows, int n_in, double jump_thresh,
+                                     double* grid_out, double* policy_out, double* value_out, int n_out,
+                                     int* n_kept, void* stream) {
+  if (!ctx || !grid || !policy || !value || !grid_out || !policy_out || !value_out || !n_kept || n_rows < 0 ||
+      n_in < 1 || n_out < 1 || !(jump_thresh > 0.0))
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan_static: bad arguments");
+  if (n_in > kMaxSort)
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan_static: rows longer than 8192 candidates");
+  const size_t need = lcmx_fues_workspace_bytes(n_rows, n_in);
+  if (need > kStaticScratchBytes)
+    return lcmx_set_error_from(
+        ctx, LCMX_ERR_ARGS,
+        "lcmx_fues_scan_static: " + std::to_string(n_rows) + " rows of " + std::to_string(n_in) +
+            " candidates need " + std::to_string(need) + " bytes of scratch, more than the 8 MiB static array (at most " +
+            std::to_string(kStaticScratchBytes / (4 * sizeof(double) * (size_t)n_in)) + " rows of this length)");
+  if (n_rows == 0) return LCMX_OK;
+  const int dev = lcmx_ctx_device_of(ctx);
+  if (dev < 0 || dev >= 64) return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan_static: device ordinal >= 64");
+  cudaError_t e = cudaSetDevice(dev);
+  if (e != cudaSuccess) return lcmx_set_error_from(ctx, LCMX_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  double* work = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_static_mu);
+    if (!g_static_ptr[dev]) {
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_fues_static_scratch);
+      if (e != cudaSuccess || !p)
+        return lcmx_set_error_from(ctx, LCMX_ERR_CUDA,
+                                   std::string("cudaGetSymbolAddress(static FUES scratch): ") + cudaGetErrorString(e));
+      g_static_ptr[dev] = static_cast<double*>(p);
+    }
+    work = g_static_ptr[dev];
+  }
+  std::string err;
+  int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
+                       n_out, n_kept, work, (cudaStream_t)stream, err);
   if (rc) return lcmx_set_error_from(ctx, rc, err);
   return LCMX_OK;
 }

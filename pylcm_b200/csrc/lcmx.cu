@@ -395,3 +395,6 @@ extern "C" int lcmx_count_nonfinite(lcmx_ctx* ctx, const double* x, long long n,
 
 // error helper shared with the other translation units of this library
 int lcmx_set_error_from(lcmx_ctx* ctx, int code, const std::string& msg) { return set_err(ctx, code, msg); }
+
+// device ordinal of a context (for translation units that cannot see the struct)
+int lcmx_ctx_device_of(const lcmx_ctx* ctx) { return ctx ? ctx->device : 0; }

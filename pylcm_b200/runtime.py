@@ -29,6 +29,7 @@ EXPORTED = (
     "lcmx_count_nonfinite",
     "lcmx_fues_workspace_bytes",
     "lcmx_fues_scan",
+    "lcmx_fues_scan_static",
 )
 
 
@@ -81,6 +82,7 @@ def load_library() -> ctypes.CDLL:
                 [vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp, ctypes.c_size_t, vp],
                 ip,
             ),
+            "lcmx_fues_scan_static": ([vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
