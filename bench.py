@@ -195,22 +195,16 @@ def run_ours(args) -> dict:
 
     # ---- kernel-level timing of the dominant kernel (kernel a), eager, events
     plan = fast.plan
-    ib, pb = plan.items.data_ptr(), plan.prefix.data_ptr()
+    prepared = plan._prepare()
     k_times, k_bytes, k_evals = [], [], []
     e_times = []
     flush_l2(torch, flush)
     torch.cuda.synchronize()
-    for l in plan.launches:
+    for l, launch in zip(plan.launches, prepared):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        mod = l.module.module
-        ip = ib + 8 * l.item_off
-        pp = pb + 4 * l.prefix_off
-        if l.kind == "bellman":
-            mod.bellman_step(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream.cuda_stream)
-        else:
-            mod.expectation(l.kernel, ip, pp, l.n_items, l.n_tiles, l.block, l.smem, stream.cuda_stream)
+        launch(stream.cuda_stream)
         b.record(stream)
         if l.kind == "bellman":
             spec = l.module.spec

@@ -121,6 +121,9 @@ def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R):
             mass += p
             if p == 0.0:
                 continue
+            if tg.unreachable:
+                EV = EV * np.nan
+                continue
             if tg.next_R is None:
                 EV = EV + p * float(np.asarray(V_next[tg.spec.name]))
                 continue

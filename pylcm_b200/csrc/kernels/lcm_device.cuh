@@ -308,3 +308,52 @@ __device__ __forceinline__ int lcm_categorical(const double* p, double u) {
   for (int i = 0; i < N; ++i) { acc += p[i]; if (thr < acc) { pick = i; break; } }
   return pick;
 }
+
+// ---------------------------------------------------------------------------
+// Reads of a NaN-padded, weakly ascending refined row (DC-EGM carry rows),
+// with the reference's rules (src/_lcm/egm/interp.py:63-131): linear
+// extrapolation below the first node, clamp at or above the last, a
+// duplicated abscissa read right-continuously, a -inf endpoint forcing -inf
+// in the bracket's interior.  The value read is a cubic Hermite with node
+// slopes dp, limited by Fritsch & Carlson (1980); it falls back to linear
+// where a slope or endpoint is not finite.  The slope row itself is read
+// linearly.  L is the number of valid (non-NaN) leading entries.
+__device__ __forceinline__ void lcm_row_read(const double* __restrict__ xp, const double* __restrict__ fp,
+                                             const double* __restrict__ dp, int L, double xq,
+                                             double& val, double& slope_val) {
+  if (L <= 0) { val = slope_val = LCM_NAN; return; }
+  if (L == 1) { val = fp[0]; slope_val = dp ? dp[0] : LCM_NAN; return; }
+  int lo = 0, hi = L;  // first index with xp > xq
+  while (lo < hi) { const int mid = (lo + hi) >> 1; if (xp[mid] > xq) hi = mid; else lo = mid + 1; }
+  const int idx = lo - 1;
+  if (idx >= L - 1) { val = fp[L - 1]; slope_val = dp ? dp[L - 1] : LCM_NAN; return; }
+  const int b = idx < 0 ? 0 : idx;
+  const double x0 = xp[b], x1 = xp[b + 1], f0 = fp[b], f1 = fp[b + 1];
+  const double h = x1 - x0;
+  const double t = h > 0.0 ? (xq - x0) / h : 0.0;
+  double v = h > 0.0 ? f0 + t * (f1 - f0) : f1;
+  double s = LCM_NAN;
+  if (dp) {
+    const double d0 = dp[b], d1 = dp[b + 1];
+    s = h > 0.0 ? d0 + t * (d1 - d0) : d1;
+    if (lcm_isfinite(f0) && lcm_isfinite(f1) && lcm_isfinite(d0) && lcm_isfinite(d1) && h > 0.0 && idx >= 0) {
+      const double delta = (f1 - f0) / h;
+      double e0 = 0.0, e1 = 0.0;
+      if (delta != 0.0) {
+        double a = d0 / delta, bb = d1 / delta;
+        a = a > 0.0 ? a : 0.0;
+        bb = bb > 0.0 ? bb : 0.0;
+        const double r2 = a * a + bb * bb;
+        const double tau = r2 > 9.0 ? 3.0 / sqrt(r2) : 1.0;
+        e0 = tau * a * delta;
+        e1 = tau * bb * delta;
+      }
+      const double t2 = t * t, t3 = t2 * t;
+      v = (2 * t3 - 3 * t2 + 1) * f0 + (t3 - 2 * t2 + t) * h * e0 + (-2 * t3 + 3 * t2) * f1 + (t3 - t2) * h * e1;
+    }
+  }
+  const bool neg0 = f0 == -LCM_INF, neg1 = f1 == -LCM_INF;
+  if (idx >= 0 && (neg0 || neg1) && !((xq == x0) && lcm_isfinite(f0)) && !((xq == x1) && lcm_isfinite(f1))) v = -LCM_INF;
+  val = v;
+  slope_val = s;
+}

@@ -58,6 +58,9 @@ class EgmTarget:
     disc_laws: dict  # state name -> NextState (target's discrete states)
     next_R: ir.Expr | None  # law of the liquid state in A (None: stateless target)
     dR_dA: ir.Expr | None
+    # no law for one of the target's states: the source cannot reach the
+    # target; a non-zero probability toward it poisons the continuation (NaN)
+    unreachable: bool = False
 
 
 @dataclasses.dataclass
@@ -171,14 +174,20 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
             raise ModelInitializationError(f"DCEGM target {tname!r} must be a DCEGM regime or stateless")
         laws = {}
         nextR = None
+        src_states = {a.name for a in spec.states}
+        unreachable = False
         for ax in tg.states:
             if ax.kind == "process":
+                if ax.name not in src_states:
+                    unreachable = True
+                    break
                 laws[ax.name] = NextState("process", None, ax.name)
                 continue
             fname = f"next_{ax.name}"
             if fname not in spec.functions:
-                if ax.kind == "continuous":
-                    raise ModelInitializationError(f"{spec.name}->{tname}: no law for {ax.name!r}")
+                if ax.kind == "continuous" or ax.name not in src_states:
+                    unreachable = True
+                    break
                 laws[ax.name] = NextState("det", ir.var("state", ax.name, "i"))
                 continue
             law = spec.functions[fname]
@@ -189,8 +198,9 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
                 laws[ax.name] = NextState("markov", val)
             else:
                 laws[ax.name] = NextState("det", ir.const(val))
-        if nextR is None:
-            raise ModelInitializationError(f"{spec.name}->{tname}: no law for the liquid state")
+        if unreachable or nextR is None:
+            tgs.append(EgmTarget(tg, probs[tg.rid], {}, None, None, unreachable=True))
+            continue
         tgs.append(EgmTarget(tg, probs[tg.rid], laws, nextR, ir.diff(nextR, A_VAR)))
     sav = np.asarray(solver.savings_grid.to_numpy(), dtype=np.float64)
     nc = int(solver.n_constrained_points)
@@ -217,3 +227,28 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
         feasible=feasible,
         tracer=t,
     )
+
+
+def _as_traced(er: "EgmRegime"):
+    """A TracedRegime view of the EGM tracer's parameters (layout / packing)."""
+    from pylcm_b200.spec import TracedRegime
+
+    t = er.tracer
+    return TracedRegime(
+        spec=er.spec, U=er.U, F=ir.const(True), regime_probs=None, regime_id=None, next_states={},
+        param_values=t.param_values, param_order=t.param_order, param_sources=t.param_sources,
+        beta=er.beta, taste_scale=er.taste_scale, process_tables={},
+    )
+
+
+def _tracer_layout(self):
+    return _as_traced(self).param_layout()
+
+
+def _pack_for(self, resolver):
+    tr = _as_traced(self)
+    return tr.pack_params(tr.values_for(resolver))
+
+
+EgmRegime.tracer_layout = _tracer_layout
+EgmRegime.pack_for = _pack_for

@@ -28,6 +28,7 @@ import numpy as np
 
 from pylcm_b200.codegen import LaunchConfig, RegimeKernels
 from pylcm_b200.exceptions import ModelInitializationError
+from pylcm_b200.egm import is_egm
 from pylcm_b200.spec import ParamResolver, RegimeSpec, TracedRegime, trace_regime
 
 
@@ -105,6 +106,19 @@ class SolveEngine:
             self._kernels[key] = rk
         return rk
 
+    def egm_kernels(self, spec: RegimeSpec, targets: tuple[str, ...], params):
+        """Generated DC-EGM kernels of a regime for one next-period target set."""
+        from pylcm_b200.egm import trace_egm_regime
+        from pylcm_b200.egm_codegen import EgmKernels
+
+        key = ("egm", spec.name, targets)
+        ek = self._kernels.get(key)
+        if ek is None:
+            er = trace_egm_regime(spec, self.specs, self.resolver(params), targets)
+            ek = EgmKernels(er)
+            self._kernels[key] = ek
+        return ek
+
     def module(self, rk: RegimeKernels):
         from pylcm_b200.runtime import get_context
 
@@ -175,7 +189,8 @@ class SolvePlan:
         by = {s.name: s for s in specs}
         self.params: dict[tuple, Any] = {}
         self.ev: dict[tuple, tuple] = {}
-        step_list: list[tuple[int, RegimeSpec, tuple, RegimeKernels]] = []
+        step_list: list[tuple[int, RegimeSpec, tuple, Any]] = []
+        egm_steps: list = []
         for period in range(T - 1, -1, -1):
             for s in specs:
                 if period not in s.active_periods:
@@ -183,14 +198,52 @@ class SolvePlan:
                 if not s.terminal and period == T - 1:
                     raise ModelInitializationError(f"non-terminal regime {s.name} active in the last period")
                 targets = eng.targets_at(s, period)
-                rk = eng.kernels(s, targets, params_list[0], n)
                 key = (s.name, targets)
+                if is_egm(s) and not s.terminal:
+                    ek = eng.egm_kernels(s, targets, params_list[0])
+                    if key not in self.params:
+                        vecs = [ek.er.pack_for(r) for r in resolvers]
+                        self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                    egm_steps.append((period, s, targets, ek))
+                    step_list.append((period, s, targets, ek))
+                    continue
+                rk = eng.kernels(s, targets, params_list[0], n)
                 if key not in self.params:
                     vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in resolvers]
                     self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
                 step_list.append((period, s, targets, rk))
+        # DC-EGM buffers: carry rows per active period, scratch per regime
+        self.egm: dict[str, dict] = {}
+        for period, s, targets, ek in egm_steps:
+            if s.name in self.egm:
+                continue
+            er = ek.er
+            nslot = max(len(s.active_periods), 1)
+            npad, nrow, ncand = er.n_pad, er.n_rows, er.n_cand
+            f64 = dict(dtype=torch.float64, device=dev)
+            self.egm[s.name] = {
+                "rg": torch.full((nslot, n, nrow, npad), float("nan"), **f64),
+                "rc": torch.full((nslot, n, nrow, npad), float("nan"), **f64),
+                "rv": torch.full((nslot, n, nrow, npad), float("nan"), **f64),
+                "mu": torch.full((nslot, n, nrow, npad), float("nan"), **f64),
+                "nk": torch.zeros((nslot, n, nrow), dtype=torch.int32, device=dev),
+                "cand": [torch.empty((n, nrow, ncand), **f64) for _ in range(4)],
+                "ev0": torch.empty((n, nrow), **f64),
+                "npad": npad,
+                "nrow": nrow,
+                "ncand": ncand,
+                "sav": torch.as_tensor(er.savings, **f64),
+            }
+            from pylcm_b200.runtime import get_context
+
+            wb = get_context(eng.device).fues_workspace_bytes(n * nrow, ncand)
+            self.egm[s.name]["ws"] = torch.empty(max(wb, 8), dtype=torch.uint8, device=dev)
+            self.egm[s.name]["wb"] = wb
+
         # EV buffers per (source, target set, target)
         for period, s, targets, rk in step_list:
+            if not isinstance(rk, RegimeKernels):
+                continue
             for t in rk.targets:
                 if t.scalar:
                     continue
@@ -208,6 +261,8 @@ class SolvePlan:
         # action tables (kernel a0 output) per (regime, target set), reused across periods
         self.atab: dict[tuple, Any] = {}
         for period, s, targets, rk in step_list:
+            if not isinstance(rk, RegimeKernels):
+                continue
             k = (s.name, targets)
             if k not in self.atab:
                 words = max(1, rk.atab_words) * s.n_actions
@@ -244,6 +299,9 @@ class SolvePlan:
 
         ages = model.ages.values
         for period, s, targets, rk in step_list:
+            if not isinstance(rk, RegimeKernels):
+                self._egm_launches(rk, period, s, targets, float(ages[period]), resolvers, add_launch)
+                continue
             age = float(ages[period])
             pbuf = self.params[(s.name, targets)]
             plen = pbuf.shape[1]
@@ -344,21 +402,101 @@ class SolvePlan:
 
         self.items = torch.as_tensor(np.concatenate(words), dtype=torch.int64, device=dev)
         self.prefix = torch.as_tensor(np.concatenate(prefixes), dtype=torch.int32, device=dev)
-        for rk in {id(l.module): l.module for l in self.launches}.values():
+        for rk in {id(l.module): l.module for l in self.launches if l.kind != "fues"}.values():
             eng.module(rk)
         self.graph = None
         self._prepared = None
+
+    # ------------------------------------------------------------- DC-EGM
+    def _egm_launches(self, ek, period, s, targets, age, resolvers, add_launch) -> None:
+        """Records and launches of one DC-EGM period: candidates (c1), FUES,
+        carry marginal utilities, publication on the state grid."""
+        n = self.n
+        er = ek.er
+        b = self.egm[s.name]
+        slot = self.slot[s.name][period]
+        pbuf = self.params[(s.name, targets)]
+        grid = self.sgrid[s.name][[a.name for a in s.states].index(er.E)]
+        recs = []
+        for i in range(n):
+            r = np.zeros(ek.n_words, dtype=np.int64)
+            r[ek.W_P] = pbuf[i].data_ptr()
+            r[ek.W_PERIOD] = period
+            r[ek.W_AGE] = _f2w(age)
+            r[ek.W_NSAV] = len(er.savings)
+            r[ek.W_SAV] = b["sav"].data_ptr()
+            r[ek.W_NGRID] = grid.numel()
+            r[ek.W_GRID] = grid.data_ptr()
+            for wname, arr in zip(("W_CG", "W_CC", "W_CV", "W_CS"), b["cand"]):
+                r[getattr(ek, wname)] = arr[i].data_ptr()
+            r[ek.W_EV0] = b["ev0"][i].data_ptr()
+            r[ek.W_RG] = b["rg"][slot, i].data_ptr()
+            r[ek.W_RC] = b["rc"][slot, i].data_ptr()
+            r[ek.W_RV] = b["rv"][slot, i].data_ptr()
+            r[ek.W_MU] = b["mu"][slot, i].data_ptr()
+            r[ek.W_NK] = b["nk"][slot, i].data_ptr()
+            r[ek.W_V] = self.V[s.name][i, slot].data_ptr()
+            r[ek.W_POL] = self.pol[s.name][i, slot].data_ptr()
+            r[ek.W_NPAD] = b["npad"]
+            r[ek.W_TASTE] = _f2w(resolvers[i].taste_scale(s.name) if s.taste_shocks else 0.0)
+            for t, w in zip(er.targets, ek.W_T):
+                tslot = self.slot[t.spec.name][period + 1]
+                if t.unreachable:
+                    continue
+                if t.next_R is None:
+                    r[w["scalar"]] = self.V[t.spec.name][i, tslot].data_ptr()
+                    continue
+                cb = self.egm[t.spec.name]
+                r[w["rg"]] = cb["rg"][tslot, i].data_ptr()
+                r[w["rv"]] = cb["rv"][tslot, i].data_ptr()
+                r[w["mu"]] = cb["mu"][tslot, i].data_ptr()
+                r[w["nk"]] = cb["nk"][tslot, i].data_ptr()
+                r[w["npad"]] = cb["npad"]
+                r[w["taste"]] = _f2w(resolvers[i].taste_scale(t.spec.name) if t.spec.taste_shocks else 0.0)
+            recs.append(r)
+        cname, uname, pname = ek.names()
+        nrow, npad, ncand = b["nrow"], b["npad"], b["ncand"]
+        ns = nrow // er.n_disc_actions
+        add_launch("egm", ek, cname, recs, [math.ceil(nrow * len(er.savings) / 256)] * n, 256, 0, period)
+        self.launches.append(
+            Launch("fues", ("fues", s.name, slot, er.jump_thresh), "lcmx_fues_scan", 0, 0, n * nrow, 0, 0, 0, period)
+        )
+        add_launch("egm", ek, uname, recs, [math.ceil(nrow * npad / 256)] * n, 256, 0, period)
+        add_launch("egm", ek, pname, recs, [math.ceil(ns * grid.numel() / 256)] * n, 256, 0, period)
+
+    def _fues_launch(self, spec_name, slot, thr):
+        from pylcm_b200.runtime import get_context
+
+        ctx = get_context(self.eng.device)
+        b = self.egm[spec_name]
+        cg, cc, cv, cs = b["cand"]
+        nrows = self.n * b["nrow"]
+        ptrs = (cg.data_ptr(), cc.data_ptr(), cv.data_ptr(), cs.data_ptr())
+        outs = (b["rg"][slot].data_ptr(), b["rc"][slot].data_ptr(), b["rv"][slot].data_ptr())
+        nk = b["nk"][slot].data_ptr()
+        ws, wb, ncand, npad = b["ws"].data_ptr(), b["wb"], b["ncand"], b["npad"]
+
+        def launch(stream):
+            ctx.fues_scan(*ptrs, nrows, ncand, thr, *outs, npad, nk, ws, wb, stream)
+
+        return launch
 
     # ---------------------------------------------------------------- run
     def _prepare(self) -> list:
         ib = self.items.data_ptr()
         pb = self.prefix.data_ptr()
-        return [
-            l.module.module.prepared(
-                l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem
+        out = []
+        for l in self.launches:
+            if l.kind == "fues":
+                _, name, slot, thr = l.module
+                out.append(self._fues_launch(name, slot, thr))
+                continue
+            out.append(
+                l.module.module.prepared(
+                    l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem
+                )
             )
-            for l in self.launches
-        ]
+        return out
 
     def run(self, stream: int | None = None) -> None:
         """Issue every launch of the plan (all periods) on `stream`."""

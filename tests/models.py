@@ -437,3 +437,121 @@ def hc_params(seed=0, n_shock=32, beta=None, crra=None, interest_rate=None):
         "shock_transition": P,
         "shock_levels": levels,
     }
+
+
+# --------------------------------------------------------------------------
+# DC-EGM retirement model with income shocks (CRRA, 16-node Gauss-Hermite
+# lognormal income weights carried by a discrete iid shock state, optional EV1
+# taste shocks on the work/retire choice)
+@categorical(ordered=False)
+class EgmRegimeId:
+    working: int
+    retired: int
+    dead: int
+
+
+def _make_shock16():
+    ns = {"__annotations__": {f"n{i}": int for i in range(16)}}
+    return categorical(ordered=False)(type("GHShock16", (), ns))
+
+
+GHShock16 = _make_shock16()
+
+
+def _egm_savings(wealth, consumption):
+    return wealth - consumption
+
+
+def _egm_u_work(consumption, labor_supply, crra, disutility_of_work):
+    return consumption ** (1.0 - crra) / (1.0 - crra) - disutility_of_work * (labor_supply == LaborSupply.work)
+
+
+def _egm_u_ret(consumption, crra):
+    return consumption ** (1.0 - crra) / (1.0 - crra)
+
+
+def _egm_inv_mu(marginal_continuation, crra):
+    return marginal_continuation ** (-1.0 / crra)
+
+
+def _egm_next_wealth_work(savings, labor_supply, shock, interest_rate, wage, shock_values):
+    return (1 + interest_rate) * savings + wage * shock_values[shock] * (labor_supply == LaborSupply.work)
+
+
+def _egm_next_wealth_ret(savings, interest_rate):
+    return (1 + interest_rate) * savings
+
+
+def _egm_next_shock(shock, shock_weights):
+    return shock_weights[shock]
+
+
+def _egm_nr_work(labor_supply, period, last_decision_period):
+    return jnp.where(
+        period >= last_decision_period,
+        EgmRegimeId.dead,
+        jnp.where(labor_supply == LaborSupply.work, EgmRegimeId.working, EgmRegimeId.retired),
+    )
+
+
+def _egm_nr_ret(period, last_decision_period):
+    return jnp.where(period >= last_decision_period, EgmRegimeId.dead, EgmRegimeId.retired)
+
+
+def dcegm_model(n_periods=40, n_savings=2000, n_wealth=2000, taste=False, n_constrained=20):
+    """Savings grid 500 (i/(n-1))^3, wealth grid linspace(0, 500, n_wealth)."""
+    from pylcm_b200 import DCEGM, ConsumptionSavingsRegime, ExtremeValueTasteShocks, FUESEnvelope, IrregSpacedGrid, LiquidMargin
+
+    sav = IrregSpacedGrid(points=tuple(500.0 * (i / (n_savings - 1)) ** 3 for i in range(n_savings)))
+    solver = DCEGM(savings_grid=sav, n_constrained_points=n_constrained, envelope=FUESEnvelope())
+    margin = LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings")
+    wealth = LinSpacedGrid(start=0, stop=500, n_points=n_wealth)
+    cons = LinSpacedGrid(start=0.1, stop=500, n_points=200)
+    last = n_periods - 1
+    working = ConsumptionSavingsRegime(
+        actions={"labor_supply": DiscreteGrid(LaborSupply), "consumption": cons},
+        states={"shock": DiscreteGrid(GHShock16), "wealth": wealth},
+        state_transitions={"wealth": _egm_next_wealth_work, "shock": MarkovTransition(_egm_next_shock)},
+        transition=_egm_nr_work,
+        functions={"utility": _egm_u_work, "savings": _egm_savings, "inverse_marginal_utility": _egm_inv_mu},
+        solver=solver,
+        liquid=margin,
+        taste_shocks=ExtremeValueTasteShocks() if taste else None,
+        active=lambda age, last=last: age < last,
+    )
+    retired = ConsumptionSavingsRegime(
+        actions={"consumption": cons},
+        states={"wealth": wealth},
+        state_transitions={"wealth": _egm_next_wealth_ret},
+        transition=_egm_nr_ret,
+        functions={"utility": _egm_u_ret, "savings": _egm_savings, "inverse_marginal_utility": _egm_inv_mu},
+        solver=solver,
+        liquid=margin,
+        active=lambda age, last=last: age < last,
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(
+        regimes={"working": working, "retired": retired, "dead": dead},
+        ages=AgeGrid(start=0, stop=last, step="Y"),
+        regime_id_class=EgmRegimeId,
+        fixed_params={"last_decision_period": n_periods - 2},
+    )
+
+
+def dcegm_params(seed=0, taste_scale=None, beta=0.97, crra=2.0, interest_rate=0.04, wage=20.0, sigma=0.1):
+    rng = np.random.default_rng(seed)
+    x, w = np.polynomial.hermite.hermgauss(16)
+    values = np.exp(np.sqrt(2.0) * sigma * x)
+    weights = w / np.sqrt(np.pi)
+    p = {
+        "discount_factor": beta,
+        "crra": crra,
+        "interest_rate": interest_rate,
+        "wage": wage,
+        "disutility_of_work": float(rng.uniform(0.2, 1.0)),
+        "shock_values": values,
+        "shock_weights": np.tile(weights, (16, 1)),
+    }
+    if taste_scale is not None:
+        p["working"] = {"taste_shocks": {"scale": taste_scale}}
+    return p
