@@ -95,8 +95,10 @@ int lcmx_bellman_step(lcmx_module* mod, const char* kernel, const lcmx_launch_ar
  * of (instance, source regime, target regime) items. */
 int lcmx_expectation(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
                      void* stream);
-/* Kernel (d): one simulated period for a batch of subjects (Philox-4x32-10
- * counter RNG keyed by `seed`, subject and period). */
+/* Kernel (d): one simulated period for a batch of (instance, regime) items,
+ * each with its own subjects (Philox-4x32-10 counter RNG; the key of an item
+ * is `seed` XOR the item's seed word, the counter is (subject, period,
+ * stream id)). */
 int lcmx_simulate(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
                   unsigned long long seed, void* stream);
 /* Kernel (c), part 1: DC-EGM Euler inversion and candidate generation. */

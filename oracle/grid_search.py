@@ -302,6 +302,13 @@ def bellman_step(
     F = np.ones(bshape, dtype=bool)
     for c in spec.constraint_names:
         F = F & np.broadcast_to(np.asarray(ev.value(c), dtype=bool), bshape)
+    if _is_egm(spec) and not spec.terminal:
+        # intrinsic budget of an endogenous-grid regime's grid argmax
+        # (src/_lcm/egm/budget.py:36-100): c <= resources - lowest savings node
+        liq = spec.user.liquid
+        lb = float(np.asarray(spec.solver.savings_grid.to_numpy(), dtype=np.float64)[0])
+        res = ev.value(liq.resources) if liq.resources in spec.functions else ev.env[liq.resources]
+        F = F & np.broadcast_to(np.asarray(env[liq.action]) <= np.asarray(res) - lb, bshape)
 
     if spec.terminal:
         Q = U
@@ -329,6 +336,9 @@ def bellman_step(
             neg = neg | (p < 0)
             if not tgt.states:
                 E = np.broadcast_to(np.asarray(next_V[tgt.name], dtype=np.float64), bshape)
+            elif _unreachable(spec, tgt):
+                # no law for one of the target's states: NaN where p != 0
+                E = np.full(bshape, np.nan)
             else:
                 E = _expected_next_value(
                     spec, tgt, resolver, ev, next_V[tgt.name], procs, sidx_of, aidx_of, bshape, period, age, blend
@@ -382,6 +392,23 @@ def bellman_step(
 
 
 LAST_GAP = None
+
+
+def _is_egm(spec) -> bool:
+    from pylcm_b200.solvers import DCEGM
+
+    return isinstance(spec.solver, DCEGM)
+
+
+def _unreachable(spec, tgt) -> bool:
+    """True when `spec` has no law of motion for one of `tgt`'s states."""
+    src = {a.name for a in spec.states}
+    for ax in tgt.states:
+        if ax.name in src:
+            continue
+        if ax.kind == "process" or f"next_{ax.name}" not in spec.functions:
+            return True
+    return False
 
 
 def _lookup_table(deps, table, sidx_of, aidx_of, bshape, n_out):

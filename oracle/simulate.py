@@ -91,7 +91,14 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
     specs = model.regime_specs
     res = ParamResolver(params, model.fixed_params, tuple(s.name for s in specs))
     if V is None:
-        V, _ = solve(model, params)
+        from oracle.grid_search import _is_egm
+
+        if any(_is_egm(s) for s in specs):
+            from oracle.dcegm import solve as egm_solve
+
+            V, _ = egm_solve(model, params)
+        else:
+            V, _ = solve(model, params)
     T = model.n_periods
     ic = dict(initial_conditions)
     rid = np.asarray(ic.pop("regime_id"), dtype=np.int64)
@@ -162,7 +169,7 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
             for tname in targets:
                 tgt = next(s for s in specs if s.name == tname)
                 m = r_new == tgt.rid
-                if not m.any():
+                if not m.any() or tr.next_states.get(tname) is None:
                     continue
                 for k, ax in enumerate(tgt.states):
                     law = tr.next_states[tname][ax.name]

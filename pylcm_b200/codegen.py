@@ -305,6 +305,7 @@ class TargetPlan:
     w_sizes: int = -1
     w_coord: int = -1
     w_scalar: int = -1
+    unreachable: bool = False  # no law for one of the target's states
 
     @property
     def K(self) -> int:
@@ -325,6 +326,8 @@ def _target_plan(tr: TracedRegime, tgt: RegimeSpec) -> TargetPlan:
     if not tgt.states:
         return TargetPlan(tgt, True, prob, [], [], [], [], {})
     laws = tr.next_states[tgt.name]
+    if laws is None:
+        return TargetPlan(tgt, True, prob, [], [], [], [], {}, unreachable=True)
     stoch, det, cont = [], [], []
     key_deps: set = set()
     for pos, ax in enumerate(tgt.states):
@@ -423,6 +426,8 @@ class RegimeKernels:
         self.W_TASTE = take()
         self.W_ATAB = take()  # global action table (kernel a0 output) of this item
         for t in self.targets:
+            if t.unreachable:
+                continue
             if t.scalar:
                 t.w_scalar = take()
             else:
@@ -560,6 +565,8 @@ class RegimeKernels:
         ap(f"template <typename T, typename E> struct Ctx_{self.tag} {{")
         loads = []
         for ti, t in enumerate(self.targets):
+            if t.unreachable:
+                continue
             if t.scalar:
                 ap(f"  T sv{ti};")
                 loads.append(f"sv{ti} = (T)(*lcm_wp<const double>(it, {t.w_scalar}));")
@@ -664,7 +671,9 @@ class RegimeKernels:
                 else:
                     out.append(f"{{ {T} p = ({T})({pnames[ti]}); mass += p; neg = neg || (p < ({T})0);")
                     out.append("  if (p != 0) {")
-                if t.scalar:
+                if t.unreachable:
+                    out.append(f"    {T} ev = lcm_lim<{T}>::nan();")
+                elif t.scalar:
                     out.append(f"    {T} ev = C.sv{ti};")
                 else:
                     inner: list[str] = []
@@ -1081,7 +1090,8 @@ class RegimeKernels:
         spec = self.spec
         w = self.n_words
         self.SW_N, self.SW_RID_IN, self.SW_RID_OUT, self.SW_VAL, self.SW_AIDX = w, w + 1, w + 2, w + 3, w + 4
-        w += 5
+        self.SW_SEED = w + 5  # XOR-ed into the launch seed: one Philox key per item
+        w += 6
         self.SW_ACT = w
         w += len(spec.actions)
         self.SW_SIN = w
@@ -1179,7 +1189,8 @@ class RegimeKernels:
         ap(f"    const double* __restrict__ atf = lcm_wp<const double>(it, {self.W_ATAB});")
         ap(f"    const int* __restrict__ ati = reinterpret_cast<const int*>(atf + (i64){nf} * n_actions);")
         ap("    (void)period; (void)age; (void)ati; (void)PV;")
-        ap("    LcmRng rng; rng.k0 = (u32)seed; rng.k1 = (u32)(seed >> 32); rng.subject = (u32)s; rng.period = (u32)period;")
+        ap(f"    const u64 key = seed ^ (u64)it[{self.SW_SEED}];")
+        ap("    LcmRng rng; rng.k0 = (u32)key; rng.k1 = (u32)(key >> 32); rng.subject = (u32)s; rng.period = (u32)period;")
         for s_ in eP.lines:
             ap("    " + s_)
         ap(f"    double PVd[{nP}]; PVd[0] = 0.0;")
@@ -1293,6 +1304,8 @@ class RegimeKernels:
                 ap(f"    const int rid = lcm_categorical<{len(probs)}>(rp, rng.uniform(0u));")
             ap(f"    {rid_out} = rid;")
             for t in self.targets:
+                if t.unreachable:
+                    continue  # the drawn target's states stay NaN
                 ap(f"    if (rid == {t.spec.rid}) {{")
                 # scoped emitter: expressions bound inside this branch stay in it
                 et = Emitter("double", self.param_off, dict(e.vals), f"n{t.spec.rid}_")

@@ -50,6 +50,55 @@ class Launch:
     period: int
 
 
+class _Records:
+    """Item records and the launch list of a plan, concatenated into one
+    int64 item buffer and one int32 tile-prefix buffer."""
+
+    def __init__(self) -> None:
+        self.words: list[np.ndarray] = []
+        self.prefixes: list[np.ndarray] = []
+        self.launches: list[Launch] = []
+        self.w_off = 0
+        self.p_off = 0
+
+    def _prefix(self, tiles_per_item) -> tuple[int, int]:
+        pre = np.zeros(len(tiles_per_item) + 1, dtype=np.int32)
+        pre[1:] = np.cumsum(tiles_per_item)
+        off = self.p_off
+        self.prefixes.append(pre)
+        self.p_off += pre.size
+        # keep the prefix offsets 16-byte aligned for the device pointer math
+        pad = (-self.p_off) % 4
+        if pad:
+            self.prefixes.append(np.zeros(pad, dtype=np.int32))
+            self.p_off += pad
+        return off, int(pre[-1])
+
+    def add(self, kind, rk, kernel, recs, tiles_per_item, block, smem, period) -> None:
+        arr = np.stack(recs).astype(np.int64)
+        self.words.append(arr.ravel())
+        p_off, n_tiles = self._prefix(tiles_per_item)
+        self.launches.append(Launch(kind, rk, kernel, self.w_off, p_off, len(recs), n_tiles, block, smem, period))
+        self.w_off += arr.size
+
+    def add_same_records(self, kind, rk, kernel, tiles_per_item, block, smem, period) -> None:
+        """A launch over the previous launch's item records, own tiling."""
+        last = self.launches[-1]
+        p_off, n_tiles = self._prefix(tiles_per_item)
+        self.launches.append(Launch(kind, rk, kernel, last.item_off, p_off, last.n_items, n_tiles, block, smem, period))
+
+    def append(self, launch: Launch) -> None:
+        self.launches.append(launch)
+
+    def tensors(self, torch, dev):
+        words = np.concatenate(self.words) if self.words else np.zeros(1, dtype=np.int64)
+        pre = np.concatenate(self.prefixes) if self.prefixes else np.zeros(4, dtype=np.int32)
+        return (
+            torch.as_tensor(words, dtype=torch.int64, device=dev),
+            torch.as_tensor(pre, dtype=torch.int32, device=dev),
+        )
+
+
 SM_COUNT = 148
 RESIDENT_THREADS_PER_SM = 1024
 
@@ -163,6 +212,7 @@ class SolvePlan:
         self.dev = dev
         fp32 = eng.precision == "fp32"
         resolvers = [eng.resolver(p) for p in params_list]
+        self.params_list = params_list
 
         # ---- per regime: slots (active periods), V / policy buffers, grids
         self.slot: dict[str, dict[int, int]] = {}
@@ -270,145 +320,172 @@ class SolvePlan:
                 self.atab[k] = torch.empty((n, words), dtype=torch.int32, device=dev)
 
         # ---- item records
-        words: list[np.ndarray] = []
-        prefixes: list[np.ndarray] = []
-        self.launches: list[Launch] = []
         # host copies of the Bellman item records per (period, regime), reused
         # by the simulation (same layout, extended with simulation words)
         self.records: dict[tuple, tuple] = {}
-        w_off = 0
-        p_off = 0
-
-        def add_launch(kind, rk, kernel, recs, tiles_per_item, block, smem, period):
-            nonlocal w_off, p_off
-            arr = np.stack(recs).astype(np.int64)
-            pre = np.zeros(len(recs) + 1, dtype=np.int32)
-            pre[1:] = np.cumsum(tiles_per_item)
-            words.append(arr.ravel())
-            prefixes.append(pre)
-            self.launches.append(
-                Launch(kind, rk, kernel, w_off, p_off, len(recs), int(pre[-1]), block, smem, period)
-            )
-            w_off += arr.size
-            p_off += pre.size
-            # keep the prefix offsets 16-byte aligned for the device pointer math
-            pad = (-p_off) % 4
-            if pad:
-                prefixes.append(np.zeros(pad, dtype=np.int32))
-                p_off += pad
-
+        self.resolvers = resolvers
+        b = _Records()
         ages = model.ages.values
         for period, s, targets, rk in step_list:
             if not isinstance(rk, RegimeKernels):
-                self._egm_launches(rk, period, s, targets, float(ages[period]), resolvers, add_launch)
+                self._egm_launches(rk, period, s, targets, float(ages[period]), resolvers, b)
                 continue
-            age = float(ages[period])
-            pbuf = self.params[(s.name, targets)]
-            plen = pbuf.shape[1]
-            # kernel (b) launches
-            for t in rk.targets:
-                if t.scalar:
-                    continue
-                if not (t.needs_contraction or fp32):
-                    continue
-                e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
-                Vt = self.V[t.spec.name]
-                tslot = self.slot[t.spec.name][period + 1]
-                recs = []
-                for i in range(n):
-                    r = np.zeros(rk.e_words_for(t), dtype=np.int64)
-                    r[0] = Vt[i, tslot].data_ptr()
-                    r[1] = e64[i].data_ptr()
-                    r[2] = e32[i].data_ptr() if e32 is not None else 0
-                    r[3] = pbuf[i].data_ptr()
-                    r[4] = period
-                    r[5] = _f2w(age)
-                    r[6] = cblk
-                    r[7] = ncols
-                    for k, ax in enumerate(t.spec.states):
-                        r[8 + k] = ax.size
-                    recs.append(r)
-                tiles = [math.ceil(ncols / 256)] * n
-                add_launch("expect", rk, rk.expect_name(t), recs, tiles, 256, 0, period)
-            # kernel (a)
-            slot = self.slot[s.name][period]
-            recs = []
-            for i in range(n):
-                r = np.zeros(rk.n_words, dtype=np.int64)
-                r[rk.W_P] = pbuf[i].data_ptr()
-                r[rk.W_V] = self.V[s.name][i, slot].data_ptr()
-                r[rk.W_POL] = self.pol[s.name][i, slot].data_ptr()
-                r[rk.W_PERIOD] = period
-                r[rk.W_AGE] = _f2w(age)
-                r[rk.W_NSTATES] = s.n_states
-                r[rk.W_NACT] = s.n_actions
-                for k, ax in enumerate(s.states):
-                    r[rk.W_SSIZE + k] = ax.size
-                    g = self.sgrid[s.name][k]
-                    r[rk.W_SGRID + k] = g.data_ptr() if g is not None else 0
-                for k, ax in enumerate(s.actions):
-                    r[rk.W_ASIZE + k] = ax.size
-                    g = self.agrid[s.name][k]
-                    r[rk.W_AGRID + k] = g.data_ptr() if g is not None else 0
-                r[rk.W_TASTE] = _f2w(rk.tr.taste_scale if rk.tr.taste_scale else 0.0)
-                r[rk.W_ATAB] = self.atab[(s.name, targets)][i].data_ptr()
-                if s.taste_shocks:
-                    r[rk.W_TASTE] = _f2w(resolvers[i].taste_scale(s.name))
-                for t in rk.targets:
-                    tV = self.V[t.spec.name]
-                    tslot = self.slot[t.spec.name][period + 1]
-                    if t.scalar:
-                        r[t.w_scalar] = tV[i, tslot].data_ptr()
-                        continue
-                    if t.needs_contraction or fp32:
-                        e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
-                        r[t.w_ev64] = e64[i].data_ptr()
-                        r[t.w_ev32] = e32[i].data_ptr() if e32 is not None else 0
-                    else:
-                        r[t.w_ev64] = tV[i, tslot].data_ptr()
-                        r[t.w_ev32] = 0
-                    for k, ax in enumerate(t.spec.states):
-                        r[t.w_sizes + k] = ax.size
-                    for ci, pos in enumerate(t.cont_pos):
-                        ax = t.spec.states[pos]
-                        kind, a, b, npts = ax.grid.coordinate_spec()
-                        base = t.w_coord + 3 * ci
-                        if kind == "lin":
-                            r[base] = _f2w(a)
-                            r[base + 1] = _f2w(1.0 / b if npts > 1 else 0.0)
-                        elif kind == "log":
-                            r[base] = _f2w(a)
-                            r[base + 1] = _f2w(b)
-                        else:
-                            r[base + 2] = self.sgrid[t.spec.name][pos].data_ptr()
-                recs.append(r)
-            spt = rk.cfg.states_per_tile
-            tiles = [math.ceil(s.n_states / spt)] * n
-            self.records[(period, s.name)] = (rk, np.stack(recs).astype(np.int64))
-            add_launch("atab", rk, rk.atab_name(), recs, [math.ceil(s.n_actions / 256)] * n, 256, 0, period)
-            # kernel (a) reads the same records
-            self.launches.append(
-                Launch("bellman", rk, rk.bellman_name(), self.launches[-1].item_off, p_off, n,
-                       int(sum(tiles)), rk.cfg.block, rk.smem_bytes, period)
-            )
-            pre = np.zeros(n + 1, dtype=np.int32)
-            pre[1:] = np.cumsum(tiles)
-            prefixes.append(pre)
-            p_off += pre.size
-            pad = (-p_off) % 4
-            if pad:
-                prefixes.append(np.zeros(pad, dtype=np.int32))
-                p_off += pad
-
-        self.items = torch.as_tensor(np.concatenate(words), dtype=torch.int64, device=dev)
-        self.prefix = torch.as_tensor(np.concatenate(prefixes), dtype=torch.int32, device=dev)
+            self._gs_launches(b, rk, period, s, targets, (s.name, targets))
+        self.launches = b.launches
+        self.items, self.prefix = b.tensors(torch, dev)
         for rk in {id(l.module): l.module for l in self.launches if l.kind != "fues"}.values():
             eng.module(rk)
         self.graph = None
         self._prepared = None
+        # grid-search records of endogenous-grid regimes (simulation only)
+        self.sim_launches: list[Launch] = []
+        self._sim_prepared = None
+        self._egm_steps = [(p_, s_, t_) for p_, s_, t_, _ in egm_steps]
+
+    def _gs_launches(self, b: "_Records", rk: RegimeKernels, period: int, s: RegimeSpec, targets, pkey) -> None:
+        """Kernel (b) and (a0, a) records and launches of one grid-search step."""
+        n = self.n
+        fp32 = self.eng.precision == "fp32"
+        resolvers = self.resolvers
+        age = float(self.eng.model.ages.values[period])
+        pbuf = self.params[pkey]
+        # kernel (b) launches
+        for t in rk.targets:
+            if t.scalar:
+                continue
+            if not (t.needs_contraction or fp32):
+                continue
+            e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
+            Vt = self.V[t.spec.name]
+            tslot = self.slot[t.spec.name][period + 1]
+            recs = []
+            for i in range(n):
+                r = np.zeros(rk.e_words_for(t), dtype=np.int64)
+                r[0] = Vt[i, tslot].data_ptr()
+                r[1] = e64[i].data_ptr()
+                r[2] = e32[i].data_ptr() if e32 is not None else 0
+                r[3] = pbuf[i].data_ptr()
+                r[4] = period
+                r[5] = _f2w(age)
+                r[6] = cblk
+                r[7] = ncols
+                for k, ax in enumerate(t.spec.states):
+                    r[8 + k] = ax.size
+                recs.append(r)
+            tiles = [math.ceil(ncols / 256)] * n
+            b.add("expect", rk, rk.expect_name(t), recs, tiles, 256, 0, period)
+        # kernel (a)
+        slot = self.slot[s.name][period]
+        recs = []
+        for i in range(n):
+            r = np.zeros(rk.n_words, dtype=np.int64)
+            r[rk.W_P] = pbuf[i].data_ptr()
+            r[rk.W_V] = self.V[s.name][i, slot].data_ptr()
+            r[rk.W_POL] = self.pol[s.name][i, slot].data_ptr()
+            r[rk.W_PERIOD] = period
+            r[rk.W_AGE] = _f2w(age)
+            r[rk.W_NSTATES] = s.n_states
+            r[rk.W_NACT] = s.n_actions
+            for k, ax in enumerate(s.states):
+                r[rk.W_SSIZE + k] = ax.size
+                g = self.sgrid[s.name][k]
+                r[rk.W_SGRID + k] = g.data_ptr() if g is not None else 0
+            for k, ax in enumerate(s.actions):
+                r[rk.W_ASIZE + k] = ax.size
+                g = self.agrid[s.name][k]
+                r[rk.W_AGRID + k] = g.data_ptr() if g is not None else 0
+            r[rk.W_TASTE] = _f2w(rk.tr.taste_scale if rk.tr.taste_scale else 0.0)
+            r[rk.W_ATAB] = self.atab[(s.name, targets)][i].data_ptr()
+            if s.taste_shocks:
+                r[rk.W_TASTE] = _f2w(resolvers[i].taste_scale(s.name))
+            for t in rk.targets:
+                if t.unreachable:
+                    continue
+                tV = self.V[t.spec.name]
+                tslot = self.slot[t.spec.name][period + 1]
+                if t.scalar:
+                    r[t.w_scalar] = tV[i, tslot].data_ptr()
+                    continue
+                if t.needs_contraction or fp32:
+                    e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
+                    r[t.w_ev64] = e64[i].data_ptr()
+                    r[t.w_ev32] = e32[i].data_ptr() if e32 is not None else 0
+                else:
+                    r[t.w_ev64] = tV[i, tslot].data_ptr()
+                    r[t.w_ev32] = 0
+                for k, ax in enumerate(t.spec.states):
+                    r[t.w_sizes + k] = ax.size
+                for ci, pos in enumerate(t.cont_pos):
+                    ax = t.spec.states[pos]
+                    kind, a, bb, npts = ax.grid.coordinate_spec()
+                    base = t.w_coord + 3 * ci
+                    if kind == "lin":
+                        r[base] = _f2w(a)
+                        r[base + 1] = _f2w(1.0 / bb if npts > 1 else 0.0)
+                    elif kind == "log":
+                        r[base] = _f2w(a)
+                        r[base + 1] = _f2w(bb)
+                    else:
+                        r[base + 2] = self.sgrid[t.spec.name][pos].data_ptr()
+            recs.append(r)
+        spt = rk.cfg.states_per_tile
+        tiles = [math.ceil(s.n_states / spt)] * n
+        self.records[(period, s.name)] = (rk, np.stack(recs).astype(np.int64))
+        b.add("atab", rk, rk.atab_name(), recs, [math.ceil(s.n_actions / 256)] * n, 256, 0, period)
+        # kernel (a) reads the same records
+        b.add_same_records("bellman", rk, rk.bellman_name(), tiles, rk.cfg.block, rk.smem_bytes, period)
+
+    def ensure_sim_records(self) -> None:
+        """Grid-search records of the endogenous-grid regimes.
+
+        The simulate phase decides a DC-EGM regime's actions by the grid
+        argmax of Q over its action grid (with the intrinsic budget mask)
+        against the solved value functions, like a brute-force regime
+        (``src/_lcm/simulation/simulate.py:671-770``: the off-grid policy
+        read is disabled for every shipped envelope,
+        ``src/_lcm/regime_building/processing.py:1662-1699, 1765-1800``).
+        Their expectation / action-table launches run only before a
+        simulated period, never in the solve.
+        """
+        if self.sim_launches or not self._egm_steps:
+            return
+        torch = self.torch
+        eng = self.eng
+        n = self.n
+        dev = self.dev
+        fp32 = eng.precision == "fp32"
+        b = _Records()
+        for period, s, targets in self._egm_steps:
+            rk = eng.kernels(s, targets, self.params_list[0], n)
+            pkey = (s.name, targets, "gs")
+            if pkey not in self.params:
+                vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in self.resolvers]
+                self.params[pkey] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+            for t in rk.targets:
+                if t.scalar or not (t.needs_contraction or fp32):
+                    continue
+                k = (s.name, targets, t.spec.name)
+                if k not in self.ev:
+                    cblk = int(np.prod([t.spec.states[p].size for p in t.cont_pos])) if t.cont_pos else 1
+                    ncols = int(np.prod([t.spec.states[p].size for p in t.det_pos])) * cblk if t.det_pos else cblk
+                    e64 = torch.empty((n, t.K, ncols), dtype=torch.float64, device=dev)
+                    e32 = torch.empty((n, t.K, ncols), dtype=torch.float32, device=dev) if fp32 else None
+                    self.ev[k] = (e64, e32, ncols, cblk)
+            k = (s.name, targets)
+            if k not in self.atab:
+                words = max(1, rk.atab_words) * s.n_actions
+                words += words % 2
+                self.atab[k] = torch.empty((n, words), dtype=torch.int32, device=dev)
+            self._gs_launches(b, rk, period, s, targets, pkey)
+        # only the inputs of the simulation: drop the Bellman launches
+        b.launches = [l for l in b.launches if l.kind != "bellman"]
+        self.sim_launches = b.launches
+        self.sim_items, self.sim_prefix = b.tensors(torch, dev)
+        for rk in {id(l.module): l.module for l in self.sim_launches}.values():
+            eng.module(rk)
 
     # ------------------------------------------------------------- DC-EGM
-    def _egm_launches(self, ek, period, s, targets, age, resolvers, add_launch) -> None:
+    def _egm_launches(self, ek, period, s, targets, age, resolvers, rec: "_Records") -> None:
         """Records and launches of one DC-EGM period: candidates (c1), FUES,
         carry marginal utilities, publication on the state grid."""
         n = self.n
@@ -457,8 +534,9 @@ class SolvePlan:
         cname, uname, pname = ek.names()
         nrow, npad, ncand = b["nrow"], b["npad"], b["ncand"]
         ns = nrow // er.n_disc_actions
+        add_launch = rec.add
         add_launch("egm", ek, cname, recs, [math.ceil(nrow * len(er.savings) / 256)] * n, 256, 0, period)
-        self.launches.append(
+        rec.append(
             Launch("fues", ("fues", s.name, slot, er.jump_thresh), "lcmx_fues_scan", 0, 0, n * nrow, 0, 0, 0, period)
         )
         add_launch("egm", ek, uname, recs, [math.ceil(nrow * npad / 256)] * n, 256, 0, period)
@@ -482,11 +560,13 @@ class SolvePlan:
         return launch
 
     # ---------------------------------------------------------------- run
-    def _prepare(self) -> list:
-        ib = self.items.data_ptr()
-        pb = self.prefix.data_ptr()
+    def _prepare(self, launches=None, items=None, prefix=None) -> list:
+        if launches is None:
+            launches, items, prefix = self.launches, self.items, self.prefix
+        ib = items.data_ptr()
+        pb = prefix.data_ptr()
         out = []
-        for l in self.launches:
+        for l in launches:
             if l.kind == "fues":
                 _, name, slot, thr = l.module
                 out.append(self._fues_launch(name, slot, thr))
@@ -515,6 +595,12 @@ class SolvePlan:
         for l, launch in zip(self.launches, self._prepared):
             if l.period == period and l.kind in ("expect", "atab"):
                 launch(stream)
+        if self.sim_launches:
+            if self._sim_prepared is None:
+                self._sim_prepared = self._prepare(self.sim_launches, self.sim_items, self.sim_prefix)
+            for l, launch in zip(self.sim_launches, self._sim_prepared):
+                if l.period == period:
+                    launch(stream)
 
     def capture(self) -> None:
         """Capture the launch list in a CUDA graph (replayed by run_graph)."""

@@ -101,9 +101,16 @@ def _initial_arrays(model, initial_conditions: Mapping) -> tuple[np.ndarray, dic
 
 
 class SimPlan:
-    """Device buffers and launches of one simulation (one solve instance)."""
+    """Device buffers and launches of the simulations of solve instances.
 
-    def __init__(self, solve_plan, initial_conditions: Mapping, seed: int) -> None:
+    `instances` lists (solve-plan instance, initial conditions, seed): one
+    kernel (d) launch per (period, regime) covers every listed instance, each
+    with its own subjects, buffers and seed (the Philox key of an item is the
+    launch seed XOR the item's seed word; the launch seed is 0 here).
+    """
+
+    def __init__(self, solve_plan, initial_conditions: Mapping | None = None, seed: int = 0,
+                 instances: list | None = None) -> None:
         import torch
 
         self.torch = torch
@@ -113,56 +120,77 @@ class SimPlan:
         specs = eng.specs
         T = model.n_periods
         dev = solve_plan.dev
-        rid0, states0 = _initial_arrays(model, initial_conditions)
-        N = rid0.shape[0]
-        self.N, self.T, self.seed = N, T, int(seed) & 0xFFFFFFFFFFFFFFFF
+        if instances is None:
+            instances = [(0, initial_conditions, seed)]
+        solve_plan.ensure_sim_records()
+        self.T = T
         names = sorted({a.name for s in specs for a in s.states})
         anames = sorted({a.name for s in specs for a in s.actions})
-        for s in specs:
-            for a in s.states:
-                if a.name not in states0 and (rid0 == s.rid).any():
-                    raise InvalidParamsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
         nan = float("nan")
-        self.S = {n: torch.full((T + 1, N), nan, dtype=torch.float64, device=dev) for n in names}
-        for n, v in states0.items():
-            if n in self.S:
-                self.S[n][0] = torch.as_tensor(v, device=dev)
-        self.R = torch.full((T + 1, N), -1, dtype=torch.int32, device=dev)
-        self.R[0] = torch.as_tensor(rid0, dtype=torch.int32, device=dev)
-        self.val = torch.full((T, N), nan, dtype=torch.float64, device=dev)
-        self.aidx = torch.zeros((T, N), dtype=torch.int32, device=dev)
-        self.A = {n: torch.full((T, N), nan, dtype=torch.float64, device=dev) for n in anames}
-        # item records: the Bellman record of (period, regime) + simulation words
+        self.inst = []
+        for idx, ic, sd in instances:
+            if not 0 <= idx < solve_plan.n:
+                raise InvalidParamsError(f"instance {idx} outside the solve plan's batch of {solve_plan.n}")
+            rid0, states0 = _initial_arrays(model, ic)
+            N = rid0.shape[0]
+            for s in specs:
+                for a in s.states:
+                    if a.name not in states0 and (rid0 == s.rid).any():
+                        raise InvalidParamsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
+            b = {
+                "idx": idx,
+                "N": N,
+                "seed": int(sd) & 0xFFFFFFFFFFFFFFFF,
+                "S": {n: torch.full((T + 1, N), nan, dtype=torch.float64, device=dev) for n in names},
+                "R": torch.full((T + 1, N), -1, dtype=torch.int32, device=dev),
+                "val": torch.full((T, N), nan, dtype=torch.float64, device=dev),
+                "aidx": torch.zeros((T, N), dtype=torch.int32, device=dev),
+                "A": {n: torch.full((T, N), nan, dtype=torch.float64, device=dev) for n in anames},
+            }
+            for n, v in states0.items():
+                if n in b["S"]:
+                    b["S"][n][0] = torch.as_tensor(v, device=dev)
+            b["R"][0] = torch.as_tensor(rid0, dtype=torch.int32, device=dev)
+            self.inst.append(b)
+        # item records: the Bellman record of (period, regime, instance) + simulation words
         recs = []
+        prefs = []
         self.launches = []
         off = 0
+        poff = 0
         for period in range(T):
             for s in specs:
                 if period not in s.active_periods:
                     continue
                 rk, base = solve_plan.records[(period, s.name)]
                 eng.module(rk)
-                r = np.zeros(rk.sim_words, dtype=np.int64)
-                r[: rk.n_words] = base[0]
-                r[rk.SW_N] = N
-                r[rk.SW_RID_IN] = self.R[period].data_ptr()
-                r[rk.SW_RID_OUT] = self.R[period + 1].data_ptr()
-                r[rk.SW_VAL] = self.val[period].data_ptr()
-                r[rk.SW_AIDX] = self.aidx[period].data_ptr()
-                for k, a in enumerate(s.actions):
-                    r[rk.SW_ACT + k] = self.A[a.name][period].data_ptr()
-                for k, a in enumerate(s.states):
-                    r[rk.SW_SIN + k] = self.S[a.name][period].data_ptr()
-                for k, name in enumerate(rk.sim_out_names):
-                    r[rk.SW_SOUT + k] = self.S[name][period + 1].data_ptr()
-                recs.append(r)
-                self.launches.append((period, rk, off, math.ceil(N / 8)))
-                off += r.size
+                tiles = []
+                for b in self.inst:
+                    r = np.zeros(rk.sim_words, dtype=np.int64)
+                    r[: rk.n_words] = base[b["idx"]]
+                    r[rk.SW_N] = b["N"]
+                    r[rk.SW_RID_IN] = b["R"][period].data_ptr()
+                    r[rk.SW_RID_OUT] = b["R"][period + 1].data_ptr()
+                    r[rk.SW_VAL] = b["val"][period].data_ptr()
+                    r[rk.SW_AIDX] = b["aidx"][period].data_ptr()
+                    r[rk.SW_SEED] = np.uint64(b["seed"]).astype(np.int64)
+                    for k, a in enumerate(s.actions):
+                        r[rk.SW_ACT + k] = b["A"][a.name][period].data_ptr()
+                    for k, a in enumerate(s.states):
+                        r[rk.SW_SIN + k] = b["S"][a.name][period].data_ptr()
+                    for k, name in enumerate(rk.sim_out_names):
+                        r[rk.SW_SOUT + k] = b["S"][name][period + 1].data_ptr()
+                    recs.append(r)
+                    tiles.append(math.ceil(b["N"] / 8))
+                pre = np.zeros(len(tiles) + 1, dtype=np.int32)
+                pre[1:] = np.cumsum(tiles)
+                pad = (-pre.size) % 4
+                prefs.append(np.concatenate([pre, np.zeros(pad, dtype=np.int32)]))
+                self.launches.append((period, rk, off, poff, len(self.inst), int(pre[-1])))
+                off += rk.sim_words * len(self.inst)
+                poff += pre.size + pad
         self.items = torch.as_tensor(np.concatenate(recs), dtype=torch.int64, device=dev)
-        pref = []
-        for _, _, _, tiles in self.launches:
-            pref.append(np.array([0, tiles, 0, 0], dtype=np.int32))
-        self.prefix = torch.as_tensor(np.concatenate(pref), dtype=torch.int32, device=dev)
+        self.prefix = torch.as_tensor(np.concatenate(prefs), dtype=torch.int32, device=dev)
 
     def run(self, stream: int | None = None) -> None:
         torch = self.torch
@@ -170,24 +198,25 @@ class SimPlan:
             stream = torch.cuda.current_stream(self.plan.dev).cuda_stream
         ib, pb = self.items.data_ptr(), self.prefix.data_ptr()
         done_inputs = set()
-        for k, (period, rk, off, tiles) in enumerate(self.launches):
+        for period, rk, off, poff, n_items, tiles in self.launches:
             if period not in done_inputs:
                 self.plan.run_period_inputs(period, stream)
                 done_inputs.add(period)
-            rk.module.simulate(rk.sim_name(), ib + 8 * off, pb + 16 * k, 1, tiles, 256, 0, self.seed, stream)
+            rk.module.simulate(rk.sim_name(), ib + 8 * off, pb + 4 * poff, n_items, tiles, 256, 0, 0, stream)
 
     @property
     def gpu_launches(self) -> int:
         return len(self.launches)
 
-    def result(self, model) -> SimulationResult:
+    def result(self, model, k: int = 0) -> SimulationResult:
         torch = self.torch
         torch.cuda.current_stream(self.plan.dev).synchronize()
+        b = self.inst[k]
         periods = {}
-        R = self.R.cpu().numpy()
-        V = self.val.cpu().numpy()
-        S = {n: v.cpu().numpy() for n, v in self.S.items()}
-        A = {n: v.cpu().numpy() for n, v in self.A.items()}
+        R = b["R"].cpu().numpy()
+        V = b["val"].cpu().numpy()
+        S = {n: v.cpu().numpy() for n, v in b["S"].items()}
+        A = {n: v.cpu().numpy() for n, v in b["A"].items()}
         for p in range(self.T):
             periods[p] = {
                 "regime_id": R[p],

@@ -466,6 +466,33 @@ def _as_bool(e: Any) -> ir.Expr:
     return e
 
 
+def _unreachable(spec: RegimeSpec, tgt: RegimeSpec) -> bool:
+    """True when `spec` has no law of motion for one of `tgt`'s states."""
+    src = {a.name for a in spec.states}
+    for ax in tgt.states:
+        if ax.name in src:
+            continue
+        if ax.kind == "process" or f"next_{ax.name}" not in spec.functions:
+            return True
+    return False
+
+
+def _intrinsic_budget(spec: RegimeSpec, t: "_Tracer") -> ir.Expr | None:
+    """The budget mask an endogenous-grid regime's grid argmax (simulation)
+    needs: continuous action <= resources - lowest savings node
+    (``src/_lcm/egm/budget.py:36-100``,
+    ``src/_lcm/regime_building/processing.py:1517-1545``)."""
+    from pylcm_b200.solvers import DCEGM
+
+    if not isinstance(spec.solver, DCEGM) or spec.terminal:
+        return None
+    liq = spec.user.liquid
+    lb = float(np.asarray(spec.solver.savings_grid.to_numpy(), dtype=np.float64)[0])
+    res = t.resolve_arg("utility", liq.resources, inspect.Parameter.empty)
+    c = ir.var("action", liq.action, "f")
+    return ir._cmp("<=", c, ir.const(res) - lb)
+
+
 def trace_regime(
     spec: RegimeSpec,
     all_specs: list[RegimeSpec],
@@ -481,6 +508,9 @@ def trace_regime(
     F: ir.Expr = ir.const(True)
     for c in spec.constraint_names:
         F = ir.logical("and", F, _as_bool(t.trace(c)))
+    budget = _intrinsic_budget(spec, t)
+    if budget is not None:
+        F = ir.logical("and", F, budget)
     # process tables (node values, transition matrix) enter the parameter vector
     process_tables = {}
     for ax in spec.states:
@@ -524,6 +554,12 @@ def trace_regime(
         by_name = {s.name: s for s in all_specs}
         for tname in targets:
             tgt = by_name[tname]
+            if _unreachable(spec, tgt):
+                # the source has no law for one of the target's states: it
+                # cannot move there; a non-zero probability toward it poisons
+                # the continuation (NaN)
+                next_states[tname] = None
+                continue
             laws: dict[str, NextState] = {}
             for ax in tgt.states:
                 if ax.kind == "process":
