@@ -58,6 +58,8 @@ class _Records:
         self.words: list[np.ndarray] = []
         self.prefixes: list[np.ndarray] = []
         self.launches: list[Launch] = []
+        # per launch: (records, tiles per item), None for a launch without records
+        self.host: list[tuple | None] = []
         self.w_off = 0
         self.p_off = 0
 
@@ -79,6 +81,7 @@ class _Records:
         self.words.append(arr.ravel())
         p_off, n_tiles = self._prefix(tiles_per_item)
         self.launches.append(Launch(kind, rk, kernel, self.w_off, p_off, len(recs), n_tiles, block, smem, period))
+        self.host.append((arr, list(tiles_per_item)))
         self.w_off += arr.size
 
     def add_same_records(self, kind, rk, kernel, tiles_per_item, block, smem, period) -> None:
@@ -86,9 +89,11 @@ class _Records:
         last = self.launches[-1]
         p_off, n_tiles = self._prefix(tiles_per_item)
         self.launches.append(Launch(kind, rk, kernel, last.item_off, p_off, last.n_items, n_tiles, block, smem, period))
+        self.host.append((self.host[-1][0], list(tiles_per_item)))
 
     def append(self, launch: Launch) -> None:
         self.launches.append(launch)
+        self.host.append(None)
 
     def tensors(self, torch, dev):
         words = np.concatenate(self.words) if self.words else np.zeros(1, dtype=np.int64)
@@ -196,7 +201,7 @@ class SolveEngine:
 class SolvePlan:
     """Buffers, item records and the launch list for a batch of instances."""
 
-    def __init__(self, eng: SolveEngine, params_list: list) -> None:
+    def __init__(self, eng: SolveEngine, params_list: list, upload: bool = True) -> None:
         import torch
 
         self.eng = eng
@@ -332,9 +337,11 @@ class SolvePlan:
                 continue
             self._gs_launches(b, rk, period, s, targets, (s.name, targets))
         self.launches = b.launches
-        self.items, self.prefix = b.tensors(torch, dev)
+        self._rec = b
         for rk in {id(l.module): l.module for l in self.launches if l.kind != "fues"}.values():
             eng.module(rk)
+        if upload:
+            self.items, self.prefix = b.tensors(torch, dev)
         self.graph = None
         self._prepared = None
         # grid-search records of endogenous-grid regimes (simulation only)
@@ -435,7 +442,7 @@ class SolvePlan:
         # kernel (a) reads the same records
         b.add_same_records("bellman", rk, rk.bellman_name(), tiles, rk.cfg.block, rk.smem_bytes, period)
 
-    def ensure_sim_records(self) -> None:
+    def ensure_sim_records(self, upload: bool = True) -> None:
         """Grid-search records of the endogenous-grid regimes.
 
         The simulate phase decides a DC-EGM regime's actions by the grid
@@ -449,6 +456,7 @@ class SolvePlan:
         """
         if self.sim_launches or not self._egm_steps:
             return
+        self._sim_upload = upload
         torch = self.torch
         eng = self.eng
         n = self.n
@@ -478,11 +486,19 @@ class SolvePlan:
                 self.atab[k] = torch.empty((n, words), dtype=torch.int32, device=dev)
             self._gs_launches(b, rk, period, s, targets, pkey)
         # only the inputs of the simulation: drop the Bellman launches
-        b.launches = [l for l in b.launches if l.kind != "bellman"]
+        keep = [k for k, l in enumerate(b.launches) if l.kind != "bellman"]
+        b.launches = [b.launches[k] for k in keep]
+        b.host = [b.host[k] for k in keep]
         self.sim_launches = b.launches
-        self.sim_items, self.sim_prefix = b.tensors(torch, dev)
+        self._sim_rec = b
+        if upload:
+            self.sim_items, self.sim_prefix = b.tensors(torch, dev)
         for rk in {id(l.module): l.module for l in self.sim_launches}.values():
             eng.module(rk)
+
+    def instance(self, idx: int):
+        """(engine, Bellman records per (period, regime), row) of instance `idx`."""
+        return self.eng, self.records, idx
 
     # ------------------------------------------------------------- DC-EGM
     def _egm_launches(self, ek, period, s, targets, age, resolvers, rec: "_Records") -> None:
@@ -633,3 +649,129 @@ class SolvePlan:
                 V.setdefault(period, {})[s.name] = self.V[s.name][i, k].reshape(shape)
                 P.setdefault(period, {})[s.name] = self.pol[s.name][i, k].reshape(shape)
         return dict(sorted(V.items())), dict(sorted(P.items()))
+
+
+class BatchPlan:
+    """Instances of different models of one family in one launch per kernel.
+
+    A family is a set of models whose regimes generate the same kernels:
+    the same functions and state / action structure, with grid sizes,
+    horizons (T) and parameters free per instance -- they are item words.
+    Each instance gets its own buffers (a one-instance plan); the launches
+    of all instances are merged:
+
+    - the solve aligns instances by steps from the end (step k is period
+      T_i - 1 - k of instance i) and, within a step, merges the i-th launch
+      of every instance by kernel: one launch per (step, position, kernel)
+      covers every instance with its own tiles;
+    - the simulation inputs (expectation and action tables of a period) are
+      merged by (period, position, kernel) the same way.
+
+    The upper-envelope scan (kernel c's FUES stage) runs per instance.
+    """
+
+    def __init__(self, members: Sequence) -> None:
+        import torch
+
+        self.torch = torch
+        if not members:
+            raise ValueError("empty batch")
+        self.plans = [SolvePlan(eng, [p], upload=False) for eng, p in members]
+        self.n = len(self.plans)
+        self.dev = self.plans[0].dev
+        self.launches, self.items, self.prefix = self._merge(
+            [(pl, pl._rec, pl.launches, lambda l, pl=pl: pl.eng.model.n_periods - 1 - l.period) for pl in self.plans]
+        )
+        self._prepared = None
+        self._inputs = None
+
+    def _merge(self, sources):
+        """Merge per-instance launch lists by (key, position within key, kernel)."""
+        by_key: dict[int, list] = {}
+        for pl, rec, launches, key_of in sources:
+            seq: dict[int, list] = {}
+            for l, h in zip(launches, rec.host):
+                seq.setdefault(key_of(l), []).append((pl, l, h))
+            for k, lst in seq.items():
+                by_key.setdefault(k, []).append(lst)
+        b = _Records()
+        for k in sorted(by_key):
+            lists = by_key[k]
+            depth = max(len(x) for x in lists)
+            for j in range(depth):
+                groups: dict[tuple, list] = {}
+                for lst in lists:
+                    if j >= len(lst):
+                        continue
+                    pl, l, h = lst[j]
+                    if l.kind == "fues":
+                        b.append(Launch("fues", (pl,) + tuple(l.module[1:]), l.kernel, 0, 0, l.n_items, 0, 0, 0, k))
+                        continue
+                    gk = (l.kind, l.kernel, l.module.key if hasattr(l.module, "key") else id(l.module))
+                    groups.setdefault(gk, []).append((l, h))
+                for gk, members in groups.items():
+                    l0 = members[0][0]
+                    recs = [row for _, h in members for row in h[0]]
+                    tiles = [t for _, h in members for t in h[1]]
+                    b.add(l0.kind, l0.module, l0.kernel, recs, tiles, l0.block, l0.smem, k)
+        items, prefix = b.tensors(self.torch, self.dev)
+        return b.launches, items, prefix
+
+    def _prepare(self, launches, items, prefix) -> list:
+        ib = items.data_ptr()
+        pb = prefix.data_ptr()
+        out = []
+        for l in launches:
+            if l.kind == "fues":
+                pl, name, slot, thr = l.module
+                out.append(pl._fues_launch(name, slot, thr))
+                continue
+            out.append(
+                l.module.module.prepared(
+                    l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem
+                )
+            )
+        return out
+
+    def run(self, stream: int | None = None) -> None:
+        if stream is None:
+            stream = self.torch.cuda.current_stream(self.dev).cuda_stream
+        if self._prepared is None:
+            self._prepared = self._prepare(self.launches, self.items, self.prefix)
+        for launch in self._prepared:
+            launch(stream)
+
+    @property
+    def gpu_launches(self) -> int:
+        return len(self.launches)
+
+    # -------------------------------------------------------- simulation
+    def ensure_sim_records(self) -> None:
+        if self._inputs is not None:
+            return
+        sources = []
+        for pl in self.plans:
+            pl.ensure_sim_records(upload=False)
+            keep = [(l, h) for l, h in zip(pl.launches, pl._rec.host) if l.kind in ("expect", "atab")]
+            rec = _Records()
+            rec.launches = [l for l, _ in keep]
+            rec.host = [h for _, h in keep]
+            sources.append((pl, rec, rec.launches, lambda l: l.period))
+            if pl.sim_launches:
+                sources.append((pl, pl._sim_rec, pl.sim_launches, lambda l: l.period))
+        launches, items, prefix = self._merge(sources)
+        self._inputs = (launches, items, prefix, self._prepare(launches, items, prefix))
+
+    def run_period_inputs(self, period: int, stream: int) -> None:
+        self.ensure_sim_records()
+        launches, _, _, prepared = self._inputs
+        for l, launch in zip(launches, prepared):
+            if l.period == period:
+                launch(stream)
+
+    def instance(self, idx: int):
+        pl = self.plans[idx]
+        return pl.eng, pl.records, 0
+
+    def result(self, i: int) -> tuple[dict, dict]:
+        return self.plans[i].result(0)

@@ -1,0 +1,323 @@
+"""Serving: continuous batching of solve+simulate requests on one GPU.
+
+The reference has no serving layer; its unit of work is one
+``model.solve(params)`` followed by ``model.simulate(...)``
+(``src/lcm/model.py:440-519, 648-848``) -- the inner loop of a
+simulated-moments estimation.  This module runs a stream of such requests:
+
+- a request names a model, a parameter set, the initial conditions of the
+  simulated subjects and a seed; its model family groups the requests whose
+  kernels are the same (grid sizes, horizons and parameters are item words
+  and may differ within a family);
+- requests that arrive while others run wait in per-family queues; when one
+  of the server's CUDA streams is free, the family whose oldest request has
+  waited longest is batched -- every waiting request of it, up to
+  `max_batch` -- into one job: one heterogeneous solve plan over the batch
+  (one launch per (step, kernel) covers every instance, whatever its grid
+  sizes and horizon) and one simulation plan over it;
+- a job is admitted only when its HBM footprint (value and policy arrays of
+  all periods, expectation and action tables, DC-EGM carry rows, simulation
+  buffers) fits the budget left by the jobs in flight; otherwise it waits
+  for memory to free up;
+- jobs on different streams overlap on the device; a job's result (per
+  period simulated moments, optionally the value functions) is copied to
+  pinned host memory on its stream and the request completes when the host
+  sees the job's event.
+
+A request's numbers do not depend on the batch it lands in: each instance
+has its own item records, the launch shape of a family is pinned, and the
+simulation's counter RNG is keyed by the request's seed and indexed by
+subject and period.
+"""
+
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+from typing import Any, Hashable, Mapping, Sequence
+
+import numpy as np
+
+from pylcm_b200.engine import LaunchConfig, SolveEngine
+
+
+@dataclasses.dataclass
+class Request:
+    """One solve+simulate request.
+
+    `family` groups requests that may share a job: models whose regimes
+    generate the same kernels (same functions and state / action structure;
+    grid sizes, horizon and parameters may differ).  `key` names the model
+    itself (requests with equal keys share one model object and engine).
+    """
+
+    family: Hashable
+    key: Hashable
+    model: Any
+    params: Mapping
+    initial_conditions: Mapping
+    seed: int = 0
+    arrival: float = 0.0  # seconds after the start of the request stream
+    rid: int = 0
+    return_V: bool = False
+
+
+@dataclasses.dataclass
+class Result:
+    rid: int
+    family: Hashable
+    moments: dict  # name -> (T,) per-period mean over the simulated subjects
+    V: dict | None  # {period: {regime: array}} when requested
+    arrival: float
+    admitted: float
+    finished: float
+    batch_size: int
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def footprint_bytes(eng: SolveEngine, n_agents: int) -> int:
+    """HBM bytes one solve+simulate instance of `eng`'s model holds.
+
+    T x states value (float64) and policy (int32) arrays per regime, the
+    expectation tables (float64, plus float32 copies in the single-precision
+    search), the action tables, the DC-EGM carry rows and candidates, and
+    the simulation's per-period subject arrays.
+    """
+    from pylcm_b200.egm import is_egm
+
+    model = eng.model
+    specs = eng.specs
+    T = model.n_periods
+    fp32 = eng.precision == "fp32"
+    b = 0
+    for s in specs:
+        slots = max(len(s.active_periods), 1)
+        b += slots * s.n_states * (8 + 4)
+        if is_egm(s) and not s.terminal:
+            n_rows = 1
+            for a in s.states + s.actions:
+                if a.kind != "continuous":
+                    n_rows *= a.size
+            solver = s.solver
+            n_cand = int(solver.n_constrained_points) + len(solver.savings_grid.to_numpy())
+            n_pad = int(np.ceil(solver.refined_grid_factor * n_cand))
+            b += slots * n_rows * (4 * n_pad * 8 + 4)  # refined grid, policy, value, u'(c); counts
+            b += n_rows * n_cand * 8 * 4 * 2  # candidates + envelope workspace
+        # expectation tables of the targets (at most one per target and target set)
+        for t in specs:
+            if t.states and not s.terminal:
+                b += t.n_states * (8 + (4 if fp32 else 0))
+        b += 4 * s.n_actions * 4  # action table
+    names = sorted({a.name for s in specs for a in s.states})
+    anames = sorted({a.name for s in specs for a in s.actions})
+    b += n_agents * (T + 1) * (8 * len(names) + 4)
+    b += n_agents * T * (8 + 4 + 8 * len(anames))
+    return int(b)
+
+
+class _Job:
+    def __init__(self, family, reqs, stream, plan, sim, host, event, nbytes, admitted, v_host, lengths) -> None:
+        self.family, self.reqs, self.stream = family, reqs, stream
+        self.lengths = lengths
+        self.plan, self.sim, self.host, self.event = plan, sim, host, event
+        self.nbytes, self.admitted, self.v_host = nbytes, admitted, v_host
+
+
+class Server:
+    """Continuous-batching solve+simulate server on one GPU.
+
+    precision -- "fp32" (single-precision search, double-precision values;
+                 the fast form) or "fp64" (the plain form);
+    max_batch -- most requests of one family per job;
+    n_streams -- jobs in flight at once;
+    hbm_budget_bytes -- admission budget (default: half the free HBM).
+    """
+
+    def __init__(self, device: int = 0, precision: str = "fp32", max_batch: int = 32, n_streams: int = 4,
+                 hbm_budget_bytes: int | None = None, configs: Mapping | None = None) -> None:
+        import torch
+
+        self.torch = torch
+        self.device = device
+        self.precision = precision
+        self.max_batch = int(max_batch)
+        self.dev = torch.device("cuda", device)
+        self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(int(n_streams))]
+        if hbm_budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.dev)
+            hbm_budget_bytes = free // 2
+        self.budget = int(hbm_budget_bytes)
+        self.configs = dict(configs or {})
+        self._engines: dict[Hashable, SolveEngine] = {}
+        self._family_cfg: dict[Hashable, dict] = {}
+        self.in_use = 0
+        self.peak_in_use = 0
+        self.jobs_run = 0
+        self.batch_sizes: list[int] = []
+
+    # ---------------------------------------------------------------- engines
+    def engine(self, req: Request) -> SolveEngine:
+        """The solve engine of a request's model, with one launch shape per
+        regime and family (independent of the batch and of the grid sizes,
+        so a family's models share kernels and results do not depend on the
+        batch)."""
+        eng = self._engines.get(req.key)
+        if eng is None:
+            cfgs = self._family_cfg.get(req.family)
+            if cfgs is None:
+                cfgs = dict(self.configs.get(req.family, {}))
+                for s in req.model.regime_specs:
+                    if s.name not in cfgs:
+                        cfgs[s.name] = LaunchConfig(block=256, lanes=1, chunk=512, sb=1)
+                self._family_cfg[req.family] = cfgs
+            eng = SolveEngine(req.model, self.precision, configs=cfgs, device=self.device)
+            self._engines[req.key] = eng
+        return eng
+
+    def footprint(self, req: Request) -> int:
+        n = int(np.asarray(req.initial_conditions["regime_id"]).shape[0])
+        return footprint_bytes(self.engine(req), n)
+
+    # ------------------------------------------------------------------ jobs
+    def _launch(self, family, reqs: list, stream, nbytes: int, now: float) -> _Job:
+        from pylcm_b200.engine import BatchPlan
+        from pylcm_b200.simulate import SimPlan
+
+        torch = self.torch
+        with torch.cuda.stream(stream):
+            plan = BatchPlan([(self.engine(r), r.params) for r in reqs])
+            plan.run(stream.cuda_stream)
+            sim = SimPlan(plan, instances=[(k, r.initial_conditions, r.seed) for k, r in enumerate(reqs)])
+            sim.run(stream.cuda_stream)
+            rows, lengths = [], []
+            for b in sim.inst:
+                T = b["T"]
+                cols = [b["val"]]
+                cols += [b["S"][n][:T] for n in sorted(b["S"])]
+                cols += [b["A"][n] for n in sorted(b["A"])]
+                cols += [(b["R"][:T] == s.rid).to(torch.float64) for s in b["eng"].specs]
+                m = torch.nanmean(torch.stack(cols), dim=-1)
+                rows.append(m.reshape(-1))
+                lengths.append((len(cols), T))
+            dev_out = torch.cat(rows)
+            host = torch.empty(tuple(dev_out.shape), dtype=torch.float64, pin_memory=True)
+            host.copy_(dev_out, non_blocking=True)
+            v_host = {}
+            for k, r in enumerate(reqs):
+                if r.return_V:
+                    vh = {}
+                    for name, v in plan.plans[k].V.items():
+                        t = torch.empty(tuple(v[0].shape), dtype=torch.float64, pin_memory=True)
+                        t.copy_(v[0], non_blocking=True)
+                        vh[name] = t
+                    v_host[k] = vh
+            event = torch.cuda.Event()
+            event.record(stream)
+        self.jobs_run += 1
+        self.batch_sizes.append(len(reqs))
+        return _Job(family, reqs, stream, plan, sim, host, event, nbytes, now, v_host, lengths)
+
+    def _finish(self, job: _Job, now: float) -> list[Result]:
+        arr = job.host.numpy()
+        out = []
+        off = 0
+        for k, r in enumerate(job.reqs):
+            b = job.sim.inst[k]
+            eng = b["eng"]
+            names = ["value"] + sorted(b["S"]) + sorted(b["A"]) + [f"share_{s.name}" for s in eng.specs]
+            ncol, T = job.lengths[k]
+            block = arr[off: off + ncol * T].reshape(ncol, T)
+            off += ncol * T
+            moments = {n: block[i].copy() for i, n in enumerate(names)}
+            V = None
+            if k in job.v_host:
+                V = {}
+                pl = job.plan.plans[k]
+                for name, t in job.v_host[k].items():
+                    spec = next(s for s in eng.specs if s.name == name)
+                    for p, slot in pl.slot[name].items():
+                        V.setdefault(p, {})[name] = t[slot].numpy().reshape(spec.state_shape).copy()
+            out.append(Result(r.rid, job.family, moments, V, r.arrival, job.admitted, now, len(job.reqs)))
+        return out
+
+    # ------------------------------------------------------------------- run
+    def run(self, requests: Sequence[Request], realtime: bool = True) -> list[Result]:
+        """Serve `requests`, released at their arrival times (seconds after
+        the start) when `realtime`, all at once otherwise.  Returns the
+        results in request order; `Result.latency` is end-to-end (arrival to
+        the host seeing the result)."""
+        torch = self.torch
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        foot = {}
+        for r in reqs:
+            fp = self.footprint(r)
+            if fp > self.budget:
+                raise MemoryError(
+                    f"request {r.rid}: footprint {fp} B exceeds the HBM budget {self.budget} B"
+                )
+            foot[r.rid] = fp
+        waiting: dict[Hashable, collections.deque] = collections.OrderedDict()
+        free = list(self.streams)
+        inflight: list[_Job] = []
+        results: dict[int, Result] = {}
+        i = 0
+        t0 = time.perf_counter()
+        n = len(reqs)
+        while len(results) < n:
+            now = time.perf_counter() - t0
+            while i < n and (not realtime or reqs[i].arrival <= now):
+                r = reqs[i]
+                if not realtime:
+                    r.arrival = 0.0
+                waiting.setdefault(r.family, collections.deque()).append(r)
+                i += 1
+            progressed = False
+            for job in list(inflight):
+                if job.event.query():
+                    now = time.perf_counter() - t0
+                    for res in self._finish(job, now):
+                        results[res.rid] = res
+                    inflight.remove(job)
+                    free.append(job.stream)
+                    self.in_use -= job.nbytes
+                    progressed = True
+            while free and any(waiting.values()):
+                key = min((k for k, q in waiting.items() if q), key=lambda k: waiting[k][0].arrival)
+                q = waiting[key]
+                batch, nbytes = [], 0
+                while q and len(batch) < self.max_batch and self.in_use + nbytes + foot[q[0].rid] <= self.budget:
+                    nbytes += foot[q[0].rid]
+                    batch.append(q.popleft())
+                if not batch:
+                    break  # admission: wait for memory to free up
+                self.in_use += nbytes
+                self.peak_in_use = max(self.peak_in_use, self.in_use)
+                inflight.append(self._launch(key, batch, free.pop(0), nbytes, time.perf_counter() - t0))
+                progressed = True
+            if not progressed:
+                if inflight:
+                    time.sleep(5e-5)
+                elif i < n:
+                    time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 1e-3)))
+        torch.cuda.synchronize(self.dev)
+        return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]
+
+
+def latency_summary(results: Sequence[Result], wall_s: float | None = None) -> dict:
+    lat = np.array([r.latency for r in results])
+    out = {
+        "requests": len(results),
+        "p50_ms": float(np.percentile(lat, 50) * 1e3),
+        "p99_ms": float(np.percentile(lat, 99) * 1e3),
+        "mean_ms": float(lat.mean() * 1e3),
+        "mean_batch": float(np.mean([r.batch_size for r in results])),
+    }
+    if wall_s is None:
+        wall_s = max(r.finished for r in results) - min(r.arrival for r in results)
+    out["wall_s"] = float(wall_s)
+    out["solves_per_s"] = len(results) / wall_s
+    return out

@@ -103,10 +103,12 @@ def _initial_arrays(model, initial_conditions: Mapping) -> tuple[np.ndarray, dic
 class SimPlan:
     """Device buffers and launches of the simulations of solve instances.
 
-    `instances` lists (solve-plan instance, initial conditions, seed): one
-    kernel (d) launch per (period, regime) covers every listed instance, each
-    with its own subjects, buffers and seed (the Philox key of an item is the
-    launch seed XOR the item's seed word; the launch seed is 0 here).
+    `instances` lists (solve-plan instance, initial conditions, seed).  Per
+    period, one kernel (d) launch per kernel covers every listed instance
+    whose regime uses it, each instance with its own subjects, buffers,
+    horizon and seed (the Philox key of an item is the launch seed XOR the
+    item's seed word; the launch seed is 0 here).  `solve_plan` is a
+    `SolvePlan` (one model) or a `BatchPlan` (a model family).
     """
 
     def __init__(self, solve_plan, initial_conditions: Mapping | None = None, seed: int = 0,
@@ -115,22 +117,21 @@ class SimPlan:
 
         self.torch = torch
         self.plan = solve_plan
-        eng = solve_plan.eng
-        model = eng.model
-        specs = eng.specs
-        T = model.n_periods
         dev = solve_plan.dev
         if instances is None:
             instances = [(0, initial_conditions, seed)]
         solve_plan.ensure_sim_records()
-        self.T = T
-        names = sorted({a.name for s in specs for a in s.states})
-        anames = sorted({a.name for s in specs for a in s.actions})
         nan = float("nan")
         self.inst = []
         for idx, ic, sd in instances:
             if not 0 <= idx < solve_plan.n:
                 raise InvalidParamsError(f"instance {idx} outside the solve plan's batch of {solve_plan.n}")
+            eng, records, row = solve_plan.instance(idx)
+            model = eng.model
+            specs = eng.specs
+            T = model.n_periods
+            names = sorted({a.name for s in specs for a in s.states})
+            anames = sorted({a.name for s in specs for a in s.actions})
             rid0, states0 = _initial_arrays(model, ic)
             N = rid0.shape[0]
             for s in specs:
@@ -139,6 +140,10 @@ class SimPlan:
                         raise InvalidParamsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
             b = {
                 "idx": idx,
+                "eng": eng,
+                "records": records,
+                "row": row,
+                "T": T,
                 "N": N,
                 "seed": int(sd) & 0xFFFFFFFFFFFFFFFF,
                 "S": {n: torch.full((T + 1, N), nan, dtype=torch.float64, device=dev) for n in names},
@@ -152,22 +157,25 @@ class SimPlan:
                     b["S"][n][0] = torch.as_tensor(v, device=dev)
             b["R"][0] = torch.as_tensor(rid0, dtype=torch.int32, device=dev)
             self.inst.append(b)
+        self.T = max(b["T"] for b in self.inst)
         # item records: the Bellman record of (period, regime, instance) + simulation words
         recs = []
         prefs = []
         self.launches = []
         off = 0
         poff = 0
-        for period in range(T):
-            for s in specs:
-                if period not in s.active_periods:
+        for period in range(self.T):
+            groups: dict[tuple, list] = {}
+            for b in self.inst:
+                if period >= b["T"]:
                     continue
-                rk, base = solve_plan.records[(period, s.name)]
-                eng.module(rk)
-                tiles = []
-                for b in self.inst:
+                for s in b["eng"].specs:
+                    if period not in s.active_periods:
+                        continue
+                    rk, base = b["records"][(period, s.name)]
+                    b["eng"].module(rk)
                     r = np.zeros(rk.sim_words, dtype=np.int64)
-                    r[: rk.n_words] = base[b["idx"]]
+                    r[: rk.n_words] = base[b["row"]]
                     r[rk.SW_N] = b["N"]
                     r[rk.SW_RID_IN] = b["R"][period].data_ptr()
                     r[rk.SW_RID_OUT] = b["R"][period + 1].data_ptr()
@@ -180,14 +188,17 @@ class SimPlan:
                         r[rk.SW_SIN + k] = b["S"][a.name][period].data_ptr()
                     for k, name in enumerate(rk.sim_out_names):
                         r[rk.SW_SOUT + k] = b["S"][name][period + 1].data_ptr()
-                    recs.append(r)
-                    tiles.append(math.ceil(b["N"] / 8))
+                    groups.setdefault((rk.sim_name(), rk.key), []).append((rk, r, math.ceil(b["N"] / 8)))
+            for members in groups.values():
+                rk = members[0][0]
+                tiles = [t for _, _, t in members]
                 pre = np.zeros(len(tiles) + 1, dtype=np.int32)
                 pre[1:] = np.cumsum(tiles)
                 pad = (-pre.size) % 4
                 prefs.append(np.concatenate([pre, np.zeros(pad, dtype=np.int32)]))
-                self.launches.append((period, rk, off, poff, len(self.inst), int(pre[-1])))
-                off += rk.sim_words * len(self.inst)
+                recs.extend(r for _, r, _ in members)
+                self.launches.append((period, rk, off, poff, len(members), int(pre[-1])))
+                off += rk.sim_words * len(members)
                 poff += pre.size + pad
         self.items = torch.as_tensor(np.concatenate(recs), dtype=torch.int64, device=dev)
         self.prefix = torch.as_tensor(np.concatenate(prefs), dtype=torch.int32, device=dev)
@@ -208,16 +219,17 @@ class SimPlan:
     def gpu_launches(self) -> int:
         return len(self.launches)
 
-    def result(self, model, k: int = 0) -> SimulationResult:
+    def result(self, model=None, k: int = 0) -> SimulationResult:
         torch = self.torch
         torch.cuda.current_stream(self.plan.dev).synchronize()
         b = self.inst[k]
+        model = b["eng"].model if model is None else model
         periods = {}
         R = b["R"].cpu().numpy()
         V = b["val"].cpu().numpy()
         S = {n: v.cpu().numpy() for n, v in b["S"].items()}
         A = {n: v.cpu().numpy() for n, v in b["A"].items()}
-        for p in range(self.T):
+        for p in range(b["T"]):
             periods[p] = {
                 "regime_id": R[p],
                 "value": V[p],
