@@ -296,6 +296,354 @@ __global__ void __launch_bounds__(kBlock) fues_kernel(const double* __restrict__
   }
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory form (rows of up to kSmemMaxN candidates).
+//
+// Same three stages and the same decisions as fues_kernel, with the sorted
+// row staged in shared memory and the scan's per-step work cut to what a
+// step uses:
+//   * a step without a policy jump between j and i never reads the
+//     look-ahead, the intersections or i's own neighbours -- it is dropped
+//     or emits j and shifts (k, j) <- (j, i);
+//   * when j is the previous candidate (the common case), the policy-jump
+//     test and the secant of (j, i) are precomputed for every position in
+//     parallel before the scan; grad_before is the previous secant while k is
+//     the candidate before j, unmodified;
+//   * the look-ahead searches (warp ballot over shared memory) run only on
+//     steps with a policy jump.
+// Every value the scan uses is computed with the same operations and
+// operands as in fues_kernel, so the rows are identical.
+constexpr int kSmemMaxN = 4096;
+constexpr int kFuesItemWords = 12;
+
+__host__ __device__ constexpr size_t fues_smem_bytes(int n) {
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  return (size_t)5 * n * sizeof(double) + (size_t)np2 * sizeof(int);
+}
+
+struct FuesRowIO {
+  const double* G;
+  const double* P;
+  const double* V;
+  const double* S;
+  double* GO;
+  double* PO;
+  double* VO;
+  int* nk;
+  int n_in;
+  int n_out;
+  double thr;
+};
+
+struct FuesContig {
+  const double* grid;
+  const double* policy;
+  const double* value;
+  const double* savings;
+  double* go;
+  double* po;
+  double* vo;
+  int* nk;
+  int n_rows, n_in, n_out;
+  double thr;
+  __device__ __forceinline__ int count() const { return n_rows; }
+  __device__ __forceinline__ FuesRowIO row(int r) const {
+    FuesRowIO io;
+    io.G = grid + (int64_t)r * n_in;
+    io.P = policy + (int64_t)r * n_in;
+    io.V = value + (int64_t)r * n_in;
+    io.S = savings ? savings + (int64_t)r * n_in : nullptr;
+    io.GO = go + (int64_t)r * n_out;
+    io.PO = po + (int64_t)r * n_out;
+    io.VO = vo + (int64_t)r * n_out;
+    io.nk = nk + r;
+    io.n_in = n_in;
+    io.n_out = n_out;
+    io.thr = thr;
+    return io;
+  }
+};
+
+// item words: 0 grid, 1 policy, 2 value, 3 savings (0: none), 4 grid_out,
+// 5 policy_out, 6 value_out, 7 n_kept (int32), 8 n_rows, 9 n_in, 10 n_out,
+// 11 jump_thresh (double bits); one tile per row
+struct FuesItems {
+  const int64_t* items;
+  const int* prefix;
+  int n_items, n_tiles;
+  __device__ __forceinline__ int count() const { return n_tiles; }
+  __device__ __forceinline__ FuesRowIO row(int tile) const {
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= tile) lo = mid; else hi = mid - 1;
+    }
+    const int64_t* it = items + (int64_t)lo * kFuesItemWords;
+    const int r = tile - prefix[lo];
+    FuesRowIO io;
+    io.n_in = (int)it[9];
+    io.n_out = (int)it[10];
+    io.thr = __longlong_as_double(it[11]);
+    io.G = reinterpret_cast<const double*>(it[0]) + (int64_t)r * io.n_in;
+    io.P = reinterpret_cast<const double*>(it[1]) + (int64_t)r * io.n_in;
+    io.V = reinterpret_cast<const double*>(it[2]) + (int64_t)r * io.n_in;
+    io.S = it[3] ? reinterpret_cast<const double*>(it[3]) + (int64_t)r * io.n_in : nullptr;
+    io.GO = reinterpret_cast<double*>(it[4]) + (int64_t)r * io.n_out;
+    io.PO = reinterpret_cast<double*>(it[5]) + (int64_t)r * io.n_out;
+    io.VO = reinterpret_cast<double*>(it[6]) + (int64_t)r * io.n_out;
+    io.nk = reinterpret_cast<int*>(it[7]) + r;
+    return io;
+  }
+};
+
+template <class Rows>
+__global__ void __launch_bounds__(kBlock) fues_smem_kernel(Rows rows) {
+  extern __shared__ __align__(16) unsigned char fues_smem[];
+  const int total = rows.count();
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  for (int row = blockIdx.x; row < total; row += gridDim.x) {
+    const FuesRowIO io = rows.row(row);
+    const int n = io.n_in;
+    const int n_out = io.n_out;
+    const double thr = io.thr;
+    const double* G = io.G;
+    const double* P = io.P;
+    const double* V = io.V;
+    int np2 = 1;
+    while (np2 < n) np2 <<= 1;
+    double* g = reinterpret_cast<double*>(fues_smem);
+    double* p = g + n;
+    double* v = p + n;
+    double* s = v + n;
+    double* sec = s + n;
+    int* sidx = reinterpret_cast<int*>(sec + n);
+    __syncthreads();  // the previous row is done with shared memory
+    // ---- 1. bitonic sort of indices by the lexsort key
+    for (int t = threadIdx.x; t < np2; t += kBlock) sidx[t] = t;
+    __syncthreads();
+    for (int size = 2; size <= np2; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = threadIdx.x; t < np2; t += kBlock) {
+          const int partner = t ^ stride;
+          if (partner > t) {
+            const bool ascending = (t & size) == 0;
+            const Key a = load_key(G, V, P, sidx[t], n);
+            const Key b = load_key(G, V, P, sidx[partner], n);
+            const bool swap = ascending ? key_less(b, a) : key_less(a, b);
+            if (swap) {
+              const int tmp = sidx[t];
+              sidx[t] = sidx[partner];
+              sidx[partner] = tmp;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int t = threadIdx.x; t < n; t += kBlock) {
+      const int i = sidx[t];
+      g[t] = G[i];
+      p[t] = P[i];
+      v[t] = V[i];
+      s[t] = io.S ? io.S[i] : G[i] - P[i];
+    }
+    __syncthreads();
+    // ---- 2. coincident groups: keep the maximisers, one per savings source
+    for (int t = threadIdx.x; t < n; t += kBlock) {
+      const double gt = g[t];
+      bool keep = !isnan_(gt);
+      if (keep) {
+        int lo = t, hi = t;
+        while (lo > 0 && g[lo - 1] == gt) --lo;
+        while (hi + 1 < n && g[hi + 1] == gt) ++hi;
+        if (hi > lo) {
+          double vmax = -__longlong_as_double(0x7ff0000000000000LL);
+          for (int k = lo; k <= hi; ++k) {
+            const double vk = v[k];
+            if (!isnan_(vk) && vk > vmax) vmax = vk;
+          }
+          keep = v[t] == vmax;
+          if (keep) {
+            for (int k = lo; k < t; ++k)
+              if (v[k] == vmax && s[k] == s[t]) keep = false;
+          }
+        }
+      }
+      sidx[t] = keep ? 1 : 0;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += kBlock) {
+      if (!sidx[t]) g[t] = p[t] = v[t] = s[t] = nan;
+    }
+    for (int t = threadIdx.x; t < n_out; t += kBlock) io.GO[t] = io.PO[t] = io.VO[t] = nan;
+    __syncthreads();
+    // ---- 3a. per position t: policy jump and secant of (t - 1, t)
+    for (int t = threadIdx.x + 1; t < n; t += kBlock) {
+      sidx[t] = policy_jump(g[t - 1], p[t - 1], g[t], p[t], thr, true, s[t - 1], s[t]) ? 1 : 0;
+      sec[t] = slope(g[t - 1], v[t - 1], g[t], v[t]);
+    }
+    __syncthreads();
+    // ---- 3b. the scan (warp 0; all lanes hold the state, lane 0 writes)
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double* GO = io.GO;
+      double* PO = io.PO;
+      double* VO = io.VO;
+      int cnt = 0;
+      auto emit = [&](double eg, double ep, double ev) {
+        if (lane == 0 && cnt < n_out) {
+          GO[cnt] = eg;
+          PO[cnt] = ep;
+          VO[cnt] = ev;
+        }
+        ++cnt;
+      };
+      double gk = g[0], pk = p[0], vk = v[0];
+      double gj = g[0], pj = p[0], vj = v[0], sj = s[0];
+      int jidx = 0, kidx = 0;  // candidates j and k are (kidx < 0: k is a kink point)
+      const double near = 16.0 * 2.220446049250313e-16;
+      for (int idx = 1; idx < n; ++idx) {
+        const double gi = g[idx], vi = v[idx];
+        if (isnan_(gi) || isnan_(vi)) continue;
+        const double pi = p[idx], si = s[idx];
+        const bool prev = jidx == idx - 1;
+        const bool sw = prev ? (sidx[idx] != 0) : policy_jump(gj, pj, gi, pi, thr, true, sj, si);
+        const bool node_crossing = sw && gi == gj && vi == vj;
+        bool have_sec = false, have_gb = false;
+        double secant = 0.0, grad_before = 0.0;
+        auto get_secant = [&]() {
+          if (!have_sec) {
+            secant = prev ? sec[idx] : slope(gj, vj, gi, vi);
+            have_sec = true;
+          }
+          return secant;
+        };
+        auto get_gb = [&]() {
+          if (!have_gb) {
+            grad_before = (kidx >= 0 && kidx == jidx - 1) ? sec[jidx] : slope(gk, vk, gj, vj);
+            have_gb = true;
+          }
+          return grad_before;
+        };
+        bool drop = (vi < vj) && !sw;
+        if (!drop && si < sj) drop = get_secant() < get_gb();
+        double jg = nan, jp = nan, jv = nan;
+        bool jf = false;
+        if (sw) {
+          jf = find_same_segment(g, p, v, n, gj, pj, idx, 1, thr, jg, jp, jv);
+          if (!drop && jf) drop = (gi == jg) ? (vi < jv) : (get_secant() < slope(gi, vi, jg, jv));
+        }
+        if (drop && !node_crossing) continue;
+        if (!sw) {
+          emit(gj, pj, vj);
+          gk = gj;
+          pk = pj;
+          vk = vj;
+          kidx = jidx;
+          gj = gi;
+          pj = pi;
+          vj = vi;
+          sj = si;
+          jidx = idx;
+          continue;
+        }
+        const double sc = get_secant();
+        const double gb = get_gb();
+        double fg, fp, fv, bg, bp, bv;
+        const bool ff = find_same_segment(g, p, v, n, gi, pi, idx, 1, thr, fg, fp, fv);
+        const bool bf = find_same_segment(g, p, v, n, gi, pi, idx, -1, thr, bg, bp, bv);
+        const bool found = ff || bf;
+        const double pg = ff ? fg : bg, pp = ff ? fp : bp, pv = ff ? fv : bv;
+        const double i_slope = slope(gi, vi, pg, pv);
+        const double i_pslope = slope(gi, pi, pg, pp);
+        const bool j_dom = found && (sc > i_slope) && !node_crossing;
+        const double pslope_kj = slope(gk, pk, gj, pj);
+        double k6g, k6v;
+        intersect(gj, vj, gb, gi, vi, i_slope, k6g, k6v);
+        const double k6pl = pj + pslope_kj * (k6g - gj);
+        const double k6pr = pi + i_pslope * (k6g - gi);
+        const bool kink6 = j_dom && (k6g > gk) && (k6g < gj) && (k6g < gi);
+        const double j_slope = jf ? slope(gj, vj, jg, jv) : gb;
+        const double j_pslope = jf ? slope(gj, pj, jg, jp) : pslope_kj;
+        double k5g, k5v;
+        intersect(gj, vj, j_slope, gi, vi, i_slope, k5g, k5v);
+        const double k5pl = pj + j_pslope * (k5g - gj);
+        const double k5pr = pi + i_pslope * (k5g - gi);
+        const bool crossing = !j_dom && !node_crossing && found;
+        const double tol = near * fmax(fmax(fabs(gj), fabs(gi)), 1.0);
+        const bool on_j = crossing && fabs(k5g - gj) <= tol;
+        const bool on_i = crossing && !on_j && fabs(k5g - gi) <= tol;
+        const bool kink5 = crossing && !on_j && !on_i && (k5g > gj) && (k5g < gi);
+        const bool plain = !j_dom && !kink5 && !on_j && !on_i;
+        if (kink6) {
+          emit(k6g, k6pl, k6v);
+          emit(k6g, k6pr, k6v);
+        } else if (plain || kink5 || on_j || on_i) {
+          emit(gj, pj, vj);
+          if (kink5) {
+            emit(k5g, k5pl, k5v);
+            emit(k5g, k5pr, k5v);
+          } else if (on_j) {
+            emit(gj, k5pr, k5v);
+          } else if (on_i) {
+            emit(gi, k5pl, k5v);
+          }
+        }
+        const bool keeps_k = j_dom && !kink6;
+        if (!keeps_k) {
+          if (kink5) {
+            gk = k5g; pk = k5pr; vk = k5v; kidx = -1;
+          } else if (kink6) {
+            gk = k6g; pk = k6pr; vk = k6v; kidx = -1;
+          } else {
+            gk = gj;
+            pk = on_j ? k5pr : pj;
+            vk = on_j ? k5v : vj;
+            kidx = on_j ? -1 : jidx;
+          }
+        }
+        gj = gi; pj = pi; vj = vi; sj = si;
+        jidx = idx;
+      }
+      if (!isnan_(gj) && !isnan_(vj)) emit(gj, pj, vj);
+      if (lane == 0) *io.nk = cnt;
+    }
+  }
+}
+
+// the dynamic shared-memory limit of both instantiations, set once per device
+std::mutex g_attr_mu;
+bool g_attr_done[64] = {};
+
+int fues_smem_attr(std::string& err) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) {
+    err = "fues: device ordinal >= 64";
+    return LCMX_ERR_ARGS;
+  }
+  std::lock_guard<std::mutex> g(g_attr_mu);
+  if (g_attr_done[dev]) return LCMX_OK;
+  const int bytes = (int)fues_smem_bytes(kSmemMaxN);
+  cudaError_t e = cudaFuncSetAttribute(fues_smem_kernel<FuesContig>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fues_smem_kernel<FuesItems>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) {
+    err = std::string("fues: shared-memory attribute: ") + cudaGetErrorString(e);
+    return LCMX_ERR_CUDA;
+  }
+  g_attr_done[dev] = true;
+  return LCMX_OK;
+}
+
+int fues_grid(int rows) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return rows < sms * 16 ? rows : sms * 16;
+}
+
 }  // namespace
 
 extern "C" size_t lcmx_fues_workspace_bytes(int n_rows, int n_in) {
@@ -307,6 +655,19 @@ static int launch_fues(const double* grid, const double* policy, const double* v
                        int n_rows, int n_in, double jump_thresh, double* grid_out, double* policy_out,
                        double* value_out, int n_out, int* n_kept, double* work, cudaStream_t stream,
                        std::string& err) {
+  if (n_in <= kSmemMaxN) {
+    int rc = fues_smem_attr(err);
+    if (rc) return rc;
+    FuesContig rows{grid, policy, value, savings, grid_out, policy_out, value_out, n_kept,
+                    n_rows, n_in, n_out, jump_thresh};
+    fues_smem_kernel<FuesContig><<<fues_grid(n_rows), kBlock, fues_smem_bytes(n_in), stream>>>(rows);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      err = std::string("fues launch: ") + cudaGetErrorString(e);
+      return LCMX_ERR_LAUNCH;
+    }
+    return LCMX_OK;
+  }
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -412,5 +773,26 @@ extern "C" int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const do
   int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
                        n_out, n_kept, work, (cudaStream_t)stream, err);
   if (rc) return lcmx_set_error_from(ctx, rc, err);
+  return LCMX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Item form: the rows of several candidate blocks (one per solve instance)
+// in one launch; see FuesItems for the item words.
+extern "C" int lcmx_fues_step(lcmx_ctx* ctx, const void* items, const int* tile_prefix, int n_items, int n_rows,
+                              int max_n_in, void* stream) {
+  if (!ctx || n_items < 0 || n_rows < 0 || (n_items > 0 && (!items || !tile_prefix)))
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_step: bad arguments");
+  if (max_n_in < 1 || max_n_in > kSmemMaxN)
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS,
+                               "lcmx_fues_step: rows must hold 1.." + std::to_string(kSmemMaxN) + " candidates");
+  if (n_items == 0 || n_rows == 0) return LCMX_OK;
+  std::string err;
+  int rc = fues_smem_attr(err);
+  if (rc) return lcmx_set_error_from(ctx, rc, err);
+  FuesItems rows{static_cast<const int64_t*>(items), tile_prefix, n_items, n_rows};
+  fues_smem_kernel<FuesItems><<<fues_grid(n_rows), kBlock, fues_smem_bytes(max_n_in), (cudaStream_t)stream>>>(rows);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return lcmx_set_error_from(ctx, LCMX_ERR_LAUNCH, std::string("lcmx_fues_step: ") + cudaGetErrorString(e));
   return LCMX_OK;
 }

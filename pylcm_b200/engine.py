@@ -106,6 +106,7 @@ class _Records:
 
 SM_COUNT = 148
 RESIDENT_THREADS_PER_SM = 1024
+FUES_SMEM_MAX_N = 4096  # longest candidate row of the item-form FUES launch
 
 
 def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> LaunchConfig:
@@ -552,11 +553,36 @@ class SolvePlan:
         ns = nrow // er.n_disc_actions
         add_launch = rec.add
         add_launch("egm", ek, cname, recs, [math.ceil(nrow * len(er.savings) / 256)] * n, 256, 0, period)
-        rec.append(
-            Launch("fues", ("fues", s.name, slot, er.jump_thresh), "lcmx_fues_scan", 0, 0, n * nrow, 0, 0, 0, period)
-        )
+        # FUES over every instance's candidate rows (one tile per row)
+        cg, cc, cv, cs = b["cand"]
+        frecs = []
+        for i in range(n):
+            fr = np.zeros(12, dtype=np.int64)
+            fr[0], fr[1], fr[2], fr[3] = cg[i].data_ptr(), cc[i].data_ptr(), cv[i].data_ptr(), cs[i].data_ptr()
+            fr[4], fr[5], fr[6] = b["rg"][slot, i].data_ptr(), b["rc"][slot, i].data_ptr(), b["rv"][slot, i].data_ptr()
+            fr[7] = b["nk"][slot, i].data_ptr()
+            fr[8], fr[9], fr[10] = nrow, ncand, npad
+            fr[11] = _f2w(er.jump_thresh)
+            frecs.append(fr)
+        if ncand <= FUES_SMEM_MAX_N:
+            add_launch("fues", None, "lcmx_fues_step", frecs, [nrow] * n, 0, ncand, period)
+        else:
+            rec.append(
+                Launch("fues", ("fues", s.name, slot, er.jump_thresh), "lcmx_fues_scan", 0, 0, n * nrow, 0, 0, 0, period)
+            )
         add_launch("egm", ek, uname, recs, [math.ceil(nrow * npad / 256)] * n, 256, 0, period)
         add_launch("egm", ek, pname, recs, [math.ceil(ns * grid.numel() / 256)] * n, 256, 0, period)
+
+    def _fues_item_launch(self, l: Launch, ib: int, pb: int):
+        from pylcm_b200.runtime import get_context
+
+        ctx = get_context(self.eng.device if hasattr(self, "eng") else self.plans[0].eng.device)
+        args = (ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.smem)
+
+        def launch(stream):
+            ctx.fues_step(*args, stream)
+
+        return launch
 
     def _fues_launch(self, spec_name, slot, thr):
         from pylcm_b200.runtime import get_context
@@ -584,8 +610,7 @@ class SolvePlan:
         out = []
         for l in launches:
             if l.kind == "fues":
-                _, name, slot, thr = l.module
-                out.append(self._fues_launch(name, slot, thr))
+                out.append(self._fues_item_launch(l, ib, pb) if l.module is None else self._fues_launch(*l.module[1:]))
                 continue
             out.append(
                 l.module.module.prepared(
@@ -704,7 +729,7 @@ class BatchPlan:
                     if j >= len(lst):
                         continue
                     pl, l, h = lst[j]
-                    if l.kind == "fues":
+                    if l.kind == "fues" and l.module is not None:
                         b.append(Launch("fues", (pl,) + tuple(l.module[1:]), l.kernel, 0, 0, l.n_items, 0, 0, 0, k))
                         continue
                     gk = (l.kind, l.kernel, l.module.key if hasattr(l.module, "key") else id(l.module))
@@ -713,7 +738,8 @@ class BatchPlan:
                     l0 = members[0][0]
                     recs = [row for _, h in members for row in h[0]]
                     tiles = [t for _, h in members for t in h[1]]
-                    b.add(l0.kind, l0.module, l0.kernel, recs, tiles, l0.block, l0.smem, k)
+                    smem = max(l.smem for l, _ in members)  # FUES: the longest candidate row
+                    b.add(l0.kind, l0.module, l0.kernel, recs, tiles, l0.block, smem, k)
         items, prefix = b.tensors(self.torch, self.dev)
         return b.launches, items, prefix
 
@@ -723,8 +749,11 @@ class BatchPlan:
         out = []
         for l in launches:
             if l.kind == "fues":
-                pl, name, slot, thr = l.module
-                out.append(pl._fues_launch(name, slot, thr))
+                if l.module is None:
+                    out.append(SolvePlan._fues_item_launch(self, l, ib, pb))
+                else:
+                    pl, name, slot, thr = l.module
+                    out.append(pl._fues_launch(name, slot, thr))
                 continue
             out.append(
                 l.module.module.prepared(

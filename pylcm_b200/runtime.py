@@ -30,6 +30,7 @@ EXPORTED = (
     "lcmx_fues_workspace_bytes",
     "lcmx_fues_scan",
     "lcmx_fues_scan_static",
+    "lcmx_fues_step",
 )
 
 
@@ -83,6 +84,7 @@ def load_library() -> ctypes.CDLL:
                 ip,
             ),
             "lcmx_fues_scan_static": ([vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
+            "lcmx_fues_step": ([vp, vp, vp, ip, ip, ip, vp], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
@@ -130,6 +132,10 @@ class Context:
 
     def count_nonfinite(self, ptr: int, n: int, counts_ptr: int, stream: int) -> None:
         self.check(self.lib.lcmx_count_nonfinite(self.h, ptr, n, counts_ptr, stream))
+
+    def fues_step(self, items: int, prefix: int, n_items: int, n_rows: int, max_n_in: int, stream: int) -> None:
+        """FUES of the rows of several candidate blocks (device item records)."""
+        self.check(self.lib.lcmx_fues_step(self.h, items, prefix, n_items, n_rows, max_n_in, stream))
 
     def fues_workspace_bytes(self, n_rows: int, n_in: int) -> int:
         return int(self.lib.lcmx_fues_workspace_bytes(n_rows, n_in))

@@ -158,6 +158,8 @@ class Server:
         self.peak_in_use = 0
         self.jobs_run = 0
         self.batch_sizes: list[int] = []
+        self.host_launch_s = 0.0  # host time building and issuing jobs
+        self.host_finish_s = 0.0  # host time unpacking results
 
     # ---------------------------------------------------------------- engines
     def engine(self, req: Request) -> SolveEngine:
@@ -278,9 +280,11 @@ class Server:
             progressed = False
             for job in list(inflight):
                 if job.event.query():
-                    now = time.perf_counter() - t0
+                    h0 = time.perf_counter()
+                    now = h0 - t0
                     for res in self._finish(job, now):
                         results[res.rid] = res
+                    self.host_finish_s += time.perf_counter() - h0
                     inflight.remove(job)
                     free.append(job.stream)
                     self.in_use -= job.nbytes
@@ -296,7 +300,9 @@ class Server:
                     break  # admission: wait for memory to free up
                 self.in_use += nbytes
                 self.peak_in_use = max(self.peak_in_use, self.in_use)
-                inflight.append(self._launch(key, batch, free.pop(0), nbytes, time.perf_counter() - t0))
+                h0 = time.perf_counter()
+                inflight.append(self._launch(key, batch, free.pop(0), nbytes, h0 - t0))
+                self.host_launch_s += time.perf_counter() - h0
                 progressed = True
             if not progressed:
                 if inflight:

@@ -87,3 +87,51 @@ def test_fues_kernel_reports_overflow():
     go, co, vo, nk = _gpu_fues(G, C, V, S, 4)
     assert np.all(nk > 4)
     assert np.all(np.isfinite(go[:, :4]))
+
+
+def test_shared_memory_and_global_kernels_give_identical_rows():
+    """Rows of 3000 candidates take the shared-memory kernel; the same rows
+    padded with absent (NaN) candidates to 5000 take the global-workspace
+    kernel.  NaN candidates sort last and are dropped, so the rows must be
+    bit-identical."""
+    G, C, V, S = _rows_nonconcave(5, 3000, seed=11)
+    pad = lambda a: np.concatenate([a, np.full((a.shape[0], 2000), np.nan)], axis=1)  # noqa: E731
+    a = _gpu_fues(G, C, V, S, 6100)
+    b = _gpu_fues(pad(G), pad(C), pad(V), pad(S), 6100)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_item_form_matches_the_contiguous_form():
+    """lcmx_fues_step over several candidate blocks (different row counts,
+    row lengths and thresholds) gives each block's lcmx_fues_scan rows."""
+    import torch
+
+    from pylcm_b200.engine import _f2w
+    from pylcm_b200.runtime import get_context
+
+    ctx = get_context(0)
+    blocks = [(4, 2020, 2.0, 1), (1, 300, 1.5, 2), (7, 777, 2.5, 3)]
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    keep, words, tiles = [], [], []
+    for n_rows, n_in, thr, seed in blocks:
+        G, C, V, S = _rows_nonconcave(n_rows, n_in, seed=seed)
+        n_out = 2 * n_in + 2
+        ins = [d(G), d(C), d(V), d(S)]
+        outs = [torch.full((n_rows, n_out), 7.0, dtype=torch.float64, device="cuda") for _ in range(3)]
+        nk = torch.zeros(n_rows, dtype=torch.int32, device="cuda")
+        w = [t.data_ptr() for t in ins] + [t.data_ptr() for t in outs] + [nk.data_ptr(), n_rows, n_in, n_out, _f2w(thr)]
+        words.append(np.array(w, dtype=np.int64))
+        tiles.append(n_rows)
+        keep.append((G, C, V, S, n_out, thr, ins, outs, nk))
+    items = torch.as_tensor(np.concatenate(words), dtype=torch.int64, device="cuda")
+    prefix = torch.as_tensor(np.concatenate([[0], np.cumsum(tiles)]).astype(np.int32), device="cuda")
+    ctx.fues_step(items.data_ptr(), prefix.data_ptr(), len(blocks), int(sum(tiles)), max(b[1] for b in blocks),
+                  torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    for G, C, V, S, n_out, thr, ins, outs, nk in keep:
+        go, co, vo, k = _gpu_fues(G, C, V, S, n_out, thr)
+        np.testing.assert_array_equal(outs[0].cpu().numpy(), go)
+        np.testing.assert_array_equal(outs[1].cpu().numpy(), co)
+        np.testing.assert_array_equal(outs[2].cpu().numpy(), vo)
+        np.testing.assert_array_equal(nk.cpu().numpy(), k)
