@@ -51,56 +51,77 @@ class Launch:
 
 
 class _Records:
-    """Item records and the launch list of a plan, concatenated into one
-    int64 item buffer and one int32 tile-prefix buffer."""
+    """Item records and the launch list of a plan.
+
+    Launches are collected with their host records (a 2-D int64 array, one
+    row per item) and tiles per item; `tensors()` lays the records out in one
+    int64 item buffer and the tile prefixes in one int32 buffer (each prefix
+    16-byte aligned) and fills in the launches' offsets.
+    """
 
     def __init__(self) -> None:
-        self.words: list[np.ndarray] = []
-        self.prefixes: list[np.ndarray] = []
         self.launches: list[Launch] = []
         # per launch: (records, tiles per item), None for a launch without records
         self.host: list[tuple | None] = []
-        self.w_off = 0
-        self.p_off = 0
-
-    def _prefix(self, tiles_per_item) -> tuple[int, int]:
-        pre = np.zeros(len(tiles_per_item) + 1, dtype=np.int32)
-        pre[1:] = np.cumsum(tiles_per_item)
-        off = self.p_off
-        self.prefixes.append(pre)
-        self.p_off += pre.size
-        # keep the prefix offsets 16-byte aligned for the device pointer math
-        pad = (-self.p_off) % 4
-        if pad:
-            self.prefixes.append(np.zeros(pad, dtype=np.int32))
-            self.p_off += pad
-        return off, int(pre[-1])
+        self.shared: list[int] = []  # launch whose records this one reuses (-1: own)
 
     def add(self, kind, rk, kernel, recs, tiles_per_item, block, smem, period) -> None:
-        arr = np.stack(recs).astype(np.int64)
-        self.words.append(arr.ravel())
-        p_off, n_tiles = self._prefix(tiles_per_item)
-        self.launches.append(Launch(kind, rk, kernel, self.w_off, p_off, len(recs), n_tiles, block, smem, period))
-        self.host.append((arr, list(tiles_per_item)))
-        self.w_off += arr.size
+        arr = recs if isinstance(recs, np.ndarray) and recs.ndim == 2 else np.stack(recs)
+        if arr.dtype != np.int64:
+            arr = arr.astype(np.int64)
+        tiles = list(tiles_per_item)
+        self.launches.append(Launch(kind, rk, kernel, 0, 0, arr.shape[0], int(sum(tiles)), block, smem, period))
+        self.host.append((arr, tiles))
+        self.shared.append(-1)
 
     def add_same_records(self, kind, rk, kernel, tiles_per_item, block, smem, period) -> None:
         """A launch over the previous launch's item records, own tiling."""
-        last = self.launches[-1]
-        p_off, n_tiles = self._prefix(tiles_per_item)
-        self.launches.append(Launch(kind, rk, kernel, last.item_off, p_off, last.n_items, n_tiles, block, smem, period))
-        self.host.append((self.host[-1][0], list(tiles_per_item)))
+        src = len(self.launches) - 1
+        tiles = list(tiles_per_item)
+        last = self.launches[src]
+        self.launches.append(Launch(kind, rk, kernel, 0, 0, last.n_items, int(sum(tiles)), block, smem, period))
+        self.host.append((self.host[src][0], tiles))
+        self.shared.append(src)
 
     def append(self, launch: Launch) -> None:
         self.launches.append(launch)
         self.host.append(None)
+        self.shared.append(-1)
+
+    def keep(self, pred) -> None:
+        """Drop the launches `pred` rejects.  A kept launch that reused the
+        records of a dropped one takes them over as its own."""
+        idx = [k for k, l in enumerate(self.launches) if pred(l)]
+        new_of = {k: j for j, k in enumerate(idx)}
+        self.launches = [self.launches[k] for k in idx]
+        self.host = [self.host[k] for k in idx]
+        self.shared = [new_of.get(self.shared[k], -1) if self.shared[k] >= 0 else -1 for k in idx]
 
     def tensors(self, torch, dev):
-        words = np.concatenate(self.words) if self.words else np.zeros(1, dtype=np.int64)
-        pre = np.concatenate(self.prefixes) if self.prefixes else np.zeros(4, dtype=np.int32)
+        words: list[np.ndarray] = []
+        prefs: list[np.ndarray] = []
+        w_off = p_off = 0
+        for l, h, src in zip(self.launches, self.host, self.shared):
+            if h is None:
+                continue
+            arr, tiles = h
+            if src >= 0:
+                l.item_off = self.launches[src].item_off
+            else:
+                l.item_off = w_off
+                words.append(arr.reshape(-1))
+                w_off += arr.size
+            npre = len(tiles) + 1
+            pre = np.zeros(npre + (-npre) % 4, dtype=np.int32)
+            np.cumsum(tiles, out=pre[1:npre])
+            l.prefix_off = p_off
+            prefs.append(pre)
+            p_off += pre.size
+        words_a = np.concatenate(words) if words else np.zeros(1, dtype=np.int64)
+        pre_a = np.concatenate(prefs) if prefs else np.zeros(4, dtype=np.int32)
         return (
-            torch.as_tensor(words, dtype=torch.int64, device=dev),
-            torch.as_tensor(pre, dtype=torch.int32, device=dev),
+            torch.as_tensor(words_a, dtype=torch.int64, device=dev),
+            torch.as_tensor(pre_a, dtype=torch.int32, device=dev),
         )
 
 
@@ -134,12 +155,16 @@ class SolveEngine:
         self.specs = model.regime_specs
         self._kernels: dict[tuple, RegimeKernels] = {}
         self._traces: dict[tuple, TracedRegime] = {}
+        self._targets: dict[tuple, tuple] = {}
 
     # ------------------------------------------------------------ helpers
     def targets_at(self, spec: RegimeSpec, period: int) -> tuple[str, ...]:
-        if spec.terminal:
-            return ()
-        return tuple(s.name for s in self.specs if (period + 1) in s.active_periods)
+        key = (spec.name, period)
+        t = self._targets.get(key)
+        if t is None:
+            t = () if spec.terminal else tuple(s.name for s in self.specs if (period + 1) in s.active_periods)
+            self._targets[key] = t
+        return t
 
     def resolver(self, params) -> ParamResolver:
         return ParamResolver(params, self.model.fixed_params, tuple(s.name for s in self.specs))
@@ -244,6 +269,7 @@ class SolvePlan:
         # ---- kernels per (regime, target set); params per (regime, target set)
         by = {s.name: s for s in specs}
         self.params: dict[tuple, Any] = {}
+        self._packers: dict[tuple, Any] = {}  # params key -> packer(resolver) -> float64 vector
         self.ev: dict[tuple, tuple] = {}
         step_list: list[tuple[int, RegimeSpec, tuple, Any]] = []
         egm_steps: list = []
@@ -260,6 +286,7 @@ class SolvePlan:
                     if key not in self.params:
                         vecs = [ek.er.pack_for(r) for r in resolvers]
                         self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                        self._packers[key] = ek.er.pack_for
                     egm_steps.append((period, s, targets, ek))
                     step_list.append((period, s, targets, ek))
                     continue
@@ -267,6 +294,7 @@ class SolvePlan:
                 if key not in self.params:
                     vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in resolvers]
                     self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                    self._packers[key] = lambda r, tr=rk.tr: tr.pack_params(tr.values_for(r))
                 step_list.append((period, s, targets, rk))
         # DC-EGM buffers: carry rows per active period, scratch per regime
         self.egm: dict[str, dict] = {}
@@ -274,7 +302,9 @@ class SolvePlan:
             if s.name in self.egm:
                 continue
             er = ek.er
-            nslot = max(len(s.active_periods), 1)
+            # carry rows are read only by the step of the period before: a
+            # two-slot ring indexed by period parity
+            nslot = 2
             npad, nrow, ncand = er.n_pad, er.n_rows, er.n_cand
             f64 = dict(dtype=torch.float64, device=dev)
             self.egm[s.name] = {
@@ -330,6 +360,9 @@ class SolvePlan:
         # by the simulation (same layout, extended with simulation words)
         self.records: dict[tuple, tuple] = {}
         self.resolvers = resolvers
+        self._grp: dict[tuple, dict] = {}  # per (regime, target set) group: records of all periods
+        self._geo: dict[tuple, tuple] = {}
+        self._ar = np.arange(n, dtype=np.int64)
         b = _Records()
         ages = model.ages.values
         for period, s, targets, rk in step_list:
@@ -350,14 +383,17 @@ class SolvePlan:
         self._sim_prepared = None
         self._egm_steps = [(p_, s_, t_) for p_, s_, t_, _ in egm_steps]
 
-    def _gs_launches(self, b: "_Records", rk: RegimeKernels, period: int, s: RegimeSpec, targets, pkey) -> None:
-        """Kernel (b) and (a0, a) records and launches of one grid-search step."""
+    def _gs_template(self, rk: RegimeKernels, period: int, s: RegimeSpec, targets, pkey) -> dict:
+        """Records of one grid-search step at `period` (every instance); the
+        other periods of the same regime and target set differ only in the
+        period, the age and the slot addresses."""
         n = self.n
         fp32 = self.eng.precision == "fp32"
         resolvers = self.resolvers
         age = float(self.eng.model.ages.values[period])
         pbuf = self.params[pkey]
-        # kernel (b) launches
+        out = {"expect": [], "tv": []}
+        # kernel (b) records
         for t in rk.targets:
             if t.scalar:
                 continue
@@ -380,8 +416,7 @@ class SolvePlan:
                 for k, ax in enumerate(t.spec.states):
                     r[8 + k] = ax.size
                 recs.append(r)
-            tiles = [math.ceil(ncols / 256)] * n
-            b.add("expect", rk, rk.expect_name(t), recs, tiles, 256, 0, period)
+            out["expect"].append((t, np.stack(recs).astype(np.int64), [math.ceil(ncols / 256)] * n))
         # kernel (a)
         slot = self.slot[s.name][period]
         recs = []
@@ -413,6 +448,8 @@ class SolvePlan:
                 tslot = self.slot[t.spec.name][period + 1]
                 if t.scalar:
                     r[t.w_scalar] = tV[i, tslot].data_ptr()
+                    if i == 0:
+                        out["tv"].append((t.w_scalar, t.spec.name))
                     continue
                 if t.needs_contraction or fp32:
                     e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
@@ -421,6 +458,8 @@ class SolvePlan:
                 else:
                     r[t.w_ev64] = tV[i, tslot].data_ptr()
                     r[t.w_ev32] = 0
+                    if i == 0:
+                        out["tv"].append((t.w_ev64, t.spec.name))
                 for k, ax in enumerate(t.spec.states):
                     r[t.w_sizes + k] = ax.size
                 for ci, pos in enumerate(t.cont_pos):
@@ -437,11 +476,81 @@ class SolvePlan:
                         r[base + 2] = self.sgrid[t.spec.name][pos].data_ptr()
             recs.append(r)
         spt = rk.cfg.states_per_tile
-        tiles = [math.ceil(s.n_states / spt)] * n
-        self.records[(period, s.name)] = (rk, np.stack(recs).astype(np.int64))
-        b.add("atab", rk, rk.atab_name(), recs, [math.ceil(s.n_actions / 256)] * n, 256, 0, period)
+        out["bell"] = np.stack(recs).astype(np.int64)
+        out["tiles"] = [math.ceil(s.n_states / spt)] * n
+        out["atab_tiles"] = [math.ceil(s.n_actions / 256)] * n
+        return out
+
+    # ---- device addresses of slot-indexed buffers, per instance
+    def _geom(self, key, t, slot_axis: int):
+        """(base address, per-instance offsets, per-slot step) of a buffer."""
+        g = self._geo.get(key)
+        if g is None:
+            st = [x * t.element_size() for x in t.stride()]
+            g = self._geo[key] = (t.data_ptr(), self._ar * st[1 - slot_axis], st[slot_axis])
+        return g
+
+    def _vptrs_many(self, name: str, periods: np.ndarray, pol: bool = False) -> np.ndarray:
+        """(periods, instances) device addresses of V[name] (or the policy)."""
+        base, inst, step = self._geom(("pol" if pol else "V", name), (self.pol if pol else self.V)[name], 1)
+        slots = np.array([self.slot[name][int(p)] for p in periods], dtype=np.int64)
+        return base + inst[None, :] + slots[:, None] * step
+
+    def _cptrs_many(self, name: str, field: str, periods: np.ndarray) -> np.ndarray:
+        """(periods, instances) device addresses of a DC-EGM carry field
+        (a two-slot ring indexed by period parity)."""
+        base, inst, step = self._geom(("egm", name, field), self.egm[name][field], 0)
+        return base + inst[None, :] + (np.asarray(periods, dtype=np.int64)[:, None] % 2) * step
+
+    def _group_periods(self, s: RegimeSpec, targets) -> np.ndarray:
+        return np.array([p for p in s.active_periods if self.eng.targets_at(s, p) == targets], dtype=np.int64)
+
+    def _age_words(self, periods: np.ndarray) -> np.ndarray:
+        ages = self.eng.model.ages.values
+        return np.array([_f2w(float(ages[int(p)])) for p in periods], dtype=np.int64)
+
+    def _gs_group(self, rk: RegimeKernels, s: RegimeSpec, targets, pkey) -> dict:
+        """Records of every period of one grid-search (regime, target set)
+        group: (periods, instances, words) arrays built from one template and
+        the words that vary with the period (period, age, slot addresses)."""
+        pa = self._group_periods(s, targets)
+        tm = self._gs_template(rk, int(pa[0]), s, targets, pkey)
+        P = len(pa)
+        agew = self._age_words(pa)
+        g = {"index": {int(p): k for k, p in enumerate(pa)}, "tiles": tm["tiles"], "atab_tiles": tm["atab_tiles"],
+             "taste_words": [(rk.W_TASTE, s)] if s.taste_shocks else []}
+        G = np.repeat(tm["bell"][None], P, axis=0)
+        G[:, :, rk.W_V] = self._vptrs_many(s.name, pa)
+        G[:, :, rk.W_POL] = self._vptrs_many(s.name, pa, pol=True)
+        G[:, :, rk.W_PERIOD] = pa[:, None]
+        G[:, :, rk.W_AGE] = agew[:, None]
+        for w, tname in tm["tv"]:
+            G[:, :, w] = self._vptrs_many(tname, pa + 1)
+        g["rows"] = G
+        g["expect"] = []
+        for t, erows, tiles in tm["expect"]:
+            X = np.repeat(erows[None], P, axis=0)
+            X[:, :, 0] = self._vptrs_many(t.spec.name, pa + 1)
+            X[:, :, 4] = pa[:, None]
+            X[:, :, 5] = agew[:, None]
+            g["expect"].append((t, X, tiles))
+        return g
+
+    def _gs_launches(self, b: "_Records", rk: RegimeKernels, period: int, s: RegimeSpec, targets, pkey) -> None:
+        """Kernel (b) and (a0, a) launches of one grid-search step."""
+        key = ("gs", s.name, targets, pkey)
+        g = self._grp.get(key)
+        if g is None:
+            g = self._grp[key] = self._gs_group(rk, s, targets, pkey)
+        k = g["index"][period]
+        for t, X, tiles in g["expect"]:
+            b.add("expect", rk, rk.expect_name(t), X[k], tiles, 256, 0, period)
+        rows = g["rows"][k]
+        self.records[(period, s.name)] = (rk, rows)
+        b.add("atab", rk, rk.atab_name(), rows, g["atab_tiles"], 256, 0, period)
         # kernel (a) reads the same records
-        b.add_same_records("bellman", rk, rk.bellman_name(), tiles, rk.cfg.block, rk.smem_bytes, period)
+        b.add_same_records("bellman", rk, rk.bellman_name(), g["tiles"], rk.cfg.block, rk.smem_bytes, period)
+
 
     def ensure_sim_records(self, upload: bool = True) -> None:
         """Grid-search records of the endogenous-grid regimes.
@@ -470,6 +579,7 @@ class SolvePlan:
             if pkey not in self.params:
                 vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in self.resolvers]
                 self.params[pkey] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                self._packers[pkey] = lambda r, tr=rk.tr: tr.pack_params(tr.values_for(r))
             for t in rk.targets:
                 if t.scalar or not (t.needs_contraction or fp32):
                     continue
@@ -487,9 +597,7 @@ class SolvePlan:
                 self.atab[k] = torch.empty((n, words), dtype=torch.int32, device=dev)
             self._gs_launches(b, rk, period, s, targets, pkey)
         # only the inputs of the simulation: drop the Bellman launches
-        keep = [k for k, l in enumerate(b.launches) if l.kind != "bellman"]
-        b.launches = [b.launches[k] for k in keep]
-        b.host = [b.host[k] for k in keep]
+        b.keep(lambda l: l.kind != "bellman")
         self.sim_launches = b.launches
         self._sim_rec = b
         if upload:
@@ -501,10 +609,25 @@ class SolvePlan:
         """(engine, Bellman records per (period, regime), row) of instance `idx`."""
         return self.eng, self.records, idx
 
+    def load_params(self, slot: int, params) -> None:
+        """Make instance `slot` solve `params`: its parameter vectors (device,
+        copied on the current stream) and its taste-shock words (host
+        records: build the launches after this)."""
+        torch = self.torch
+        res = self.eng.resolver(params)
+        self.resolvers[slot] = res
+        for key, pack in self._packers.items():
+            self.params[key][slot].copy_(torch.from_numpy(np.asarray(pack(res), dtype=np.float64)))
+        for g in self._grp.values():
+            for w, spec in g["taste_words"]:
+                g["rows"][:, slot, w] = _f2w(res.taste_scale(spec.name) if spec.taste_shocks else 0.0)
+
     # ------------------------------------------------------------- DC-EGM
-    def _egm_launches(self, ek, period, s, targets, age, resolvers, rec: "_Records") -> None:
-        """Records and launches of one DC-EGM period: candidates (c1), FUES,
-        carry marginal utilities, publication on the state grid."""
+    def _egm_template(self, ek, period, s, targets, age, resolvers) -> dict:
+        """Records of one DC-EGM period (every instance); other periods of the
+        same regime and target set differ only in the period, the age and the
+        slot addresses."""
+        out = {"carry": []}
         n = self.n
         er = ek.er
         b = self.egm[s.name]
@@ -524,11 +647,12 @@ class SolvePlan:
             for wname, arr in zip(("W_CG", "W_CC", "W_CV", "W_CS"), b["cand"]):
                 r[getattr(ek, wname)] = arr[i].data_ptr()
             r[ek.W_EV0] = b["ev0"][i].data_ptr()
-            r[ek.W_RG] = b["rg"][slot, i].data_ptr()
-            r[ek.W_RC] = b["rc"][slot, i].data_ptr()
-            r[ek.W_RV] = b["rv"][slot, i].data_ptr()
-            r[ek.W_MU] = b["mu"][slot, i].data_ptr()
-            r[ek.W_NK] = b["nk"][slot, i].data_ptr()
+            cslot = period % 2
+            r[ek.W_RG] = b["rg"][cslot, i].data_ptr()
+            r[ek.W_RC] = b["rc"][cslot, i].data_ptr()
+            r[ek.W_RV] = b["rv"][cslot, i].data_ptr()
+            r[ek.W_MU] = b["mu"][cslot, i].data_ptr()
+            r[ek.W_NK] = b["nk"][cslot, i].data_ptr()
             r[ek.W_V] = self.V[s.name][i, slot].data_ptr()
             r[ek.W_POL] = self.pol[s.name][i, slot].data_ptr()
             r[ek.W_NPAD] = b["npad"]
@@ -539,39 +663,91 @@ class SolvePlan:
                     continue
                 if t.next_R is None:
                     r[w["scalar"]] = self.V[t.spec.name][i, tslot].data_ptr()
+                    if i == 0:
+                        out["carry"].append((w["scalar"], t.spec.name, None))
                     continue
+                if i == 0:
+                    for f in ("rg", "rv", "mu", "nk"):
+                        out["carry"].append((w[f], t.spec.name, f))
                 cb = self.egm[t.spec.name]
-                r[w["rg"]] = cb["rg"][tslot, i].data_ptr()
-                r[w["rv"]] = cb["rv"][tslot, i].data_ptr()
-                r[w["mu"]] = cb["mu"][tslot, i].data_ptr()
-                r[w["nk"]] = cb["nk"][tslot, i].data_ptr()
+                r[w["rg"]] = cb["rg"][(period + 1) % 2, i].data_ptr()
+                r[w["rv"]] = cb["rv"][(period + 1) % 2, i].data_ptr()
+                r[w["mu"]] = cb["mu"][(period + 1) % 2, i].data_ptr()
+                r[w["nk"]] = cb["nk"][(period + 1) % 2, i].data_ptr()
                 r[w["npad"]] = cb["npad"]
                 r[w["taste"]] = _f2w(resolvers[i].taste_scale(t.spec.name) if t.spec.taste_shocks else 0.0)
             recs.append(r)
-        cname, uname, pname = ek.names()
         nrow, npad, ncand = b["nrow"], b["npad"], b["ncand"]
         ns = nrow // er.n_disc_actions
-        add_launch = rec.add
-        add_launch("egm", ek, cname, recs, [math.ceil(nrow * len(er.savings) / 256)] * n, 256, 0, period)
-        # FUES over every instance's candidate rows (one tile per row)
         cg, cc, cv, cs = b["cand"]
         frecs = []
         for i in range(n):
             fr = np.zeros(12, dtype=np.int64)
             fr[0], fr[1], fr[2], fr[3] = cg[i].data_ptr(), cc[i].data_ptr(), cv[i].data_ptr(), cs[i].data_ptr()
-            fr[4], fr[5], fr[6] = b["rg"][slot, i].data_ptr(), b["rc"][slot, i].data_ptr(), b["rv"][slot, i].data_ptr()
-            fr[7] = b["nk"][slot, i].data_ptr()
             fr[8], fr[9], fr[10] = nrow, ncand, npad
             fr[11] = _f2w(er.jump_thresh)
             frecs.append(fr)
+        out["recs"] = np.stack(recs).astype(np.int64)
+        out["fues"] = np.stack(frecs).astype(np.int64)
+        out["tiles_c"] = [math.ceil(nrow * len(er.savings) / 256)] * n
+        out["tiles_f"] = [nrow] * n
+        out["tiles_u"] = [math.ceil(nrow * npad / 256)] * n
+        out["tiles_p"] = [math.ceil(ns * grid.numel() / 256)] * n
+        return out
+
+    def _egm_group(self, ek, s: RegimeSpec, targets, resolvers) -> dict:
+        """Records of every period of one DC-EGM (regime, target set) group."""
+        pa = self._group_periods(s, targets)
+        age0 = float(self.eng.model.ages.values[int(pa[0])])
+        tm = self._egm_template(ek, int(pa[0]), s, targets, age0, resolvers)
+        P = len(pa)
+        name = s.name
+        G = np.repeat(tm["recs"][None], P, axis=0)
+        G[:, :, ek.W_PERIOD] = pa[:, None]
+        G[:, :, ek.W_AGE] = self._age_words(pa)[:, None]
+        for w, f in ((ek.W_RG, "rg"), (ek.W_RC, "rc"), (ek.W_RV, "rv"), (ek.W_MU, "mu"), (ek.W_NK, "nk")):
+            G[:, :, w] = self._cptrs_many(name, f, pa)
+        G[:, :, ek.W_V] = self._vptrs_many(name, pa)
+        G[:, :, ek.W_POL] = self._vptrs_many(name, pa, pol=True)
+        for w, tname, f in tm["carry"]:
+            G[:, :, w] = self._vptrs_many(tname, pa + 1) if f is None else self._cptrs_many(tname, f, pa + 1)
+        F = np.repeat(tm["fues"][None], P, axis=0)
+        for w, f in ((4, "rg"), (5, "rc"), (6, "rv"), (7, "nk")):
+            F[:, :, w] = self._cptrs_many(name, f, pa)
+        g = {k: tm[k] for k in ("tiles_c", "tiles_f", "tiles_u", "tiles_p")}
+        g.update({"index": {int(p): k for k, p in enumerate(pa)}, "rows": G, "fues": F})
+        tw = [(ek.W_TASTE, s)]
+        for t, w in zip(ek.er.targets, ek.W_T):
+            if not t.unreachable and t.next_R is not None:
+                tw.append((w["taste"], t.spec))
+        g["taste_words"] = tw
+        return g
+
+    def _egm_launches(self, ek, period, s, targets, age, resolvers, rec: "_Records") -> None:
+        """Launches of one DC-EGM period: candidates (c1), FUES, carry
+        marginal utilities, publication on the state grid."""
+        key = ("egm", s.name, targets)
+        g = self._grp.get(key)
+        if g is None:
+            g = self._grp[key] = self._egm_group(ek, s, targets, resolvers)
+        k = g["index"][period]
+        er = ek.er
+        name = s.name
+        rows = g["rows"][k]
+        cname, uname, pname = ek.names()
+        rec.add("egm", ek, cname, rows, g["tiles_c"], 256, 0, period)
+        # FUES over every instance's candidate rows (one tile per row)
+        b = self.egm[name]
+        ncand = b["ncand"]
         if ncand <= FUES_SMEM_MAX_N:
-            add_launch("fues", None, "lcmx_fues_step", frecs, [nrow] * n, 0, ncand, period)
+            rec.add("fues", None, "lcmx_fues_step", g["fues"][k], g["tiles_f"], 0, ncand, period)
         else:
             rec.append(
-                Launch("fues", ("fues", s.name, slot, er.jump_thresh), "lcmx_fues_scan", 0, 0, n * nrow, 0, 0, 0, period)
+                Launch("fues", ("fues", name, period % 2, er.jump_thresh), "lcmx_fues_scan", 0, 0,
+                       self.n * b["nrow"], 0, 0, 0, period)
             )
-        add_launch("egm", ek, uname, recs, [math.ceil(nrow * npad / 256)] * n, 256, 0, period)
-        add_launch("egm", ek, pname, recs, [math.ceil(ns * grid.numel() / 256)] * n, 256, 0, period)
+        rec.add("egm", ek, uname, rows, g["tiles_u"], 256, 0, period)
+        rec.add("egm", ek, pname, rows, g["tiles_p"], 256, 0, period)
 
     def _fues_item_launch(self, l: Launch, ib: int, pb: int):
         from pylcm_b200.runtime import get_context
@@ -584,20 +760,29 @@ class SolvePlan:
 
         return launch
 
-    def _fues_launch(self, spec_name, slot, thr):
+    def _fues_launch(self, spec_name, slot, thr, instances=None):
         from pylcm_b200.runtime import get_context
 
         ctx = get_context(self.eng.device)
         b = self.egm[spec_name]
         cg, cc, cv, cs = b["cand"]
-        nrows = self.n * b["nrow"]
-        ptrs = (cg.data_ptr(), cc.data_ptr(), cv.data_ptr(), cs.data_ptr())
-        outs = (b["rg"][slot].data_ptr(), b["rc"][slot].data_ptr(), b["rv"][slot].data_ptr())
-        nk = b["nk"][slot].data_ptr()
-        ws, wb, ncand, npad = b["ws"].data_ptr(), b["wb"], b["ncand"], b["npad"]
+        nrow, ncand, npad = b["nrow"], b["ncand"], b["npad"]
+        if instances is None:
+            instances = list(range(self.n))
+        calls = []
+        # one call per instance: a call touches only its instance's rows and
+        # its own part of the workspace
+        for i in instances:
+            ptrs = (cg[i].data_ptr(), cc[i].data_ptr(), cv[i].data_ptr(), cs[i].data_ptr())
+            outs = (b["rg"][slot, i].data_ptr(), b["rc"][slot, i].data_ptr(), b["rv"][slot, i].data_ptr())
+            nk = b["nk"][slot, i].data_ptr()
+            wb = ctx.fues_workspace_bytes(nrow, ncand)
+            ws = b["ws"].data_ptr() + i * wb
+            calls.append((ptrs, outs, nk, ws, wb))
 
         def launch(stream):
-            ctx.fues_scan(*ptrs, nrows, ncand, thr, *outs, npad, nk, ws, wb, stream)
+            for ptrs, outs, nk, ws, wb in calls:
+                ctx.fues_scan(*ptrs, nrow, ncand, thr, *outs, npad, nk, ws, wb, stream)
 
         return launch
 
@@ -610,7 +795,7 @@ class SolvePlan:
         out = []
         for l in launches:
             if l.kind == "fues":
-                out.append(self._fues_item_launch(l, ib, pb) if l.module is None else self._fues_launch(*l.module[1:]))
+                out.append(self._fues_item_launch(l, ib, pb) if l.module is None else self._fues_launch(*l.module[1:4]))
                 continue
             out.append(
                 l.module.module.prepared(
@@ -682,8 +867,9 @@ class BatchPlan:
     A family is a set of models whose regimes generate the same kernels:
     the same functions and state / action structure, with grid sizes,
     horizons (T) and parameters free per instance -- they are item words.
-    Each instance gets its own buffers (a one-instance plan); the launches
-    of all instances are merged:
+    The instances are slots of solve plans (`slots`: (plan, slot) pairs,
+    e.g. a server's pooled plans) or, from `members` ((engine, params)
+    pairs), one-slot plans built here.  Their launches are merged:
 
     - the solve aligns instances by steps from the end (step k is period
       T_i - 1 - k of instance i) and, within a step, merges the i-th launch
@@ -691,32 +877,39 @@ class BatchPlan:
       covers every instance with its own tiles;
     - the simulation inputs (expectation and action tables of a period) are
       merged by (period, position, kernel) the same way.
-
-    The upper-envelope scan (kernel c's FUES stage) runs per instance.
     """
 
-    def __init__(self, members: Sequence) -> None:
+    def __init__(self, members: Sequence = (), slots: Sequence | None = None) -> None:
         import torch
 
         self.torch = torch
-        if not members:
+        if slots is None:
+            slots = [(SolvePlan(eng, [p], upload=False), 0) for eng, p in members]
+        if not slots:
             raise ValueError("empty batch")
-        self.plans = [SolvePlan(eng, [p], upload=False) for eng, p in members]
-        self.n = len(self.plans)
-        self.dev = self.plans[0].dev
+        self.slots = list(slots)
+        self.n = len(self.slots)
+        by_plan: dict[int, tuple] = {}
+        for pl, k in self.slots:
+            by_plan.setdefault(id(pl), (pl, []))[1].append(k)
+        self._by_plan = list(by_plan.values())
+        self.plans = [pl for pl, _ in self._by_plan]
+        self.dev = self.slots[0][0].dev
         self.launches, self.items, self.prefix = self._merge(
-            [(pl, pl._rec, pl.launches, lambda l, pl=pl: pl.eng.model.n_periods - 1 - l.period) for pl in self.plans]
+            [(pl, pl._rec, pl.launches, lambda l, pl=pl: pl.eng.model.n_periods - 1 - l.period, sl)
+             for pl, sl in self._by_plan]
         )
         self._prepared = None
         self._inputs = None
 
     def _merge(self, sources):
-        """Merge per-instance launch lists by (key, position within key, kernel)."""
+        """Merge launch lists (restricted to the given slots of each plan) by
+        (key, position within key, kernel)."""
         by_key: dict[int, list] = {}
-        for pl, rec, launches, key_of in sources:
+        for pl, rec, launches, key_of, sl in sources:
             seq: dict[int, list] = {}
             for l, h in zip(launches, rec.host):
-                seq.setdefault(key_of(l), []).append((pl, l, h))
+                seq.setdefault(key_of(l), []).append((pl, l, h, sl))
             for k, lst in seq.items():
                 by_key.setdefault(k, []).append(lst)
         b = _Records()
@@ -728,17 +921,22 @@ class BatchPlan:
                 for lst in lists:
                     if j >= len(lst):
                         continue
-                    pl, l, h = lst[j]
+                    pl, l, h, sl = lst[j]
                     if l.kind == "fues" and l.module is not None:
-                        b.append(Launch("fues", (pl,) + tuple(l.module[1:]), l.kernel, 0, 0, l.n_items, 0, 0, 0, k))
+                        b.append(Launch("fues", (pl,) + tuple(l.module[1:4]) + (tuple(sl),), l.kernel, 0, 0,
+                                        l.n_items, 0, 0, 0, k))
                         continue
                     gk = (l.kind, l.kernel, l.module.key if hasattr(l.module, "key") else id(l.module))
-                    groups.setdefault(gk, []).append((l, h))
+                    arr, tiles = h
+                    if len(sl) != arr.shape[0] or sl != list(range(arr.shape[0])):
+                        arr = arr[sl]
+                        tiles = [tiles[i] for i in sl]
+                    groups.setdefault(gk, []).append((l, arr, tiles))
                 for gk, members in groups.items():
                     l0 = members[0][0]
-                    recs = [row for _, h in members for row in h[0]]
-                    tiles = [t for _, h in members for t in h[1]]
-                    smem = max(l.smem for l, _ in members)  # FUES: the longest candidate row
+                    recs = members[0][1] if len(members) == 1 else np.concatenate([a for _, a, _ in members])
+                    tiles = [t for _, _, ts in members for t in ts]
+                    smem = max(l.smem for l, _, _ in members)  # FUES: the longest candidate row
                     b.add(l0.kind, l0.module, l0.kernel, recs, tiles, l0.block, smem, k)
         items, prefix = b.tensors(self.torch, self.dev)
         return b.launches, items, prefix
@@ -752,8 +950,8 @@ class BatchPlan:
                 if l.module is None:
                     out.append(SolvePlan._fues_item_launch(self, l, ib, pb))
                 else:
-                    pl, name, slot, thr = l.module
-                    out.append(pl._fues_launch(name, slot, thr))
+                    pl, name, slot, thr, sl = l.module
+                    out.append(pl._fues_launch(name, slot, thr, sl))
                 continue
             out.append(
                 l.module.module.prepared(
@@ -779,15 +977,14 @@ class BatchPlan:
         if self._inputs is not None:
             return
         sources = []
-        for pl in self.plans:
+        for pl, sl in self._by_plan:
             pl.ensure_sim_records(upload=False)
-            keep = [(l, h) for l, h in zip(pl.launches, pl._rec.host) if l.kind in ("expect", "atab")]
             rec = _Records()
-            rec.launches = [l for l, _ in keep]
-            rec.host = [h for _, h in keep]
-            sources.append((pl, rec, rec.launches, lambda l: l.period))
+            rec.launches, rec.host, rec.shared = list(pl._rec.launches), list(pl._rec.host), list(pl._rec.shared)
+            rec.keep(lambda l: l.kind in ("expect", "atab"))
+            sources.append((pl, rec, rec.launches, lambda l: l.period, sl))
             if pl.sim_launches:
-                sources.append((pl, pl._sim_rec, pl.sim_launches, lambda l: l.period))
+                sources.append((pl, pl._sim_rec, pl.sim_launches, lambda l: l.period, sl))
         launches, items, prefix = self._merge(sources)
         self._inputs = (launches, items, prefix, self._prepare(launches, items, prefix))
 
@@ -799,8 +996,9 @@ class BatchPlan:
                 launch(stream)
 
     def instance(self, idx: int):
-        pl = self.plans[idx]
-        return pl.eng, pl.records, 0
+        pl, slot = self.slots[idx]
+        return pl.eng, pl.records, slot
 
     def result(self, i: int) -> tuple[dict, dict]:
-        return self.plans[i].result(0)
+        pl, slot = self.slots[i]
+        return pl.result(slot)

@@ -15,10 +15,11 @@ simulated-moments estimation.  This module runs a stream of such requests:
   `max_batch` -- into one job: one heterogeneous solve plan over the batch
   (one launch per (step, kernel) covers every instance, whatever its grid
   sizes and horizon) and one simulation plan over it;
-- a job is admitted only when its HBM footprint (value and policy arrays of
-  all periods, expectation and action tables, DC-EGM carry rows, simulation
-  buffers) fits the budget left by the jobs in flight; otherwise it waits
-  for memory to free up;
+- the requests' solve slots come from per-model pools kept on the device
+  (their item records are built once); a request is admitted when a slot and
+  its simulation buffers fit the HBM budget left by the pools and the jobs
+  in flight -- idle pools of other models are evicted, least recently used
+  first -- and otherwise waits for memory to free up;
 - jobs on different streams overlap on the device; a job's result (per
   period simulated moments, optionally the value functions) is copied to
   pinned host memory on its stream and the request completes when the host
@@ -79,19 +80,15 @@ class Result:
         return self.finished - self.arrival
 
 
-def footprint_bytes(eng: SolveEngine, n_agents: int) -> int:
-    """HBM bytes one solve+simulate instance of `eng`'s model holds.
-
+def solve_bytes(eng: SolveEngine) -> int:
+    """HBM bytes one solve instance (a pool slot) of `eng`'s model holds:
     T x states value (float64) and policy (int32) arrays per regime, the
     expectation tables (float64, plus float32 copies in the single-precision
-    search), the action tables, the DC-EGM carry rows and candidates, and
-    the simulation's per-period subject arrays.
-    """
+    search), the action tables, the DC-EGM carry rows (two-period ring) and
+    candidates."""
     from pylcm_b200.egm import is_egm
 
-    model = eng.model
     specs = eng.specs
-    T = model.n_periods
     fp32 = eng.precision == "fp32"
     b = 0
     for s in specs:
@@ -105,26 +102,56 @@ def footprint_bytes(eng: SolveEngine, n_agents: int) -> int:
             solver = s.solver
             n_cand = int(solver.n_constrained_points) + len(solver.savings_grid.to_numpy())
             n_pad = int(np.ceil(solver.refined_grid_factor * n_cand))
-            b += slots * n_rows * (4 * n_pad * 8 + 4)  # refined grid, policy, value, u'(c); counts
+            b += 2 * n_rows * (4 * n_pad * 8 + 4)  # refined grid, policy, value, u'(c); counts
             b += n_rows * n_cand * 8 * 4 * 2  # candidates + envelope workspace
         # expectation tables of the targets (at most one per target and target set)
         for t in specs:
             if t.states and not s.terminal:
                 b += t.n_states * (8 + (4 if fp32 else 0))
         b += 4 * s.n_actions * 4  # action table
-    names = sorted({a.name for s in specs for a in s.states})
-    anames = sorted({a.name for s in specs for a in s.actions})
-    b += n_agents * (T + 1) * (8 * len(names) + 4)
-    b += n_agents * T * (8 + 4 + 8 * len(anames))
     return int(b)
 
 
+def sim_bytes(eng: SolveEngine, n_agents: int) -> int:
+    """HBM bytes of the simulation of `n_agents` subjects: per period their
+    states, regime, value, action index and actions."""
+    specs = eng.specs
+    T = eng.model.n_periods
+    names = {a.name for s in specs for a in s.states}
+    anames = {a.name for s in specs for a in s.actions}
+    return int(n_agents * (T + 1) * (8 * len(names) + 4) + n_agents * T * (8 + 4 + 8 * len(anames)))
+
+
+def footprint_bytes(eng: SolveEngine, n_agents: int) -> int:
+    """HBM bytes one solve+simulate instance of `eng`'s model holds."""
+    return solve_bytes(eng) + sim_bytes(eng, n_agents)
+
+
+class _Pool:
+    """Device-resident solve slots of one model: a solve plan over `n_slots`
+    instances with its item records (all periods) built once; a request
+    borrows a slot for one job."""
+
+    def __init__(self, eng: SolveEngine, params, n_slots: int, nbytes: int) -> None:
+        from pylcm_b200.engine import SolvePlan
+
+        self.plan = SolvePlan(eng, [params] * n_slots, upload=False)
+        self.plan.ensure_sim_records(upload=False)
+        self.n_slots = n_slots
+        self.free = list(range(n_slots))
+        self.nbytes = nbytes
+        self.last_used = 0.0
+
+    @property
+    def idle(self) -> bool:
+        return len(self.free) == self.n_slots
+
+
 class _Job:
-    def __init__(self, family, reqs, stream, plan, sim, host, event, nbytes, admitted, v_host, lengths) -> None:
+    def __init__(self, family, reqs, stream, plan, sim, host, event, admitted, v_host, lengths, slots) -> None:
         self.family, self.reqs, self.stream = family, reqs, stream
-        self.lengths = lengths
         self.plan, self.sim, self.host, self.event = plan, sim, host, event
-        self.nbytes, self.admitted, self.v_host = nbytes, admitted, v_host
+        self.admitted, self.v_host, self.lengths, self.slots = admitted, v_host, lengths, slots
 
 
 class Server:
@@ -134,17 +161,28 @@ class Server:
                  the fast form) or "fp64" (the plain form);
     max_batch -- most requests of one family per job;
     n_streams -- jobs in flight at once;
-    hbm_budget_bytes -- admission budget (default: half the free HBM).
+    hbm_budget_bytes -- admission budget (default: half the free HBM);
+    pool_slots -- solve slots allocated at a time for one model.
+
+    Device state: per model, pools of solve slots (value and policy arrays,
+    expectation / action tables, DC-EGM carry rows) whose item records are
+    built once; a job borrows one slot per request and writes only the
+    request's parameters into it.  Admission: a request needs a free slot of
+    its model -- or room in the budget for a new pool, after evicting idle
+    pools of other models, least recently used first -- and room for its
+    simulation buffers.  The budget counts every pool and the simulation
+    buffers of the jobs in flight.
     """
 
     def __init__(self, device: int = 0, precision: str = "fp32", max_batch: int = 32, n_streams: int = 4,
-                 hbm_budget_bytes: int | None = None, configs: Mapping | None = None) -> None:
+                 hbm_budget_bytes: int | None = None, configs: Mapping | None = None, pool_slots: int = 4) -> None:
         import torch
 
         self.torch = torch
         self.device = device
         self.precision = precision
         self.max_batch = int(max_batch)
+        self.pool_slots = int(pool_slots)
         self.dev = torch.device("cuda", device)
         self.streams = [torch.cuda.Stream(device=self.dev) for _ in range(int(n_streams))]
         if hbm_budget_bytes is None:
@@ -154,9 +192,12 @@ class Server:
         self.configs = dict(configs or {})
         self._engines: dict[Hashable, SolveEngine] = {}
         self._family_cfg: dict[Hashable, dict] = {}
+        self._pools: dict[Hashable, list[_Pool]] = {}
         self.in_use = 0
         self.peak_in_use = 0
         self.jobs_run = 0
+        self.pools_built = 0
+        self.pools_evicted = 0
         self.batch_sizes: list[int] = []
         self.host_launch_s = 0.0  # host time building and issuing jobs
         self.host_finish_s = 0.0  # host time unpacking results
@@ -180,20 +221,67 @@ class Server:
             self._engines[req.key] = eng
         return eng
 
+    @staticmethod
+    def _n_agents(req: Request) -> int:
+        return int(np.asarray(req.initial_conditions["regime_id"]).shape[0])
+
     def footprint(self, req: Request) -> int:
-        n = int(np.asarray(req.initial_conditions["regime_id"]).shape[0])
-        return footprint_bytes(self.engine(req), n)
+        """HBM bytes of one request alone: a one-slot pool and its simulation."""
+        eng = self.engine(req)
+        return solve_bytes(eng) + sim_bytes(eng, self._n_agents(req))
+
+    def _evict(self, need: int, keep_key) -> None:
+        """Free idle pools of other models (least recently used first) until
+        `need` more bytes fit the budget."""
+        idle = [(pool.last_used, key, pool) for key, pools in self._pools.items() if key != keep_key
+                for pool in pools if pool.idle]
+        for _, key, pool in sorted(idle, key=lambda x: x[0]):
+            if self.in_use + need <= self.budget:
+                return
+            self._pools[key].remove(pool)
+            self.in_use -= pool.nbytes
+            self.pools_evicted += 1
+
+    def _acquire(self, req: Request, now: float):
+        """A free slot for `req` (building a pool if the budget allows) and
+        the admission of its simulation buffers; None when it must wait."""
+        eng = self.engine(req)
+        sb = sim_bytes(eng, self._n_agents(req))
+        pools = self._pools.setdefault(req.key, [])
+        pool = next((p for p in pools if p.free), None)
+        n_slots = self.pool_slots
+        if pool is None:
+            # a smaller pool when a full one does not fit
+            self._evict(sb + n_slots * solve_bytes(eng), req.key)
+            while n_slots > 1 and self.in_use + sb + n_slots * solve_bytes(eng) > self.budget:
+                n_slots //= 2
+        need = sb + (0 if pool is not None else n_slots * solve_bytes(eng))
+        if self.in_use + need > self.budget:
+            return None
+        if pool is None:
+            pool = _Pool(eng, req.params, n_slots, n_slots * solve_bytes(eng))
+            pools.append(pool)
+            self.pools_built += 1
+            self.in_use += pool.nbytes
+        pool.last_used = now
+        self.in_use += sb
+        self.peak_in_use = max(self.peak_in_use, self.in_use)
+        return pool, pool.free.pop(0), sb
 
     # ------------------------------------------------------------------ jobs
-    def _launch(self, family, reqs: list, stream, nbytes: int, now: float) -> _Job:
+    def _launch(self, family, reqs: list, slots: list, stream, now: float) -> _Job:
         from pylcm_b200.engine import BatchPlan
         from pylcm_b200.simulate import SimPlan
 
         torch = self.torch
         with torch.cuda.stream(stream):
-            plan = BatchPlan([(self.engine(r), r.params) for r in reqs])
-            plan.run(stream.cuda_stream)
+            # every host->device copy happens here, before the job's first kernel:
+            # a pageable copy waits for the work queued before it on the stream
+            for (pool, slot, _), r in zip(slots, reqs):
+                pool.plan.load_params(slot, r.params)
+            plan = BatchPlan(slots=[(pool.plan, slot) for pool, slot, _ in slots])
             sim = SimPlan(plan, instances=[(k, r.initial_conditions, r.seed) for k, r in enumerate(reqs)])
+            plan.run(stream.cuda_stream)
             sim.run(stream.cuda_stream)
             rows, lengths = [], []
             for b in sim.inst:
@@ -211,17 +299,18 @@ class Server:
             v_host = {}
             for k, r in enumerate(reqs):
                 if r.return_V:
+                    pl, slot = plan.slots[k]
                     vh = {}
-                    for name, v in plan.plans[k].V.items():
-                        t = torch.empty(tuple(v[0].shape), dtype=torch.float64, pin_memory=True)
-                        t.copy_(v[0], non_blocking=True)
+                    for name, v in pl.V.items():
+                        t = torch.empty(tuple(v[slot].shape), dtype=torch.float64, pin_memory=True)
+                        t.copy_(v[slot], non_blocking=True)
                         vh[name] = t
                     v_host[k] = vh
             event = torch.cuda.Event()
             event.record(stream)
         self.jobs_run += 1
         self.batch_sizes.append(len(reqs))
-        return _Job(family, reqs, stream, plan, sim, host, event, nbytes, now, v_host, lengths)
+        return _Job(family, reqs, stream, plan, sim, host, event, now, v_host, lengths, slots)
 
     def _finish(self, job: _Job, now: float) -> list[Result]:
         arr = job.host.numpy()
@@ -238,12 +327,15 @@ class Server:
             V = None
             if k in job.v_host:
                 V = {}
-                pl = job.plan.plans[k]
+                pl, slot = job.plan.slots[k]
                 for name, t in job.v_host[k].items():
                     spec = next(s for s in eng.specs if s.name == name)
-                    for p, slot in pl.slot[name].items():
-                        V.setdefault(p, {})[name] = t[slot].numpy().reshape(spec.state_shape).copy()
+                    for p, sl in pl.slot[name].items():
+                        V.setdefault(p, {})[name] = t[sl].numpy().reshape(spec.state_shape).copy()
             out.append(Result(r.rid, job.family, moments, V, r.arrival, job.admitted, now, len(job.reqs)))
+        for pool, slot, sb in job.slots:
+            pool.free.append(slot)
+            self.in_use -= sb
         return out
 
     # ------------------------------------------------------------------- run
@@ -254,14 +346,10 @@ class Server:
         the host seeing the result)."""
         torch = self.torch
         reqs = sorted(requests, key=lambda r: r.arrival)
-        foot = {}
         for r in reqs:
             fp = self.footprint(r)
             if fp > self.budget:
-                raise MemoryError(
-                    f"request {r.rid}: footprint {fp} B exceeds the HBM budget {self.budget} B"
-                )
-            foot[r.rid] = fp
+                raise MemoryError(f"request {r.rid}: footprint {fp} B exceeds the HBM budget {self.budget} B")
         waiting: dict[Hashable, collections.deque] = collections.OrderedDict()
         free = list(self.streams)
         inflight: list[_Job] = []
@@ -281,27 +369,26 @@ class Server:
             for job in list(inflight):
                 if job.event.query():
                     h0 = time.perf_counter()
-                    now = h0 - t0
-                    for res in self._finish(job, now):
+                    for res in self._finish(job, h0 - t0):
                         results[res.rid] = res
                     self.host_finish_s += time.perf_counter() - h0
                     inflight.remove(job)
                     free.append(job.stream)
-                    self.in_use -= job.nbytes
                     progressed = True
             while free and any(waiting.values()):
-                key = min((k for k, q in waiting.items() if q), key=lambda k: waiting[k][0].arrival)
-                q = waiting[key]
-                batch, nbytes = [], 0
-                while q and len(batch) < self.max_batch and self.in_use + nbytes + foot[q[0].rid] <= self.budget:
-                    nbytes += foot[q[0].rid]
+                fam = min((k for k, q in waiting.items() if q), key=lambda k: waiting[k][0].arrival)
+                q = waiting[fam]
+                h0 = time.perf_counter()
+                batch, slots = [], []
+                while q and len(batch) < self.max_batch:
+                    got = self._acquire(q[0], h0 - t0)
+                    if got is None:
+                        break  # admission: wait for memory to free up
+                    slots.append(got)
                     batch.append(q.popleft())
                 if not batch:
-                    break  # admission: wait for memory to free up
-                self.in_use += nbytes
-                self.peak_in_use = max(self.peak_in_use, self.in_use)
-                h0 = time.perf_counter()
-                inflight.append(self._launch(key, batch, free.pop(0), nbytes, h0 - t0))
+                    break
+                inflight.append(self._launch(fam, batch, slots, free.pop(0), h0 - t0))
                 self.host_launch_s += time.perf_counter() - h0
                 progressed = True
             if not progressed:
@@ -309,6 +396,8 @@ class Server:
                     time.sleep(5e-5)
                 elif i < n:
                     time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 1e-3)))
+                elif any(waiting.values()):
+                    raise MemoryError("a waiting request cannot be admitted with no job in flight")
         torch.cuda.synchronize(self.dev)
         return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]
 

@@ -159,48 +159,63 @@ class SimPlan:
             self.inst.append(b)
         self.T = max(b["T"] for b in self.inst)
         # item records: the Bellman record of (period, regime, instance) + simulation words
+        per_period: dict[int, dict[tuple, list]] = {}
+        for b in self.inst:
+            N, T = b["N"], b["T"]
+            sbytes = N * 8  # one period of a subject array (float64)
+            ibytes = N * 4  # one period of an int32 subject array
+            S0 = {n: t.data_ptr() for n, t in b["S"].items()}
+            A0 = {n: t.data_ptr() for n, t in b["A"].items()}
+            R0, V0, X0 = b["R"].data_ptr(), b["val"].data_ptr(), b["aidx"].data_ptr()
+            seed_w = np.uint64(b["seed"]).astype(np.int64)
+            tiles = math.ceil(N / 8)
+            for s in b["eng"].specs:
+                periods = [p for p in s.active_periods if p < T]
+                if not periods:
+                    continue
+                by_rk: dict[int, list] = {}
+                for p in periods:
+                    rk, base = b["records"][(p, s.name)]
+                    by_rk.setdefault(id(rk), [rk, [], []])
+                    by_rk[id(rk)][1].append(p)
+                    by_rk[id(rk)][2].append(base[b["row"]])
+                for rk, ps, bases in by_rk.values():
+                    b["eng"].module(rk)
+                    pa = np.asarray(ps, dtype=np.int64)
+                    rows = np.zeros((len(ps), rk.sim_words), dtype=np.int64)
+                    rows[:, : rk.n_words] = np.stack(bases)
+                    rows[:, rk.SW_N] = N
+                    rows[:, rk.SW_RID_IN] = R0 + pa * ibytes
+                    rows[:, rk.SW_RID_OUT] = R0 + (pa + 1) * ibytes
+                    rows[:, rk.SW_VAL] = V0 + pa * sbytes
+                    rows[:, rk.SW_AIDX] = X0 + pa * ibytes
+                    rows[:, rk.SW_SEED] = seed_w
+                    for k, a in enumerate(s.actions):
+                        rows[:, rk.SW_ACT + k] = A0[a.name] + pa * sbytes
+                    for k, a in enumerate(s.states):
+                        rows[:, rk.SW_SIN + k] = S0[a.name] + pa * sbytes
+                    for k, name in enumerate(rk.sim_out_names):
+                        rows[:, rk.SW_SOUT + k] = S0[name] + (pa + 1) * sbytes
+                    for j, p in enumerate(ps):
+                        g = per_period.setdefault(p, {}).setdefault((rk.sim_name(), rk.key), [rk, [], []])
+                        g[1].append(rows[j])
+                        g[2].append(tiles)
         recs = []
         prefs = []
         self.launches = []
         off = 0
         poff = 0
-        for period in range(self.T):
-            groups: dict[tuple, list] = {}
-            for b in self.inst:
-                if period >= b["T"]:
-                    continue
-                for s in b["eng"].specs:
-                    if period not in s.active_periods:
-                        continue
-                    rk, base = b["records"][(period, s.name)]
-                    b["eng"].module(rk)
-                    r = np.zeros(rk.sim_words, dtype=np.int64)
-                    r[: rk.n_words] = base[b["row"]]
-                    r[rk.SW_N] = b["N"]
-                    r[rk.SW_RID_IN] = b["R"][period].data_ptr()
-                    r[rk.SW_RID_OUT] = b["R"][period + 1].data_ptr()
-                    r[rk.SW_VAL] = b["val"][period].data_ptr()
-                    r[rk.SW_AIDX] = b["aidx"][period].data_ptr()
-                    r[rk.SW_SEED] = np.uint64(b["seed"]).astype(np.int64)
-                    for k, a in enumerate(s.actions):
-                        r[rk.SW_ACT + k] = b["A"][a.name][period].data_ptr()
-                    for k, a in enumerate(s.states):
-                        r[rk.SW_SIN + k] = b["S"][a.name][period].data_ptr()
-                    for k, name in enumerate(rk.sim_out_names):
-                        r[rk.SW_SOUT + k] = b["S"][name][period + 1].data_ptr()
-                    groups.setdefault((rk.sim_name(), rk.key), []).append((rk, r, math.ceil(b["N"] / 8)))
-            for members in groups.values():
-                rk = members[0][0]
-                tiles = [t for _, _, t in members]
-                pre = np.zeros(len(tiles) + 1, dtype=np.int32)
-                pre[1:] = np.cumsum(tiles)
-                pad = (-pre.size) % 4
-                prefs.append(np.concatenate([pre, np.zeros(pad, dtype=np.int32)]))
-                recs.extend(r for _, r, _ in members)
-                self.launches.append((period, rk, off, poff, len(members), int(pre[-1])))
-                off += rk.sim_words * len(members)
-                poff += pre.size + pad
-        self.items = torch.as_tensor(np.concatenate(recs), dtype=torch.int64, device=dev)
+        for period in sorted(per_period):
+            for rk, rows, tiles in per_period[period].values():
+                npre = len(tiles) + 1
+                pre = np.zeros(npre + (-npre) % 4, dtype=np.int32)
+                np.cumsum(tiles, out=pre[1:npre])
+                prefs.append(pre)
+                recs.append(np.stack(rows))
+                self.launches.append((period, rk, off, poff, len(rows), int(pre[npre - 1])))
+                off += rk.sim_words * len(rows)
+                poff += pre.size
+        self.items = torch.as_tensor(np.concatenate([r.reshape(-1) for r in recs]), dtype=torch.int64, device=dev)
         self.prefix = torch.as_tensor(np.concatenate(prefs), dtype=torch.int32, device=dev)
 
     def run(self, stream: int | None = None) -> None:

@@ -163,3 +163,28 @@ def test_footprint_estimate_covers_the_allocations():
         est = footprint_bytes(eng, 2000)
         assert 0.5 * used <= est <= 3.0 * used, (r.family, est, used)
         del bp, sim
+
+
+def test_pools_are_reused_and_evicted_without_changing_results():
+    """A second pass over the same requests reuses the pooled slots (no new
+    pools) and gives the same numbers; a budget that holds only a few pools
+    forces evictions and still gives the same numbers."""
+    reqs = E.serving_requests(10, seed=9, n_agents=300, sizes=(40, 80), horizons=(4, 7), n_consumption=60,
+                              return_V_every=1)
+    srv = Server(precision="fp32", max_batch=4, n_streams=2)
+    first = srv.run([dataclasses.replace(r) for r in reqs], realtime=False)
+    built = srv.pools_built
+    second = srv.run([dataclasses.replace(r) for r in reqs], realtime=False)
+    assert srv.pools_built == built
+    fps = [srv.footprint(r) for r in reqs]
+    tight = Server(precision="fp32", max_batch=4, n_streams=2, hbm_budget_bytes=int(3 * max(fps)), pool_slots=1)
+    third = tight.run([dataclasses.replace(r) for r in reqs], realtime=False)
+    assert tight.pools_evicted > 0
+    assert tight.peak_in_use <= tight.budget
+    for a, b, c in zip(first, second, third):
+        for name in a.moments:
+            np.testing.assert_array_equal(a.moments[name], b.moments[name])
+            np.testing.assert_array_equal(a.moments[name], c.moments[name])
+        for p in a.V:
+            for r in a.V[p]:
+                np.testing.assert_array_equal(a.V[p][r], c.V[p][r])
