@@ -504,6 +504,40 @@ __global__ void __launch_bounds__(kBlock) fues_smem_kernel(Rows rows) {
       int jidx = 0, kidx = 0;  // candidates j and k are (kidx < 0: k is a kink point)
       const double near = 16.0 * 2.220446049250313e-16;
       for (int idx = 1; idx < n; ++idx) {
+        // Runs of plain steps, 32 at a time.  While j and k are the two
+        // candidates before idx, step t keeps candidate t and only emits j
+        // when t is valid, shows no policy jump from t - 1, and is neither
+        // below t - 1 nor a savings decrease with a secant under the previous
+        // one -- all of it from the per-position tables.  Such a step leaves
+        // j = t - 1 + 1 and k = t - 1, so the next step's test is again a
+        // table lookup: the lanes test idx .. idx + 31 at once and the warp
+        // commits the leading run of passing steps (each emits its j).
+        if (kidx >= 0 && jidx == idx - 1 && kidx == jidx - 1) {
+          const int t = idx + lane;
+          bool ok = false;
+          if (t < n) {
+            const double gt = g[t], vt = v[t];
+            ok = !isnan_(gt) && !isnan_(vt) && sidx[t] == 0 && !(vt < v[t - 1]) &&
+                 !(s[t] < s[t - 1] && sec[t] < sec[t - 1]);
+          }
+          const unsigned fail = ~__ballot_sync(0xffffffffu, ok);
+          const int m = fail ? __ffs(fail) - 1 : 32;
+          if (m > 0) {
+            if (lane < m && cnt + lane < n_out) {
+              GO[cnt + lane] = g[idx - 1 + lane];
+              PO[cnt + lane] = p[idx - 1 + lane];
+              VO[cnt + lane] = v[idx - 1 + lane];
+            }
+            cnt += m;
+            const int nj = idx + m - 1;
+            gk = g[nj - 1]; pk = p[nj - 1]; vk = v[nj - 1];
+            kidx = nj - 1;
+            gj = g[nj]; pj = p[nj]; vj = v[nj]; sj = s[nj];
+            jidx = nj;
+            idx = nj;  // the loop's increment moves to the first untested step
+            continue;
+          }
+        }
         const double gi = g[idx], vi = v[idx];
         if (isnan_(gi) || isnan_(vi)) continue;
         const double pi = p[idx], si = s[idx];

@@ -199,6 +199,7 @@ class Server:
         self.pools_built = 0
         self.pools_evicted = 0
         self.batch_sizes: list[int] = []
+        self.job_gpu_ms: list[float] = []  # device time of each job (its first kernel to its result copy)
         self.host_launch_s = 0.0  # host time building and issuing jobs
         self.host_finish_s = 0.0  # host time unpacking results
 
@@ -275,12 +276,14 @@ class Server:
 
         torch = self.torch
         with torch.cuda.stream(stream):
+            t_start = torch.cuda.Event(enable_timing=True)
             # every host->device copy happens here, before the job's first kernel:
             # a pageable copy waits for the work queued before it on the stream
             for (pool, slot, _), r in zip(slots, reqs):
                 pool.plan.load_params(slot, r.params)
             plan = BatchPlan(slots=[(pool.plan, slot) for pool, slot, _ in slots])
             sim = SimPlan(plan, instances=[(k, r.initial_conditions, r.seed) for k, r in enumerate(reqs)])
+            t_start.record(stream)
             plan.run(stream.cuda_stream)
             sim.run(stream.cuda_stream)
             rows, lengths = [], []
@@ -306,11 +309,13 @@ class Server:
                         t.copy_(v[slot], non_blocking=True)
                         vh[name] = t
                     v_host[k] = vh
-            event = torch.cuda.Event()
+            event = torch.cuda.Event(enable_timing=True)
             event.record(stream)
         self.jobs_run += 1
         self.batch_sizes.append(len(reqs))
-        return _Job(family, reqs, stream, plan, sim, host, event, now, v_host, lengths, slots)
+        job = _Job(family, reqs, stream, plan, sim, host, event, now, v_host, lengths, slots)
+        job.t_start = t_start
+        return job
 
     def _finish(self, job: _Job, now: float) -> list[Result]:
         arr = job.host.numpy()
@@ -336,6 +341,7 @@ class Server:
         for pool, slot, sb in job.slots:
             pool.free.append(slot)
             self.in_use -= sb
+        self.job_gpu_ms.append(job.t_start.elapsed_time(job.event))
         return out
 
     # ------------------------------------------------------------------- run

@@ -222,6 +222,16 @@ class ParamResolver:
         return False, None
 
     def process_params(self, regime: str, state: str, proc: _Process) -> dict:
+        key = (regime, state, id(proc))
+        cache = self.__dict__.setdefault("_proc_params", {})
+        hit = cache.get(key)
+        if hit is not None:
+            return dict(hit[1])
+        out = self._process_params(regime, state, proc)
+        cache[key] = (proc, out)  # keeps `proc` alive so its id stays unique
+        return dict(out)
+
+    def _process_params(self, regime: str, state: str, proc: _Process) -> dict:
         out = dict(proc.fixed_params)
         for name in proc.runtime_param_names:
             found = False
@@ -294,7 +304,9 @@ class TracedRegime:
     def values_for(self, resolver: "ParamResolver") -> dict[str, np.ndarray]:
         """Parameter values of another parameter set, same layout as the trace."""
         out = {}
-        proc_cache: dict[str, tuple] = {}
+        # process tables of this parameter set, shared by every trace of the
+        # regime (one per target set) that packs it
+        proc_cache = resolver.__dict__.setdefault("_proc_tables", {})
         for flat in self.param_order:
             src = self.param_sources[flat]
             if src[0] == "arg":
@@ -308,14 +320,15 @@ class TracedRegime:
                 v = np.asarray(float(pp[src[2]]), dtype=np.float64)
             else:
                 state = src[1]
-                if state not in proc_cache:
+                ck = (self.spec.name, state)
+                if ck not in proc_cache:
                     ax = self.spec.state(state)
                     pp = resolver.process_params(self.spec.name, state, ax.grid)
-                    proc_cache[state] = (
+                    proc_cache[ck] = (
                         np.asarray(ax.grid.compute_gridpoints(**pp), dtype=np.float64),
                         np.asarray(ax.grid.compute_transition_probs(**pp), dtype=np.float64),
                     )
-                v = proc_cache[state][0 if src[0] == "proc_nodes" else 1]
+                v = proc_cache[ck][0 if src[0] == "proc_nodes" else 1]
             if v.shape != self.param_values[flat].shape:
                 raise InvalidParamsError(
                     f"parameter {flat} has shape {v.shape}, expected {self.param_values[flat].shape}"
@@ -325,7 +338,10 @@ class TracedRegime:
 
     def pack_params(self, values: dict | None = None) -> np.ndarray:
         values = self.param_values if values is None else values
-        layout, total = self.param_layout()
+        cached = self.__dict__.get("_layout_cache")
+        if cached is None:
+            cached = self.__dict__["_layout_cache"] = self.param_layout()
+        layout, total = cached
         vec = np.zeros(max(total, 1), dtype=np.float64)
         for name, (off, shape) in layout.items():
             v = np.asarray(values[name], dtype=np.float64).ravel()
