@@ -304,6 +304,11 @@ def run_ours(args) -> dict:
         dist.destroy_process_group()
     if rank != 0:
         return {}
+    extra = {}
+    if world == 1 and not args.no_extra:
+        extra["serving"] = run_serving(args, local)
+        extra["dcegm"] = run_dcegm(args, local)
+        extra["hc"] = run_hc(args, local)
     spec0 = model.regime_specs
     evals_per_solve = sum(s.n_states * s.n_actions * len(s.active_periods) for s in spec0)
     fl_per_eval = 20  # ~20 flops per (state, action) evaluation of the mixed part
@@ -375,43 +380,272 @@ def run_ours(args) -> dict:
         },
         "evals_per_solve": evals_per_solve,
         "clocks": clocks,
+        **extra,
         "cpu_baseline": cpu_baseline(args) if (rank == 0 and world == 1 and not args.no_cpu) else None,
     }
 
 
-def cpu_baseline(args) -> dict:
-    """The oracle (NumPy FP64 restatement) on a bounded sample: the terminal
-    period plus `cpu_periods` decision periods of one solve, extrapolated to
-    a full T-period solve."""
-    from oracle.grid_search import bellman_step
+def _rel_err(a, b) -> float:
+    a = np.asarray(a)
+    b = np.asarray(b)
+    fin = np.isfinite(b)
+    if not fin.any():
+        return 0.0
+    return float((np.abs(a[fin] - b[fin]) / np.maximum(1.0, np.abs(b[fin]))).max())
+
+
+def run_serving(args, local: int) -> dict:
+    """Serving workload (solve + simulate requests of the stochastic
+    retirement and DC-EGM retirement models, grid sizes 100..2000, T in
+    {10, 40, 60}, 10,000 simulated subjects each): capacity with every
+    request released at once, then Poisson arrivals at 0.8 x capacity for
+    end-to-end latency; the plain form is the FP64 server one request at a
+    time."""
+    import dataclasses
+
+    import torch
+
+    from pylcm_b200 import examples as E
+    from pylcm_b200.serving import Server, latency_summary
+
+    n = args.serve_requests
+    n_v = min(16, args.plain_requests, n)
+    reqs = E.serving_requests(n, seed=7, n_agents=args.agents)
+    for r in reqs[:n_v]:
+        r.return_V = True
+    srv = Server(device=local, precision="fp32", max_batch=args.serve_batch, n_streams=args.serve_streams)
+    srv.run([dataclasses.replace(r) for r in reqs], realtime=False)  # kernels compiled, pools built
+    srv.job_gpu_ms, srv.batch_sizes = [], []
+    t = time.perf_counter()
+    srv.run([dataclasses.replace(r) for r in reqs], realtime=False)
+    cap_wall = time.perf_counter() - t
+    capacity = n / cap_wall
+    cap_gpu = sum(srv.job_gpu_ms)
+    rate = 0.8 * capacity
+    arr = np.cumsum(np.random.default_rng(8).exponential(1.0 / rate, size=n))
+    reqs_p = [dataclasses.replace(r, arrival=float(a)) for r, a in zip(reqs, arr)]
+    srv.job_gpu_ms, srv.batch_sizes, srv.host_launch_s = [], [], 0.0
+    with ClockSampler(local) as clk:
+        t = time.perf_counter()
+        res = srv.run(reqs_p, realtime=True)
+        wall = time.perf_counter() - t
+    summ = latency_summary(res, wall)
+    # plain: FP64, one request at a time (compile pass first)
+    sample = reqs[: args.plain_requests]
+    pl = Server(device=local, precision="fp64", max_batch=1, n_streams=1)
+    pl.run([dataclasses.replace(r) for r in sample], realtime=False)
+    t = time.perf_counter()
+    pres = pl.run([dataclasses.replace(r) for r in sample], realtime=False)
+    pwall = time.perf_counter() - t
+    plain_rate = len(sample) / pwall
+    plain_lat = np.array([r.finished - r.admitted for r in pres]) * 1e3
+    err = 0.0
+    for a, b in zip(res[:n_v], pres[:n_v]):
+        for per in b.V:
+            for name in b.V[per]:
+                err = max(err, _rel_err(a.V[per][name], b.V[per][name]))
+    torch.cuda.synchronize()
+    return {
+        "workload": "4096-request serving stream of config 4 restated: each request the stochastic retirement "
+        "model (grid search) or the DC-EGM retirement model (taste scale none / 0.05) with prob. 1/2, wealth grid "
+        "n in {100,250,500,1000,2000}, T in {10,40,60}, beta~U[.90,.99], crra~U[1,5], r~U[.01,.06]; solve + "
+        "simulate 10,000 subjects (w0~U[1,50], income state from its stationary distribution)",
+        "requests": n,
+        "agents_per_request": args.agents,
+        "capacity_solves_per_s": capacity,
+        "arrival_rate_per_s": rate,
+        "solves_per_s": summ["solves_per_s"],
+        "p50_ms": summ["p50_ms"],
+        "p99_ms": summ["p99_ms"],
+        "mean_batch": summ["mean_batch"],
+        "gpu_busy_frac_at_capacity": cap_gpu / 1e3 / cap_wall,
+        "host_launch_s": srv.host_launch_s,
+        "plain": {
+            "solves_per_s": plain_rate,
+            "p50_service_ms": float(np.percentile(plain_lat, 50)),
+            "p99_service_ms": float(np.percentile(plain_lat, 99)),
+            "form": "fp64, max_batch 1, one stream: one request at a time",
+            "requests": len(sample),
+        },
+        "fast_vs_plain": summ["solves_per_s"] / plain_rate,
+        "capacity_vs_plain": capacity / plain_rate,
+        "max_rel_V_err_vs_fp64": err,
+        "V_checked_requests": n_v,
+        "pools_built": srv.pools_built,
+        "clocks": clk.summary(),
+    }
+
+
+def run_dcegm(args, local: int) -> dict:
+    """DC-EGM + FUES (config 2): T=40, 2000-point cubic savings grid on
+    [0, 500], wealth grid 2000 points, 16-node Gauss-Hermite income weights,
+    CRRA 2, beta 0.97, r 0.04; taste scale none / 0.05.  One solve at a time
+    (FP64, eager) and batches of `dcegm_batch` parameter draws."""
+    import torch
+
+    from pylcm_b200 import examples as E
+    from pylcm_b200.engine import SolveEngine
+    from pylcm_b200.runtime import get_context
+
+    out = {}
+    stream = torch.cuda.current_stream()
+    ctx = get_context(local)
+    for taste in (None, 0.05):
+        model = E.dcegm_model(n_periods=40, n_savings=2000, n_wealth=2000, taste=taste is not None)
+        rng = np.random.default_rng(11)
+        plist = [E.dcegm_params(seed=int(rng.integers(1 << 30)), taste_scale=taste) for _ in range(args.dcegm_batch)]
+        eng = SolveEngine(model, "fp64", device=local)
+        one = eng.plan([plist[0]])
+        one.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        counts = torch.zeros(2, dtype=torch.int64, device="cuda")
+        ms = []
+        for _ in range(3):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one.run(stream.cuda_stream)
+            counts.zero_()
+            for v in one.V.values():
+                ctx.count_nonfinite(v.data_ptr(), v.numel(), counts.data_ptr(), stream.cuda_stream)
+            _ = counts.cpu()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms.append(a.elapsed_time(b))
+        batch = eng.plan(plist)
+        batch.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        bms = []
+        for _ in range(2):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            batch.run(stream.cuda_stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            bms.append(a.elapsed_time(b))
+        err = max(_rel_err(batch.V[r][0].cpu().numpy(), one.V[r][0].cpu().numpy()) for r in one.V)
+        out["taste_none" if taste is None else "taste_0.05"] = {
+            "plain_ms_per_solve": float(np.median(ms)),
+            "plain_solves_per_s": 1e3 / float(np.median(ms)),
+            "batch": args.dcegm_batch,
+            "batched_solves_per_s": args.dcegm_batch / (float(np.median(bms)) / 1e3),
+            "batched_vs_plain": (args.dcegm_batch / float(np.median(bms))) / (1.0 / float(np.median(ms))),
+            "max_rel_V_err_batch_vs_single": err,
+        }
+    return out
+
+
+def run_hc(args, local: int) -> dict:
+    """Two continuous states (config 3): wealth 1000 x human capital 50 x a
+    32-state Markov shock (Dirichlet(1) rows), 300 consumption x 3 hours
+    actions, T=60; a batch of `hc_batch` parameter draws (beta~U[.90,.99],
+    crra~U[1,5], r~U[.01,.06]) in the fast form against one FP64 solve."""
+    import torch
+
+    from pylcm_b200 import examples as E
+    from pylcm_b200.engine import SolveEngine
+
+    stream = torch.cuda.current_stream()
+    model = E.hc_model(60, 1000, 50, 32, 300)
+    plist = [E.hc_params(seed=k) for k in range(args.hc_batch)]
+    fast = SolveEngine(model, "fp32", device=local).plan(plist)
+    plain = SolveEngine(model, "fp64", device=local).plan(plist[:1])
+    fast.run(stream.cuda_stream)
+    plain.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    res = {}
+    for name, plan, n in (("fast", fast, args.hc_batch), ("plain", plain, 1)):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        plan.run(stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        res[name] = n / (a.elapsed_time(b) / 1e3)
+    err = max(_rel_err(fast.V[r][0].cpu().numpy(), plain.V[r][0].cpu().numpy()) for r in plain.V)
+    agree = tot = 0
+    for r in plain.pol:
+        m = torch.isfinite(plain.V[r][0])
+        agree += int((fast.pol[r][0] == plain.pol[r][0])[m].sum().item())
+        tot += int(m.sum().item())
+    evals = sum(s.n_states * s.n_actions * len(s.active_periods) for s in model.regime_specs)
+    return {
+        "batch": args.hc_batch,
+        "fast_solves_per_s": res["fast"],
+        "plain_solves_per_s": res["plain"],
+        "fast_vs_plain": res["fast"] / res["plain"],
+        "q_evals_per_solve": evals,
+        "fast_q_evals_per_s": evals * res["fast"],
+        "max_rel_V_err_vs_fp64": err,
+        "policy_agreement_vs_fp64": agree / max(tot, 1),
+    }
+
+
+_W = {}
+
+
+def _cpu_init(periods, wealth, cons):
     from pylcm_b200.spec import ParamResolver
 
-    model, params = make_workload(args.periods, args.wealth, args.cons, 1)
+    model, params = make_workload(periods, wealth, cons, 1)
+    _W["model"] = model
+    _W["res"] = ParamResolver(params[0], model.fixed_params, tuple(s.name for s in model.regime_specs))
+
+
+def _cpu_rows(job):
+    from oracle.grid_search import bellman_step
+
+    name, period, rows, nxt = job
+    model = _W["model"]
     specs = model.regime_specs
-    res = ParamResolver(params[0], model.fixed_params, tuple(s.name for s in specs))
+    spec = next(s for s in specs if s.name == name)
+    V, _ = bellman_step(spec, specs, _W["res"], period, float(model.ages.values[period]), nxt, state_rows=rows)
+    return name, rows, V
+
+
+def cpu_baseline(args) -> dict:
+    """The oracle (NumPy FP64 restatement of the reference's solve) on a
+    bounded sample: the terminal period plus `cpu_periods` decision periods of
+    one solve, each period's state rows split over a pool of host processes,
+    extrapolated to a full T-period solve."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    model, _ = make_workload(args.periods, args.wealth, args.cons, 1)
+    specs = model.regime_specs
     T = model.n_periods
+    cores = max(1, min(args.cpu_cores or (os.cpu_count() or 1), 64))
     V = {}
-    t0 = time.perf_counter()
     per_period = []
-    for period in range(T - 1, T - 2 - args.cpu_periods, -1):
-        ts = time.perf_counter()
-        V[period] = {}
-        for s in specs:
-            if period in s.active_periods:
-                V[period][s.name], _ = bellman_step(
-                    s, specs, res, period, float(model.ages.values[period]), V.get(period + 1, {})
-                )
-        per_period.append(time.perf_counter() - ts)
+    with cf.ProcessPoolExecutor(cores, mp_context=mp.get_context("spawn"), initializer=_cpu_init,
+                                initargs=(args.periods, args.wealth, args.cons)) as ex:
+        list(ex.map(_cpu_rows, [(specs[-1].name, T - 1, np.arange(1), {})] * cores))  # start the workers
+        t0 = time.perf_counter()
+        for period in range(T - 1, T - 2 - args.cpu_periods, -1):
+            ts = time.perf_counter()
+            nxt = V.get(period + 1, {})
+            jobs = []
+            for s in specs:
+                if period in s.active_periods:
+                    for rows in np.array_split(np.arange(s.n_states), cores):
+                        if rows.size:
+                            jobs.append((s.name, period, rows, nxt))
+            out = {}
+            for name, rows, v in ex.map(_cpu_rows, jobs):
+                out.setdefault(name, np.empty(next(x for x in specs if x.name == name).n_states))[rows] = v
+            V[period] = {n: v.reshape(next(x for x in specs if x.name == n).state_shape) for n, v in out.items()}
+            per_period.append(time.perf_counter() - ts)
     terminal = per_period[0]
     decision = float(np.mean(per_period[1:]))
     est = terminal + (T - 1) * decision
     return {
         "value": 1.0 / est,
         "unit": UNIT,
-        "cores": 1,
+        "cores": cores,
         "kind": "port",
         "sample": f"terminal period + {args.cpu_periods} decision periods of one solve timed "
-        f"({time.perf_counter() - t0:.1f} s), extrapolated to T={T}",
+        f"({time.perf_counter() - t0:.1f} s, state rows split over {cores} processes), extrapolated to T={T}",
         "seconds_per_solve_est": est,
     }
 
@@ -426,7 +660,7 @@ def run_reference(args) -> dict:
     for _ in range(max(1, min(args.steps, 2))):
         vals.append(cpu_baseline(args)["value"])
     v = float(np.mean(vals))
-    cb = cpu_baseline.__doc__
+    cores = max(1, min(args.cpu_cores or (os.cpu_count() or 1), 64))
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -442,7 +676,7 @@ def run_reference(args) -> dict:
         "cpu_baseline": {
             "value": v,
             "unit": UNIT,
-            "cores": 1,
+            "cores": cores,
             "kind": "port",
             "sample": f"terminal + {args.cpu_periods} decision periods per step, extrapolated to a full solve",
         },
@@ -464,6 +698,15 @@ def main() -> None:
     ap.add_argument("--plain-samples", type=int, default=8)
     ap.add_argument("--cpu-periods", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-cores", type=int, default=0, help="host processes of the CPU baseline (0: all)")
+    ap.add_argument("--serve-requests", type=int, default=512)
+    ap.add_argument("--agents", type=int, default=10_000)
+    ap.add_argument("--serve-batch", type=int, default=32)
+    ap.add_argument("--serve-streams", type=int, default=2)
+    ap.add_argument("--plain-requests", type=int, default=32)
+    ap.add_argument("--no-extra", action="store_true", help="skip the serving / DC-EGM / two-state sections")
+    ap.add_argument("--dcegm-batch", type=int, default=32)
+    ap.add_argument("--hc-batch", type=int, default=8)
     args = ap.parse_args()
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out:

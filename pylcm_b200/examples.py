@@ -434,6 +434,7 @@ def serving_requests(n_requests: int = 4096, seed: int = 0, rate: float | None =
     from pylcm_b200.serving import Request
 
     rng = np.random.default_rng(seed)
+    arrivals = np.random.default_rng([seed, 1])  # arrival times do not change the requests
     models: dict = {}
     out = []
     t = 0.0
@@ -473,7 +474,7 @@ def serving_requests(n_requests: int = 4096, seed: int = 0, rate: float | None =
         rid = {s.name: s.rid for s in model.regime_specs}["working"]
         ic["regime_id"] = np.full(n_agents, rid, dtype=np.int64)
         if rate:
-            t += float(rng.exponential(1.0 / rate))
+            t += float(arrivals.exponential(1.0 / rate))
         out.append(Request(family=family, key=key, model=model, params=params, initial_conditions=ic,
                            seed=int(rng.integers(1 << 62)), arrival=t, rid=i,
                            return_V=bool(return_V_every) and i % return_V_every == 0))
