@@ -518,7 +518,7 @@ class SolvePlan:
         P = len(pa)
         agew = self._age_words(pa)
         g = {"index": {int(p): k for k, p in enumerate(pa)}, "tiles": tm["tiles"], "atab_tiles": tm["atab_tiles"],
-             "taste_words": [(rk.W_TASTE, s)] if s.taste_shocks else []}
+             "taste_words": [(rk.W_TASTE, s)] if s.taste_shocks else [], "rk": rk, "spec": s, "periods": pa}
         G = np.repeat(tm["bell"][None], P, axis=0)
         G[:, :, rk.W_V] = self._vptrs_many(s.name, pa)
         G[:, :, rk.W_POL] = self._vptrs_many(s.name, pa, pol=True)
@@ -608,6 +608,19 @@ class SolvePlan:
     def instance(self, idx: int):
         """(engine, Bellman records per (period, regime), row) of instance `idx`."""
         return self.eng, self.records, idx
+
+    def instance_plan(self, idx: int):
+        return self, idx
+
+    def sim_groups(self) -> dict:
+        """Per regime: (kernels, (periods, instances, words) Bellman records,
+        periods) of its grid-search groups -- the records the simulation
+        extends (built for every period the regime is active in)."""
+        out: dict[str, list] = {}
+        for key, g in self._grp.items():
+            if key[0] == "gs":
+                out.setdefault(g["spec"].name, []).append((g["rk"], g["rows"], g["periods"]))
+        return out
 
     def load_params(self, slot: int, params) -> None:
         """Make instance `slot` solve `params`: its parameter vectors (device,
@@ -896,7 +909,7 @@ class BatchPlan:
         self.plans = [pl for pl, _ in self._by_plan]
         self.dev = self.slots[0][0].dev
         self.launches, self.items, self.prefix = self._merge(
-            [(pl, pl._rec, pl.launches, lambda l, pl=pl: pl.eng.model.n_periods - 1 - l.period, sl)
+            [(pl, pl._rec, pl.launches, lambda l, pl=pl: pl.eng.model.n_periods - 1 - l.period, sl, "solve")
              for pl, sl in self._by_plan]
         )
         self._prepared = None
@@ -906,32 +919,44 @@ class BatchPlan:
         """Merge launch lists (restricted to the given slots of each plan) by
         (key, position within key, kernel)."""
         by_key: dict[int, list] = {}
-        for pl, rec, launches, key_of, sl in sources:
-            seq: dict[int, list] = {}
-            for l, h in zip(launches, rec.host):
-                seq.setdefault(key_of(l), []).append((pl, l, h, sl))
+        for pl, rec, launches, key_of, sl, tag in sources:
+            # a plan's launches grouped by key never change: cached on the plan
+            cache = pl.__dict__.setdefault("_seq_cache", {})
+            seq = cache.get(tag)
+            if seq is None:
+                seq = {}
+                for l, h in zip(launches, rec.host):
+                    legacy = l.kind == "fues" and l.module is not None
+                    gk = None if legacy else (l.kind, l.kernel, l.module.key if hasattr(l.module, "key") else id(l.module))
+                    seq.setdefault(key_of(l), []).append((pl, l, h, gk))
+                cache[tag] = seq
+            n_pl = pl.n
+            sub = None if list(sl) == list(range(n_pl)) else list(sl)
             for k, lst in seq.items():
-                by_key.setdefault(k, []).append(lst)
+                by_key.setdefault(k, []).append((lst, sl, sub))
         b = _Records()
         for k in sorted(by_key):
             lists = by_key[k]
-            depth = max(len(x) for x in lists)
+            depth = max(len(x) for x, _, _ in lists)
             for j in range(depth):
                 groups: dict[tuple, list] = {}
-                for lst in lists:
+                for lst, sl, sub in lists:
                     if j >= len(lst):
                         continue
-                    pl, l, h, sl = lst[j]
-                    if l.kind == "fues" and l.module is not None:
+                    pl, l, h, gk = lst[j]
+                    if gk is None:
                         b.append(Launch("fues", (pl,) + tuple(l.module[1:4]) + (tuple(sl),), l.kernel, 0, 0,
                                         l.n_items, 0, 0, 0, k))
                         continue
-                    gk = (l.kind, l.kernel, l.module.key if hasattr(l.module, "key") else id(l.module))
                     arr, tiles = h
-                    if len(sl) != arr.shape[0] or sl != list(range(arr.shape[0])):
-                        arr = arr[sl]
-                        tiles = [tiles[i] for i in sl]
-                    groups.setdefault(gk, []).append((l, arr, tiles))
+                    if sub is not None:
+                        arr = arr[sub]
+                        tiles = [tiles[i] for i in sub]
+                    g = groups.get(gk)
+                    if g is None:
+                        groups[gk] = [(l, arr, tiles)]
+                    else:
+                        g.append((l, arr, tiles))
                 for gk, members in groups.items():
                     l0 = members[0][0]
                     recs = members[0][1] if len(members) == 1 else np.concatenate([a for _, a, _ in members])
@@ -979,12 +1004,15 @@ class BatchPlan:
         sources = []
         for pl, sl in self._by_plan:
             pl.ensure_sim_records(upload=False)
-            rec = _Records()
-            rec.launches, rec.host, rec.shared = list(pl._rec.launches), list(pl._rec.host), list(pl._rec.shared)
-            rec.keep(lambda l: l.kind in ("expect", "atab"))
-            sources.append((pl, rec, rec.launches, lambda l: l.period, sl))
+            rec = pl.__dict__.get("_sim_input_rec")
+            if rec is None:
+                rec = _Records()
+                rec.launches, rec.host, rec.shared = list(pl._rec.launches), list(pl._rec.host), list(pl._rec.shared)
+                rec.keep(lambda l: l.kind in ("expect", "atab"))
+                pl._sim_input_rec = rec
+            sources.append((pl, rec, rec.launches, lambda l: l.period, sl, "sim_inputs"))
             if pl.sim_launches:
-                sources.append((pl, pl._sim_rec, pl.sim_launches, lambda l: l.period, sl))
+                sources.append((pl, pl._sim_rec, pl.sim_launches, lambda l: l.period, sl, "sim_only"))
         launches, items, prefix = self._merge(sources)
         self._inputs = (launches, items, prefix, self._prepare(launches, items, prefix))
 
@@ -998,6 +1026,9 @@ class BatchPlan:
     def instance(self, idx: int):
         pl, slot = self.slots[idx]
         return pl.eng, pl.records, slot
+
+    def instance_plan(self, idx: int):
+        return self.slots[idx]
 
     def result(self, i: int) -> tuple[dict, dict]:
         pl, slot = self.slots[i]

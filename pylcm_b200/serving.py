@@ -202,6 +202,7 @@ class Server:
         self.job_gpu_ms: list[float] = []  # device time of each job (its first kernel to its result copy)
         self.host_launch_s = 0.0  # host time building and issuing jobs
         self.host_finish_s = 0.0  # host time unpacking results
+        self.host_phase_s: dict[str, float] = {}  # host time of the phases of building and issuing jobs
 
     # ---------------------------------------------------------------- engines
     def engine(self, req: Request) -> SolveEngine:
@@ -279,23 +280,34 @@ class Server:
             t_start = torch.cuda.Event(enable_timing=True)
             # every host->device copy happens here, before the job's first kernel:
             # a pageable copy waits for the work queued before it on the stream
+            h = [time.perf_counter()]
             for (pool, slot, _), r in zip(slots, reqs):
                 pool.plan.load_params(slot, r.params)
+            h.append(time.perf_counter())
             plan = BatchPlan(slots=[(pool.plan, slot) for pool, slot, _ in slots])
+            h.append(time.perf_counter())
             sim = SimPlan(plan, instances=[(k, r.initial_conditions, r.seed) for k, r in enumerate(reqs)])
+            h.append(time.perf_counter())
             t_start.record(stream)
             plan.run(stream.cuda_stream)
+            h.append(time.perf_counter())
             sim.run(stream.cuda_stream)
-            rows, lengths = [], []
-            for b in sim.inst:
-                T = b["T"]
-                cols = [b["val"]]
-                cols += [b["S"][n][:T] for n in sorted(b["S"])]
-                cols += [b["A"][n] for n in sorted(b["A"])]
-                cols += [(b["R"][:T] == s.rid).to(torch.float64) for s in b["eng"].specs]
-                m = torch.nanmean(torch.stack(cols), dim=-1)
-                rows.append(m.reshape(-1))
-                lengths.append((len(cols), T))
+            h.append(time.perf_counter())
+            # per-period moments of every instance: a few ops per group of
+            # instances with the same horizon and subject count
+            rows, layout = [], []
+            off = 0
+            specs = sim.inst[0]["eng"].specs
+            for g in sim.groups:
+                T = g["T"]
+                cols = [g["val"]] + [g["S"][n][:, :T] for n in sorted(g["S"])] + [g["A"][n] for n in sorted(g["A"])]
+                m = [torch.nanmean(c, dim=-1) for c in cols]
+                m += [(g["R"][:, :T] == s.rid).to(torch.float64).mean(dim=-1) for s in specs]
+                block = torch.stack(m, dim=1)  # (group members, columns, T)
+                names = ["value"] + sorted(g["S"]) + sorted(g["A"]) + [f"share_{s.name}" for s in specs]
+                rows.append(block.reshape(-1))
+                layout.append((g["members"], names, T, off))
+                off += block.numel()
             dev_out = torch.cat(rows)
             host = torch.empty(tuple(dev_out.shape), dtype=torch.float64, pin_memory=True)
             host.copy_(dev_out, non_blocking=True)
@@ -311,24 +323,25 @@ class Server:
                     v_host[k] = vh
             event = torch.cuda.Event(enable_timing=True)
             event.record(stream)
+            h.append(time.perf_counter())
+        for k, name in enumerate(("params", "batch_plan", "sim_plan", "issue_solve", "issue_sim", "results")):
+            self.host_phase_s[name] = self.host_phase_s.get(name, 0.0) + h[k + 1] - h[k]
         self.jobs_run += 1
         self.batch_sizes.append(len(reqs))
-        job = _Job(family, reqs, stream, plan, sim, host, event, now, v_host, lengths, slots)
+        job = _Job(family, reqs, stream, plan, sim, host, event, now, v_host, layout, slots)
         job.t_start = t_start
         return job
 
     def _finish(self, job: _Job, now: float) -> list[Result]:
         arr = job.host.numpy()
+        moments: dict[int, dict] = {}
+        for members, names, T, off in job.lengths:
+            block = arr[off: off + len(members) * len(names) * T].reshape(len(members), len(names), T)
+            for k, i in enumerate(members):
+                moments[i] = {n: block[k, c].copy() for c, n in enumerate(names)}
         out = []
-        off = 0
         for k, r in enumerate(job.reqs):
-            b = job.sim.inst[k]
-            eng = b["eng"]
-            names = ["value"] + sorted(b["S"]) + sorted(b["A"]) + [f"share_{s.name}" for s in eng.specs]
-            ncol, T = job.lengths[k]
-            block = arr[off: off + ncol * T].reshape(ncol, T)
-            off += ncol * T
-            moments = {n: block[i].copy() for i, n in enumerate(names)}
+            eng = job.sim.inst[k]["eng"]
             V = None
             if k in job.v_host:
                 V = {}
@@ -337,7 +350,7 @@ class Server:
                     spec = next(s for s in eng.specs if s.name == name)
                     for p, sl in pl.slot[name].items():
                         V.setdefault(p, {})[name] = t[sl].numpy().reshape(spec.state_shape).copy()
-            out.append(Result(r.rid, job.family, moments, V, r.arrival, job.admitted, now, len(job.reqs)))
+            out.append(Result(r.rid, job.family, moments[k], V, r.arrival, job.admitted, now, len(job.reqs)))
         for pool, slot, sb in job.slots:
             pool.free.append(slot)
             self.in_use -= sb

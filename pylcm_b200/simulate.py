@@ -129,37 +129,67 @@ class SimPlan:
             eng, records, row = solve_plan.instance(idx)
             model = eng.model
             specs = eng.specs
-            T = model.n_periods
-            names = sorted({a.name for s in specs for a in s.states})
-            anames = sorted({a.name for s in specs for a in s.actions})
             rid0, states0 = _initial_arrays(model, ic)
-            N = rid0.shape[0]
             for s in specs:
                 for a in s.states:
                     if a.name not in states0 and (rid0 == s.rid).any():
                         raise InvalidParamsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
-            b = {
+            self.inst.append({
                 "idx": idx,
                 "eng": eng,
                 "records": records,
                 "row": row,
+                "T": model.n_periods,
+                "N": rid0.shape[0],
+                "seed": int(sd) & 0xFFFFFFFFFFFFFFFF,
+                "names": sorted({a.name for s in specs for a in s.states}),
+                "anames": sorted({a.name for s in specs for a in s.actions}),
+                "rid0": rid0,
+                "states0": states0,
+            })
+        # one (instances, periods, subjects) buffer per array for each group of
+        # instances with the same horizon and subject count; each instance
+        # works on its own slice (contiguous rows of N subjects)
+        by_shape: dict[tuple, list] = {}
+        for i, b in enumerate(self.inst):
+            by_shape.setdefault((b["T"], b["N"]), []).append(i)
+        self.groups = []
+        for (T, N), members in by_shape.items():
+            n_g = len(members)
+            names = sorted({n for i in members for n in self.inst[i]["names"]})
+            anames = sorted({n for i in members for n in self.inst[i]["anames"]})
+            g = {
                 "T": T,
                 "N": N,
-                "seed": int(sd) & 0xFFFFFFFFFFFFFFFF,
-                "S": {n: torch.full((T + 1, N), nan, dtype=torch.float64, device=dev) for n in names},
-                "R": torch.full((T + 1, N), -1, dtype=torch.int32, device=dev),
-                "val": torch.full((T, N), nan, dtype=torch.float64, device=dev),
-                "aidx": torch.zeros((T, N), dtype=torch.int32, device=dev),
-                "A": {n: torch.full((T, N), nan, dtype=torch.float64, device=dev) for n in anames},
+                "members": members,
+                "S": {n: torch.full((n_g, T + 1, N), nan, dtype=torch.float64, device=dev) for n in names},
+                "A": {n: torch.full((n_g, T, N), nan, dtype=torch.float64, device=dev) for n in anames},
+                "R": torch.full((n_g, T + 1, N), -1, dtype=torch.int32, device=dev),
+                "val": torch.full((n_g, T, N), nan, dtype=torch.float64, device=dev),
+                "aidx": torch.zeros((n_g, T, N), dtype=torch.int32, device=dev),
             }
-            for n, v in states0.items():
-                if n in b["S"]:
-                    b["S"][n][0] = torch.as_tensor(v, device=dev)
-            b["R"][0] = torch.as_tensor(rid0, dtype=torch.int32, device=dev)
-            self.inst.append(b)
+            # initial states and regimes: one host array and one copy per array
+            for n in names:
+                h = np.full((n_g, N), np.nan)
+                for k, i in enumerate(members):
+                    if n in self.inst[i]["states0"]:
+                        h[k] = self.inst[i]["states0"][n]
+                g["S"][n][:, 0, :].copy_(torch.from_numpy(h))
+            g["R"][:, 0, :].copy_(torch.from_numpy(np.stack([self.inst[i]["rid0"] for i in members]).astype(np.int32)))
+            for k, i in enumerate(members):
+                b = self.inst[i]
+                b["S"] = {n: g["S"][n][k] for n in b["names"]}
+                b["A"] = {n: g["A"][n][k] for n in b["anames"]}
+                b["R"] = g["R"][k]
+                b["val"] = g["val"][k]
+                b["aidx"] = g["aidx"][k]
+                del b["rid0"], b["states0"]
+            self.groups.append(g)
         self.T = max(b["T"] for b in self.inst)
-        # item records: the Bellman record of (period, regime, instance) + simulation words
-        per_period: dict[int, dict[tuple, list]] = {}
+        # item records: the Bellman record of (period, regime, instance) +
+        # simulation words, built per (instance, regime, kernel) for all its
+        # periods at once, then grouped per (period, kernel) with one sort
+        by_kernel: dict[tuple, list] = {}
         for b in self.inst:
             N, T = b["N"], b["T"]
             sbytes = N * 8  # one period of a subject array (float64)
@@ -169,21 +199,16 @@ class SimPlan:
             R0, V0, X0 = b["R"].data_ptr(), b["val"].data_ptr(), b["aidx"].data_ptr()
             seed_w = np.uint64(b["seed"]).astype(np.int64)
             tiles = math.ceil(N / 8)
+            pl, row = self.plan.instance_plan(b["idx"])
             for s in b["eng"].specs:
-                periods = [p for p in s.active_periods if p < T]
-                if not periods:
-                    continue
-                by_rk: dict[int, list] = {}
-                for p in periods:
-                    rk, base = b["records"][(p, s.name)]
-                    by_rk.setdefault(id(rk), [rk, [], []])
-                    by_rk[id(rk)][1].append(p)
-                    by_rk[id(rk)][2].append(base[b["row"]])
-                for rk, ps, bases in by_rk.values():
+                for rk, G, gp in pl.sim_groups().get(s.name, []):
+                    keep = gp < T
+                    if not keep.any():
+                        continue
                     b["eng"].module(rk)
-                    pa = np.asarray(ps, dtype=np.int64)
-                    rows = np.zeros((len(ps), rk.sim_words), dtype=np.int64)
-                    rows[:, : rk.n_words] = np.stack(bases)
+                    pa = gp[keep]
+                    rows = np.zeros((len(pa), rk.sim_words), dtype=np.int64)
+                    rows[:, : rk.n_words] = G[keep, row, :]
                     rows[:, rk.SW_N] = N
                     rows[:, rk.SW_RID_IN] = R0 + pa * ibytes
                     rows[:, rk.SW_RID_OUT] = R0 + (pa + 1) * ibytes
@@ -196,26 +221,36 @@ class SimPlan:
                         rows[:, rk.SW_SIN + k] = S0[a.name] + pa * sbytes
                     for k, name in enumerate(rk.sim_out_names):
                         rows[:, rk.SW_SOUT + k] = S0[name] + (pa + 1) * sbytes
-                    for j, p in enumerate(ps):
-                        g = per_period.setdefault(p, {}).setdefault((rk.sim_name(), rk.key), [rk, [], []])
-                        g[1].append(rows[j])
-                        g[2].append(tiles)
+                    g = by_kernel.setdefault((rk.sim_name(), rk.key), [rk, [], [], []])
+                    g[1].append(rows)
+                    g[2].append(pa)
+                    g[3].append(np.full(len(pa), tiles, dtype=np.int64))
+        pieces = []  # (period, kernel order, rk, rows, tiles)
+        for order, (rk, rows_l, per_l, til_l) in enumerate(by_kernel.values()):
+            rows = np.concatenate(rows_l)
+            per = np.concatenate(per_l)
+            til = np.concatenate(til_l)
+            o = np.argsort(per, kind="stable")
+            rows, per, til = rows[o], per[o], til[o]
+            cuts = np.flatnonzero(np.diff(per)) + 1
+            for r_, p_, t_ in zip(np.split(rows, cuts), np.split(per, cuts), np.split(til, cuts)):
+                pieces.append((int(p_[0]), order, rk, r_, t_))
+        pieces.sort(key=lambda x: (x[0], x[1]))
         recs = []
         prefs = []
         self.launches = []
         off = 0
         poff = 0
-        for period in sorted(per_period):
-            for rk, rows, tiles in per_period[period].values():
-                npre = len(tiles) + 1
-                pre = np.zeros(npre + (-npre) % 4, dtype=np.int32)
-                np.cumsum(tiles, out=pre[1:npre])
-                prefs.append(pre)
-                recs.append(np.stack(rows))
-                self.launches.append((period, rk, off, poff, len(rows), int(pre[npre - 1])))
-                off += rk.sim_words * len(rows)
-                poff += pre.size
-        self.items = torch.as_tensor(np.concatenate([r.reshape(-1) for r in recs]), dtype=torch.int64, device=dev)
+        for period, _, rk, rows, tiles in pieces:
+            npre = len(tiles) + 1
+            pre = np.zeros(npre + (-npre) % 4, dtype=np.int32)
+            np.cumsum(tiles, out=pre[1:npre])
+            prefs.append(pre)
+            recs.append(rows.reshape(-1))
+            self.launches.append((period, rk, off, poff, len(rows), int(pre[npre - 1])))
+            off += rows.size
+            poff += pre.size
+        self.items = torch.as_tensor(np.concatenate(recs), dtype=torch.int64, device=dev)
         self.prefix = torch.as_tensor(np.concatenate(prefs), dtype=torch.int32, device=dev)
 
     def run(self, stream: int | None = None) -> None:

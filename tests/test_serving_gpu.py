@@ -2,6 +2,7 @@
 different grid sizes and horizons) and the continuous-batching server."""
 
 import dataclasses
+import gc
 
 import numpy as np
 import pytest
@@ -154,6 +155,7 @@ def test_footprint_estimate_covers_the_allocations():
 
     for r in E.serving_requests(4, seed=8, n_agents=2000, sizes=(200,), horizons=(10,), n_consumption=100):
         eng = _engine(r.model, "fp32")
+        gc.collect()  # plans of the previous iteration hold reference cycles
         torch.cuda.synchronize()
         before = torch.cuda.memory_allocated()
         bp = BatchPlan([(eng, r.params)])
