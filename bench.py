@@ -711,7 +711,16 @@ def main() -> None:
     ap.add_argument("--no-extra", action="store_true", help="skip the serving / DC-EGM / two-state sections")
     ap.add_argument("--dcegm-batch", type=int, default=32)
     ap.add_argument("--hc-batch", type=int, default=8)
+    ap.add_argument("--only", choices=["serving", "dcegm", "hc"], default=None,
+                    help="run one extra section alone on GPU 0 and print its JSON (for profiling)")
     args = ap.parse_args()
+    if args.only:
+        import torch
+
+        torch.cuda.set_device(0)
+        fn = {"serving": run_serving, "dcegm": run_dcegm, "hc": run_hc}[args.only]
+        print(json.dumps({args.only: fn(args, 0)}))
+        return
     out = run_reference(args) if args.impl == "reference" else run_ours(args)
     if out:
         print(json.dumps(out))

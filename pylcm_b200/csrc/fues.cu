@@ -319,7 +319,16 @@ constexpr int kFuesItemWords = 12;
 __host__ __device__ constexpr size_t fues_smem_bytes(int n) {
   int np2 = 1;
   while (np2 < n) np2 <<= 1;
-  return (size_t)5 * n * sizeof(double) + (size_t)np2 * sizeof(int);
+  return (size_t)5 * n * sizeof(double) + (size_t)np2 * (sizeof(unsigned long long) + sizeof(int));
+}
+
+// Monotone 64-bit image of a grid value for the sort: NaN ranks with +inf and
+// -0 with +0, as the (double) comparison of the lexsort key treats them.
+__device__ __forceinline__ unsigned long long grid_key(double g) {
+  if (isnan_(g)) g = __longlong_as_double(0x7ff0000000000000LL);
+  if (g == 0.0) g = 0.0;
+  const unsigned long long b = (unsigned long long)__double_as_longlong(g);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
 }
 
 struct FuesRowIO {
@@ -397,6 +406,14 @@ struct FuesItems {
   }
 };
 
+// x[t] <- x[sidx[t]] for t < n, through the shared-memory buffer `tmp`
+__device__ __forceinline__ void permute_sorted(double* x, double* tmp, const int* sidx, int n) {
+  for (int t = threadIdx.x; t < n; t += kBlock) tmp[t] = x[sidx[t]];
+  __syncthreads();
+  for (int t = threadIdx.x; t < n; t += kBlock) x[t] = tmp[t];
+  __syncthreads();
+}
+
 template <class Rows>
 __global__ void __launch_bounds__(kBlock) fues_smem_kernel(Rows rows) {
   extern __shared__ __align__(16) unsigned char fues_smem[];
@@ -417,38 +434,62 @@ __global__ void __launch_bounds__(kBlock) fues_smem_kernel(Rows rows) {
     double* v = p + n;
     double* s = v + n;
     double* sec = s + n;
-    int* sidx = reinterpret_cast<int*>(sec + n);
+    unsigned long long* skey = reinterpret_cast<unsigned long long*>(sec + n);
+    int* sidx = reinterpret_cast<int*>(skey + np2);
     __syncthreads();  // the previous row is done with shared memory
-    // ---- 1. bitonic sort of indices by the lexsort key
-    for (int t = threadIdx.x; t < np2; t += kBlock) sidx[t] = t;
+    // ---- 1. stage the row in shared memory (input order), sort indices by
+    // the lexsort key read from there, then put each array in sorted order
+    // through registers
+    for (int t = threadIdx.x; t < n; t += kBlock) {
+      const double gt = G[t], pt = P[t];
+      g[t] = gt;
+      p[t] = pt;
+      v[t] = V[t];
+      s[t] = io.S ? io.S[t] : gt - pt;
+    }
     __syncthreads();
+    // (grid key, index) pairs: a compare-exchange reads positions t and
+    // t ^ stride; only equal grid keys consult value, policy and index
+    for (int t = threadIdx.x; t < np2; t += kBlock) {
+      sidx[t] = t;
+      skey[t] = t < n ? grid_key(g[t]) : ~0ULL;  // padding sorts last
+    }
+    __syncthreads();
+    const int half = np2 >> 1;
     for (int size = 2; size <= np2; size <<= 1) {
       for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int t = threadIdx.x; t < np2; t += kBlock) {
-          const int partner = t ^ stride;
-          if (partner > t) {
+        const int ls = __ffs(stride) - 1;  // stride = 2^ls
+#pragma unroll 4
+        for (int j = threadIdx.x; j < half; j += kBlock) {
+          // the j-th compare-exchange pair (t, t + stride) of this stage:
+          // the positions whose bit ls is clear, in order
+          const int t = ((j >> ls) << (ls + 1)) | (j & (stride - 1));
+          const int partner = t + stride;
+          {
             const bool ascending = (t & size) == 0;
-            const Key a = load_key(G, V, P, sidx[t], n);
-            const Key b = load_key(G, V, P, sidx[partner], n);
-            const bool swap = ascending ? key_less(b, a) : key_less(a, b);
-            if (swap) {
-              const int tmp = sidx[t];
-              sidx[t] = sidx[partner];
-              sidx[partner] = tmp;
+            const unsigned long long ka = skey[t], kb = skey[partner];
+            const int ia = sidx[t], ib = sidx[partner];
+            bool a_first;  // does (ka, ia) come before (kb, ib)?
+            if (ka != kb) {
+              a_first = ka < kb;
+            } else {
+              a_first = !key_less(load_key(g, v, p, ib, n), load_key(g, v, p, ia, n));
+            }
+            if (ascending != a_first) {
+              skey[t] = kb;
+              skey[partner] = ka;
+              sidx[t] = ib;
+              sidx[partner] = ia;
             }
           }
         }
         __syncthreads();
       }
     }
-    for (int t = threadIdx.x; t < n; t += kBlock) {
-      const int i = sidx[t];
-      g[t] = G[i];
-      p[t] = P[i];
-      v[t] = V[i];
-      s[t] = io.S ? io.S[i] : G[i] - P[i];
-    }
-    __syncthreads();
+    permute_sorted(g, sec, sidx, n);  // `sec` is free until the scan tables
+    permute_sorted(p, sec, sidx, n);
+    permute_sorted(v, sec, sidx, n);
+    permute_sorted(s, sec, sidx, n);
     // ---- 2. coincident groups: keep the maximisers, one per savings source
     for (int t = threadIdx.x; t < n; t += kBlock) {
       const double gt = g[t];
