@@ -167,10 +167,9 @@ def run_ours(args) -> dict:
         dist.barrier()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([t_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
+    from pylcm_b200.distributed import max_over_ranks
+
+    t_ms = max_over_ranks(t_ms, device="cuda")  # the slowest rank's time
     value = world * args.batch * args.steps / (t_ms / 1e3)
 
     # ---- end to end through the public batch API (host params -> host V)
