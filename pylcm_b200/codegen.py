@@ -396,6 +396,7 @@ class RegimeKernels:
         order = sorted(targets, key=lambda s: (bool(s.states), s.rid))
         self.targets = [_target_plan(tr, t) for t in order] if not self.spec.terminal else []
         self._layout()
+        self._affine = self._affine_laws()
         tag_src = repr(
             (self.spec.name, [t.spec.name for t in self.targets], precision, dataclasses.astuple(cfg))
         )
@@ -458,10 +459,43 @@ class RegimeKernels:
         return f"lcm_expect_{self.tag}_{t.spec.name}"
 
     # ..................................................................
+    def _affine_laws(self) -> dict:
+        """Continuous next-state laws that are affine in the one continuous
+        action they read: {(target, state position): (law at action 0,
+        d law / d action, action var)}.  The single-precision search then
+        computes the grid coordinate as K + M * action with K and M fixed per
+        (state, discrete action) -- one fused multiply-add per action.  Its
+        candidates are re-evaluated in double precision, so the search's
+        rounding does not reach the published values beyond that search's
+        tolerance; the double-precision form keeps the law as written."""
+        out: dict = {}
+        if self.precision != "fp32":
+            return out
+        dnames = {a.name for a in self.spec.actions if a.kind != "continuous"}
+        for ti, t in enumerate(self.targets):
+            if t.scalar:
+                continue
+            for pos in t.cont_pos:
+                x = ir.const(t.laws[t.spec.states[pos].name].expr)
+                if not isinstance(x, ir.Expr):
+                    continue
+                acts = {nm for k, nm in x.deps() if k == "action" and nm not in dnames}
+                if len(acts) != 1:
+                    continue
+                cv = ir.var("action", next(iter(acts)), "f")
+                g = ir.const(ir.diff(x, cv))
+                if not isinstance(g, ir.Expr) or any(n is cv for n in ir.topo_order([g])):
+                    continue
+                x0 = ir.substitute(x, cv, 0.0)
+                out[(ti, pos)] = (x0, g, cv)
+        return out
+
     def _roots(self):
         """Root IR nodes the per-(state, action) code needs."""
         tr = self.tr
         roots = [tr.F, tr.U]
+        for x0, g, cv in getattr(self, "_affine", {}).values():
+            roots += [x0, g, cv]
         if tr.beta is not None:
             roots.append(tr.beta)
         if tr.regime_id is not None and self.targets:
@@ -646,7 +680,7 @@ class RegimeKernels:
             out += e.lines
             e.lines = []
             sel = [(ti, t) for ti, t in enumerate(self.targets) if tsel < 0 or ti == tsel]
-            pnames, dn, xn = {}, {}, {}
+            pnames, dn, xn, affine_names = {}, {}, {}, {}
             rid_name = e.emit(self.tr.regime_id) if (det and tsel < 0) else None
             for ti, t in sel:
                 if not det:
@@ -656,7 +690,12 @@ class RegimeKernels:
                 for pos in t.det_pos:
                     dn[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
                 for pos in t.cont_pos:
-                    xn[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
+                    if not sim and (ti, pos) in self._affine:
+                        x0, g, cv = self._affine[(ti, pos)]
+                        affine_names[(ti, pos)] = (e.emit(x0), e.emit(g), e.emit(cv))
+                        xn[(ti, pos)] = None
+                    else:
+                        xn[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
             out += e.lines
             e.lines = []
             if det:
@@ -706,7 +745,12 @@ class RegimeKernels:
                         ax = t.spec.states[pos]
                         x = xn[(ti, pos)]
                         kind = ax.grid.kind
-                        if kind == "lin":
+                        if kind == "lin" and not sim and (ti, pos) in affine_names:
+                            # (x0 + g c - a) b as K + M c: K, M are loop-invariant
+                            x0n, gn, cvn = affine_names[(ti, pos)]
+                            cc = (f"((({T})({x0n}) - C.a{ti}_{ci}) * C.b{ti}_{ci} + "
+                                  f"(({T})({gn}) * C.b{ti}_{ci}) * ({T})({cvn}))")
+                        elif kind == "lin":
                             cc = f"lcm_coord_lin<{T}>(({T})({x}), C.a{ti}_{ci}, C.b{ti}_{ci})"
                         elif kind == "log":
                             cc = f"lcm_coord_log<{T}>(({T})({x}), C.a{ti}_{ci}, C.b{ti}_{ci})"

@@ -633,13 +633,20 @@ def diff(expr: Any, wrt: Expr) -> Expr:
         if e.op == "bin":
             o, a, b = e.args
             da, db = d(a), d(b)
+            za, zb = _is_zero(da), _is_zero(db)  # a symbolic zero derivative drops its term
             if o == "+":
-                return da + db
+                return db if za else (da if zb else da + db)
             if o == "-":
-                return da - db
+                return -db if za else (da if zb else da - db)
             if o == "*":
+                if za:
+                    return a * db
+                if zb:
+                    return da * b
                 return da * b + a * db
             if o == "/":
+                if zb:
+                    return da / b
                 return (da * b - a * db) / (b * b)
             if o == "pow":
                 # a**b: b * a**(b-1) * da + log(a) * a**b * db
@@ -682,6 +689,10 @@ def diff(expr: Any, wrt: Expr) -> Expr:
     return const(d(const(expr)))
 
 
+def _is_zero(x: Any) -> bool:
+    return isinstance(x, Expr) and x.op == "const" and x.args[0] == 0.0
+
+
 def _leaves(e: Expr) -> set:
     out = getattr(e, "_leaf_cache", None)
     if out is None:
@@ -697,3 +708,21 @@ class _IdSet:
 
     def __contains__(self, x: Any) -> bool:
         return id(x) in self.ids
+
+
+def substitute(expr: Any, wrt: Expr, value: float) -> Expr:
+    """`expr` with the variable `wrt` replaced by the constant `value` (nodes
+    rebuilt bottom-up; nodes without `wrt` below them are kept)."""
+    e0 = const(expr)
+    rep = const(value)
+    new: dict[int, Any] = {}
+    for n in topo_order([e0]):
+        if n is wrt:
+            new[id(n)] = rep
+            continue
+        args = tuple(new.get(id(a), a) if isinstance(a, Expr) else a for a in n.args)
+        if all(x is y for x, y in zip(args, n.args)):
+            new[id(n)] = n
+        else:
+            new[id(n)] = Expr(n.op, args, n.dtype)
+    return new[id(e0)]
