@@ -217,7 +217,8 @@ class Server:
                 cfgs = dict(self.configs.get(req.family, {}))
                 for s in req.model.regime_specs:
                     if s.name not in cfgs:
-                        cfgs[s.name] = LaunchConfig(block=256, lanes=1, chunk=512, sb=1)
+                        # jobs of tens of requests: 2 lanes x 2 states per thread
+                        cfgs[s.name] = LaunchConfig(block=256, lanes=2, chunk=512, sb=2)
                 self._family_cfg[req.family] = cfgs
             eng = SolveEngine(req.model, self.precision, configs=cfgs, device=self.device)
             self._engines[req.key] = eng
