@@ -131,17 +131,18 @@ FUES_SMEM_MAX_N = 4096  # longest candidate row of the item-form FUES launch
 
 
 def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> LaunchConfig:
-    """Launch shape of kernel (a).  Preferred: 2 lanes per state and 4 states
-    per thread (each thread's states share the shared-memory action loads and
-    give the scheduler independent work -- the fastest shape measured on the
-    B200 for batched solves); fewer states per thread, then more lanes per
-    state, only while the batch's states would not fill the GPU (SM count x
-    resident threads)."""
+    """Launch shape of kernel (a).  Preferred: 2 lanes per state and, in the
+    single-precision search, 4 states per thread (each thread's states share
+    the shared-memory action loads and give the scheduler independent work --
+    the fastest shapes measured on the B200; in double precision more states
+    per thread cost more registers than they save); fewer states per thread,
+    then more lanes per state, only while the batch's states would not fill
+    the GPU (SM count x resident threads)."""
     n_a = spec.n_actions
     total = max(1, spec.n_states * n_items)
     want = SM_COUNT * RESIDENT_THREADS_PER_SM
     lanes = 2 if n_a >= 64 else 1
-    sb = 4
+    sb = 4 if precision == "fp32" else 1
     while sb > 1 and total * lanes < want * sb:
         sb //= 2
     while lanes < 32 and total * lanes < want * sb and n_a >= 8 * lanes * 2:
