@@ -364,10 +364,10 @@ def run_ours(args) -> dict:
             "unit": "GB/s",
             "frac": achieved_gbs / pk_["hbm_gbs"],
             # DRAM bytes of one kernel (a) launch from the ncu capture of the
-            # same kernel at batch 16 (1.148672 MB), scaled by the instances
-            # per launch; the capture's bytes match that launch's algorithmic bytes
-            "traffic": 1.148672e6 * args.batch / 16,
-            "traffic_source": "ncu dram__bytes_read+write of lcm_bellman_working at batch 16, scaled x batch/16",
+            # same launch at batch 256 (17.90336 MB read, 256 B written), scaled
+            # by the instances per launch for other batch sizes
+            "traffic": (17.90336e6 + 256.0) * args.batch / 256,
+            "traffic_source": "ncu dram__bytes_read+write of lcm_bellman_working at batch 256 (x batch/256)",
             "peak_source": pk_["source"],
             "avg_launch_ms": avg_k_ms,
             "algorithmic_bytes_per_launch": bytes_per_launch,
