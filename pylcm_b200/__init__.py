@@ -12,6 +12,7 @@ from pylcm_b200.ages import AgeGrid
 from pylcm_b200.exceptions import (
     AdmissionError,
     GridInitializationError,
+    InvalidInitialConditionsError,
     InvalidParamsError,
     InvalidValueFunctionError,
     KernelError,
@@ -54,6 +55,7 @@ __all__ = [
     "FUESEnvelope",
     "GridInitializationError",
     "GridSearch",
+    "InvalidInitialConditionsError",
     "InvalidParamsError",
     "InvalidValueFunctionError",
     "IrregSpacedGrid",

@@ -9,12 +9,12 @@ class GridInitializationError(PyLCMError):
     """A grid or process was declared with invalid arguments."""
 
 
-class RegimeInitializationError(PyLCMError):
-    """A regime was declared with invalid arguments."""
-
-
 class ModelInitializationError(PyLCMError):
     """A model could not be built from its regimes."""
+
+
+class RegimeInitializationError(ModelInitializationError):
+    """A regime was declared with invalid arguments."""
 
 
 class InvalidParamsError(PyLCMError):
@@ -23,6 +23,10 @@ class InvalidParamsError(PyLCMError):
 
 class InvalidValueFunctionError(PyLCMError):
     """A solved value function contains NaN."""
+
+
+class InvalidInitialConditionsError(PyLCMError):
+    """The initial conditions passed to simulate do not match the model."""
 
 
 class TracingError(PyLCMError):
@@ -37,5 +41,6 @@ class KernelError(PyLCMError):
         self.status = status
 
 
-class AdmissionError(PyLCMError):
-    """A serving request does not fit the configured HBM budget."""
+class AdmissionError(PyLCMError, MemoryError):
+    """A serving request does not fit the configured HBM budget (no
+    counterpart in the reference, which has no serving layer)."""

@@ -41,6 +41,7 @@ from typing import Any, Hashable, Mapping, Sequence
 import numpy as np
 
 from pylcm_b200.engine import LaunchConfig, SolveEngine
+from pylcm_b200.exceptions import AdmissionError
 
 
 @dataclasses.dataclass
@@ -369,7 +370,7 @@ class Server:
         for r in reqs:
             fp = self.footprint(r)
             if fp > self.budget:
-                raise MemoryError(f"request {r.rid}: footprint {fp} B exceeds the HBM budget {self.budget} B")
+                raise AdmissionError(f"request {r.rid}: footprint {fp} B exceeds the HBM budget {self.budget} B")
         waiting: dict[Hashable, collections.deque] = collections.OrderedDict()
         free = list(self.streams)
         inflight: list[_Job] = []
@@ -417,7 +418,7 @@ class Server:
                 elif i < n:
                     time.sleep(max(0.0, min(reqs[i].arrival - (time.perf_counter() - t0), 1e-3)))
                 elif any(waiting.values()):
-                    raise MemoryError("a waiting request cannot be admitted with no job in flight")
+                    raise AdmissionError("a waiting request cannot be admitted with no job in flight")
         torch.cuda.synchronize(self.dev)
         return [results[r.rid] for r in sorted(requests, key=lambda r: r.rid)]
 

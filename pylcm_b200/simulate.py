@@ -20,7 +20,7 @@ from typing import Any, Mapping
 
 import numpy as np
 
-from pylcm_b200.exceptions import InvalidParamsError
+from pylcm_b200.exceptions import InvalidInitialConditionsError, InvalidParamsError
 from pylcm_b200.grids import DiscreteGrid
 
 
@@ -84,18 +84,18 @@ def _initial_arrays(model, initial_conditions: Mapping) -> tuple[np.ndarray, dic
     ic = dict(initial_conditions)
     rid = ic.pop("regime_id", ic.pop("regime", None))
     if rid is None:
-        raise InvalidParamsError("initial_conditions needs 'regime_id'")
+        raise InvalidInitialConditionsError("initial_conditions needs 'regime_id'")
     rid = np.asarray(rid).astype(np.int64)
     n = rid.shape[0]
     if "age" in ic:
         ages = np.asarray(ic.pop("age"), dtype=np.float64)
         if not np.all(ages == model.ages.values[0]):
-            raise InvalidParamsError("all subjects must start at the first age of the age grid")
+            raise InvalidInitialConditionsError("all subjects must start at the first age of the age grid")
     states = {}
     for k, v in ic.items():
         a = np.asarray(v, dtype=np.float64)
         if a.shape != (n,):
-            raise InvalidParamsError(f"initial condition {k!r} must have shape ({n},)")
+            raise InvalidInitialConditionsError(f"initial condition {k!r} must have shape ({n},)")
         states[k] = a
     return rid, states
 
@@ -133,7 +133,7 @@ class SimPlan:
             for s in specs:
                 for a in s.states:
                     if a.name not in states0 and (rid0 == s.rid).any():
-                        raise InvalidParamsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
+                        raise InvalidInitialConditionsError(f"initial_conditions lacks state {a.name!r} of regime {s.name!r}")
             self.inst.append({
                 "idx": idx,
                 "eng": eng,

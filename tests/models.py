@@ -221,3 +221,73 @@ from pylcm_b200.examples import (  # noqa: E402
     stochastic_model,
     stochastic_params,
 )
+
+
+# --------------------------------------------------------------------------
+# taste-shock toy model: one decision period (log consumption, binary work
+# choice, EV1 taste shocks on it) and a terminal bequest regime; restates the
+# reference's `tests/test_models/taste_shocks_toy.py` in this package's API
+# --------------------------------------------------------------------------
+TOY_KAPPA = 0.3
+TOY_WAGE = 2.0
+
+
+@categorical(ordered=False)
+class ToyRegimeId:
+    alive: int
+    done: int
+
+
+@categorical(ordered=True)
+class WorkChoice:
+    off: int
+    on: int
+
+
+def _toy_utility_alive(consumption, work, kappa):
+    return jnp.log(consumption) - kappa * work
+
+
+def _toy_utility_done(wealth):
+    return jnp.log(wealth + 1.0)
+
+
+def _toy_next_wealth(wealth, consumption, work, wage):
+    return wealth - consumption + wage * work
+
+
+def _toy_budget(consumption, wealth):
+    return consumption <= wealth
+
+
+def _toy_next_regime(age):
+    return ToyRegimeId.done
+
+
+def taste_toy_model(taste=True):
+    from pylcm_b200 import ExtremeValueTasteShocks
+
+    alive = Regime(
+        transition=_toy_next_regime,
+        states={"wealth": LinSpacedGrid(start=1.0, stop=10.0, n_points=6)},
+        state_transitions={"wealth": _toy_next_wealth},
+        actions={"work": DiscreteGrid(WorkChoice), "consumption": LinSpacedGrid(start=0.5, stop=5.0, n_points=8)},
+        constraints={"budget_constraint": _toy_budget},
+        functions={"utility": _toy_utility_alive},
+        taste_shocks=ExtremeValueTasteShocks() if taste else None,
+        active=lambda age: age < 41,
+    )
+    done = Regime(
+        transition=None,
+        states={"wealth": LinSpacedGrid(start=0.0, stop=12.0, n_points=25)},
+        functions={"utility": _toy_utility_done},
+    )
+    return Model(regimes={"alive": alive, "done": done}, ages=AgeGrid(start=40, stop=41, step="Y"),
+                 regime_id_class=ToyRegimeId)
+
+
+def taste_toy_params(scale, discount_factor=0.95):
+    return {
+        "discount_factor": discount_factor,
+        "alive": {"utility": {"kappa": TOY_KAPPA}, "next_wealth": {"wage": TOY_WAGE}, "taste_shocks": {"scale": scale}},
+    }
