@@ -291,3 +291,139 @@ def taste_toy_params(scale, discount_factor=0.95):
         "discount_factor": discount_factor,
         "alive": {"utility": {"kappa": TOY_KAPPA}, "next_wealth": {"wage": TOY_WAGE}, "taste_shocks": {"scale": scale}},
     }
+
+
+# --------------------------------------------------------------------------
+# pen-and-paper toy model with discrete actions only (deterministic): restates
+# the reference's `tests/test_solution_on_toy_model_deterministic.py` model
+# --------------------------------------------------------------------------
+@categorical(ordered=False)
+class ToyConsumption:
+    low: int
+    high: int
+
+
+@categorical(ordered=False)
+class ToyLabor:
+    do_not_work: int
+    work: int
+
+
+@categorical(ordered=False)
+class ToyDetRegimeId:
+    alive: int
+    dead: int
+
+
+def _det_utility(consumption, labor_supply, wealth, health):
+    return jnp.log(1.0 + health * consumption) - 0.5 * labor_supply
+
+
+def _det_next_wealth(wealth, consumption, labor_supply):
+    return wealth - consumption + labor_supply
+
+
+def _det_next_regime(age, final_age_alive):
+    return jnp.where(age >= final_age_alive, ToyDetRegimeId.dead, ToyDetRegimeId.alive)
+
+
+def _det_borrowing(consumption, wealth):
+    return consumption <= wealth
+
+
+def toy_deterministic_model(n_wealth=100, n_periods=3):
+    alive = Regime(
+        actions={"consumption": DiscreteGrid(ToyConsumption), "labor_supply": DiscreteGrid(ToyLabor)},
+        states={"wealth": LinSpacedGrid(start=0, stop=2, n_points=n_wealth)},
+        state_transitions={"wealth": _det_next_wealth},
+        functions={"utility": _det_utility},
+        constraints={"borrowing_constraint": _det_borrowing},
+        transition=_det_next_regime,
+        active=lambda age, last=n_periods - 1: age < last,
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0},
+                  active=lambda age, last=n_periods - 1: age >= last)
+    return Model(regimes={"alive": alive, "dead": dead}, ages=AgeGrid(start=0, stop=n_periods - 1, step="Y"),
+                 regime_id_class=ToyDetRegimeId)
+
+
+def toy_deterministic_params(discount_factor, n_periods=3):
+    return {"discount_factor": discount_factor,
+            "alive": {"utility": {"health": 1}, "next_regime": {"final_age_alive": n_periods - 2}}}
+
+
+def toy_deterministic_analytic(wealth, discount_factor):
+    """Pen-and-paper value functions of the first and second period: in the
+    last decision period consume one unit when wealth allows and do not work;
+    in the first, compare working for next period's unit (beta log 2 - 1/2)
+    with not working."""
+    v1 = np.log(1.0 + np.minimum(1.0, np.floor(wealth)))
+    gain = max(0.0, discount_factor * np.log(2.0) - 0.5)
+    v0 = np.array([gain, gain + np.log(2.0), (1.0 + discount_factor) * np.log(2.0)])[np.floor(wealth).astype(int)]
+    return v0, v1
+
+
+@categorical(ordered=False)
+class ToyHealth:
+    bad: int
+    good: int
+
+
+def _sto_next_health(health, probs_array):
+    return probs_array[health]
+
+
+def _sto_utility(consumption, labor_supply, wealth, health):
+    return jnp.log(1.0 + health * consumption) - 0.5 * labor_supply
+
+
+def toy_stochastic_model(n_wealth=100, n_periods=3):
+    """The pen-and-paper toy model with a Markov health state (reference
+    `tests/test_solution_on_toy_model_stochastic.py`)."""
+    alive = Regime(
+        actions={"consumption": DiscreteGrid(ToyConsumption), "labor_supply": DiscreteGrid(ToyLabor)},
+        states={"wealth": LinSpacedGrid(start=0, stop=2, n_points=n_wealth), "health": DiscreteGrid(ToyHealth)},
+        state_transitions={"wealth": _det_next_wealth, "health": MarkovTransition(_sto_next_health)},
+        functions={"utility": _sto_utility},
+        constraints={"borrowing_constraint": _det_borrowing},
+        transition=_det_next_regime,
+        active=lambda age, last=n_periods - 1: age < last,
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0},
+                  active=lambda age, last=n_periods - 1: age >= last)
+    return Model(regimes={"alive": alive, "dead": dead}, ages=AgeGrid(start=0, stop=n_periods - 1, step="Y"),
+                 regime_id_class=ToyDetRegimeId)
+
+
+def toy_stochastic_params(discount_factor, probs_array, n_periods=3):
+    return {"discount_factor": discount_factor,
+            "alive": {"next_health": {"probs_array": np.asarray(probs_array, dtype=np.float64)},
+                      "next_regime": {"final_age_alive": n_periods - 2}}}
+
+
+def toy_stochastic_analytic(wealth, health, discount_factor, P):
+    """Pen-and-paper values and policies of the stochastic toy model at
+    (wealth, health) points: in bad health consumption is worthless today,
+    so the only value is next period's unit in good health; in good health
+    the deterministic solution applies with the discount factor scaled by
+    the probability of staying healthy."""
+    P = np.asarray(P, dtype=np.float64)
+    wealth = np.asarray(wealth, dtype=np.float64)
+    health = np.asarray(health).astype(int)
+    beta_g = discount_factor * P[1, 1]
+    gain_b = discount_factor * P[0, 1] * np.log(2.0)
+    v0_bad = np.where(wealth < 1, max(0.0, gain_b - 0.5), gain_b)
+    l0_bad = np.where(wealth < 1, int(np.argmax((0.0, gain_b - 0.5))), 0)
+    v0_good, _ = toy_deterministic_analytic(wealth, beta_g)
+    gain_g = beta_g * np.log(2.0) - 0.5
+    idx = np.floor(wealth).astype(int)
+    c0_good = np.array([0, 1, 1])[idx]
+    l0_good = np.array([int(np.argmax((0.0, gain_g))), int(np.argmax((0.0, gain_g))), 0])[idx]
+    v0 = np.where(health == 1, v0_good, v0_bad)
+    c0 = np.where(health == 1, c0_good, 0)
+    l0 = np.where(health == 1, l0_good, l0_bad)
+    return v0, c0, l0
+
+
+def toy_stochastic_v1(wealth, health):
+    return np.log(1.0 + np.minimum(1.0, np.floor(np.asarray(wealth, dtype=np.float64)))) * np.asarray(health)
