@@ -73,6 +73,10 @@ def main() -> None:
             if src.exists():
                 arr = np.genfromtxt(src, delimiter=",")
                 np.save(OUT / f"analytical_{kind}__{what}.npy", arr)
+    # the independent `dcegm` package's solution of the IJRS retirement model
+    # with taste shocks (the reference's cross-check fixture)
+    df = pd.read_csv(data / "dcegm_reference" / "ijrs_taste_shocks_reference.csv")
+    np.savez(OUT / "ijrs_taste_shocks_reference.npz", **{c: df[c].to_numpy(np.float64) for c in df.columns})
 
 
 if __name__ == "__main__":

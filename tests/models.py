@@ -427,3 +427,124 @@ def toy_stochastic_analytic(wealth, health, discount_factor, P):
 
 def toy_stochastic_v1(wealth, health):
     return np.log(1.0 + np.minimum(1.0, np.floor(np.asarray(wealth, dtype=np.float64)))) * np.asarray(health)
+
+
+# --------------------------------------------------------------------------
+# brute-force twin of the IJRS retirement model with EV1 taste shocks, whose
+# solution the independent `dcegm` package provides (reference cross-check
+# fixture `tests/data/dcegm_reference/ijrs_taste_shocks_reference.csv`,
+# model documented with the reference's `tests/test_models/dcegm_paper_twin.py`)
+# --------------------------------------------------------------------------
+IJRS_MIN_AGE = 20
+IJRS_N_PERIODS = 10
+IJRS_LAST_ALIVE_AGE = IJRS_MIN_AGE + IJRS_N_PERIODS - 2
+
+
+@categorical(ordered=False)
+class IjrsRegimeId:
+    working_life: int
+    retirement: int
+    done_from_working: int
+    done_retired: int
+
+
+@categorical(ordered=True)
+class IjrsWork:
+    work: int
+    retire: int
+
+
+def ijrs_wealth_points():
+    """Geometric below 0.5, 0.05-steps to 5, 0.25-steps to 50: the fixture's
+    wealth points (1, 2, 5, 10, 20, 35) are grid nodes."""
+    low = tuple(0.001 * (0.5 / 0.001) ** (i / 120) for i in range(120))
+    mid = tuple(0.5 + 0.05 * i for i in range(90))
+    top = tuple(5.0 + 0.25 * i for i in range(181))
+    return low + mid + top
+
+
+def _ijrs_crra(c, rho):
+    return (c ** (1.0 - rho) - 1.0) / (1.0 - rho)
+
+
+def _ijrs_is_working(work_choice):
+    return work_choice == IjrsWork.work
+
+
+def _ijrs_u_work(consumption, is_working, rho, delta):
+    return _ijrs_crra(consumption, rho) - jnp.where(is_working, delta, 0.0)
+
+
+def _ijrs_u_ret(consumption, rho):
+    return _ijrs_crra(consumption, rho)
+
+
+def _ijrs_u_done_working(wealth, rho, delta, taste_scale):
+    # consume everything; the final period's work/retire taste shock smooths
+    # the (income-less) choice
+    return _ijrs_crra(wealth, rho) + taste_scale * jnp.log(1.0 + jnp.exp(-delta / taste_scale))
+
+
+def _ijrs_u_done_retired(wealth, rho):
+    return _ijrs_crra(wealth, rho)
+
+
+def _ijrs_labor_income(is_working, age, constant, exp_coeff, exp_squared):
+    # earned this period, paid next period at next period's age
+    a = age + 1.0
+    return jnp.where(is_working, jnp.exp(constant + exp_coeff * a + exp_squared * a ** 2), 0.0)
+
+
+def _ijrs_next_wealth(wealth, consumption, labor_income, interest_rate, floor):
+    return jnp.maximum((1.0 + interest_rate) * (wealth - consumption) + labor_income, floor)
+
+
+def _ijrs_borrowing(consumption, wealth):
+    return consumption <= wealth
+
+
+def _ijrs_nr_working(work_choice, age):
+    last = age >= IJRS_LAST_ALIVE_AGE
+    retire = work_choice == IjrsWork.retire
+    return jnp.where(last, jnp.where(retire, IjrsRegimeId.done_retired, IjrsRegimeId.done_from_working),
+                     jnp.where(retire, IjrsRegimeId.retirement, IjrsRegimeId.working_life))
+
+
+def _ijrs_nr_retired(age):
+    return jnp.where(age >= IJRS_LAST_ALIVE_AGE, IjrsRegimeId.done_retired, IjrsRegimeId.retirement)
+
+
+def ijrs_brute_model():
+    from pylcm_b200 import ExtremeValueTasteShocks, IrregSpacedGrid, LogSpacedGrid
+
+    wealth = IrregSpacedGrid(points=ijrs_wealth_points())
+    cons = LogSpacedGrid(start=0.001, stop=50.0, n_points=400)
+    alive = lambda age: age <= IJRS_LAST_ALIVE_AGE  # noqa: E731
+    working = Regime(
+        transition=_ijrs_nr_working, states={"wealth": wealth},
+        actions={"work_choice": DiscreteGrid(IjrsWork), "consumption": cons},
+        taste_shocks=ExtremeValueTasteShocks(), active=alive,
+        state_transitions={"wealth": _ijrs_next_wealth}, constraints={"borrowing_constraint": _ijrs_borrowing},
+        functions={"utility": _ijrs_u_work, "is_working": _ijrs_is_working, "labor_income": _ijrs_labor_income},
+    )
+    retired = Regime(
+        transition=_ijrs_nr_retired, states={"wealth": wealth}, actions={"consumption": cons}, active=alive,
+        state_transitions={"wealth": _ijrs_next_wealth}, constraints={"borrowing_constraint": _ijrs_borrowing},
+        functions={"utility": _ijrs_u_ret},
+    )
+    done_w = Regime(transition=None, states={"wealth": wealth}, functions={"utility": _ijrs_u_done_working})
+    done_r = Regime(transition=None, states={"wealth": wealth}, functions={"utility": _ijrs_u_done_retired})
+    return Model(regimes={"working_life": working, "retirement": retired, "done_from_working": done_w,
+                          "done_retired": done_r},
+                 ages=AgeGrid(start=IJRS_MIN_AGE, stop=IJRS_MIN_AGE + IJRS_N_PERIODS - 1, step="Y"),
+                 regime_id_class=IjrsRegimeId)
+
+
+def ijrs_params(taste_scale=0.2):
+    return {
+        "discount_factor": 0.95, "interest_rate": 0.05, "rho": 1.95, "delta": 0.35, "constant": 0.75,
+        "exp_coeff": 0.04, "exp_squared": -0.0002, "floor": 0.001,
+        "done_from_working": {"utility": {"taste_scale": taste_scale}},
+        "working_life": {"taste_shocks": {"scale": taste_scale}},
+        "retirement": {"next_wealth": {"labor_income": 0.0}},
+    }
