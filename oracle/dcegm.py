@@ -38,7 +38,7 @@ from oracle.fues import refine
 from oracle.grid_search import _process_tables, bellman_step
 from pylcm_b200 import ir
 from pylcm_b200.egm import A_VAR, MU, is_egm, trace_egm_regime
-from pylcm_b200.spec import ParamResolver
+from pylcm_b200.spec import ParamResolver, trace_regime
 
 EPS = np.finfo(np.float64).eps
 
@@ -96,8 +96,99 @@ def _eval(expr, env, tr):
     return ir.evaluate(expr, env, {k: v for k, v in tr.param_values.items()})
 
 
-def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R):
-    """Rows of V_d on the state grid and carry rows for one EGM regime."""
+def value_carry_marginal(spec, euler, V_arr, specs, res, period, age):
+    """Marginal-value rows of a regime whose value array a DC-EGM regime
+    reads (``egm/terminal.py:76-330``), in the value array's layout.
+
+    Terminal regime: the derivative of its utility with respect to the Euler
+    state at the grid nodes, zero where the value is -inf.  Grid-search
+    regime: the value array's slope along the Euler axis -- ``np.gradient``'s
+    second-order stencil where both neighbours are feasible (finite), the
+    one-sided difference toward the single feasible neighbour, zero without
+    one and at infeasible states (``terminal.py:272-314``).
+    """
+    V_arr = np.asarray(V_arr, dtype=np.float64).reshape(spec.state_shape)
+    names = [a.name for a in spec.states]
+    ax = names.index(euler)
+    grid = spec.state(euler).grid.to_numpy()
+    if spec.terminal:
+        tr = trace_regime(spec, specs, res, ())
+        dU = ir.diff(tr.U, ir.var("state", euler, "f"))
+        idx = np.indices(spec.state_shape)
+        env = {("period", "period"): period, ("age", "age"): age}
+        for k, a in enumerate(spec.states):
+            env[("state", a.name)] = grid[idx[k]] if a.name == euler else idx[k]
+        with np.errstate(all="ignore"):
+            mu = np.broadcast_to(np.asarray(_eval(dU, env, tr), dtype=np.float64), spec.state_shape)
+        return np.where(np.isneginf(V_arr), 0.0, mu)
+    v = np.moveaxis(V_arr, ax, -1)
+    feas = np.isfinite(v)
+    safe = np.where(feas, v, 0.0)
+    fwd = np.diff(safe, axis=-1) / np.diff(grid)
+    pad = np.zeros(v.shape[:-1] + (1,))
+    right = np.concatenate([fwd, pad], axis=-1)
+    left = np.concatenate([pad, fwd], axis=-1)
+    fpad = np.zeros(v.shape[:-1] + (1,), dtype=bool)
+    has_r = np.concatenate([feas[..., 1:], fpad], axis=-1)
+    has_l = np.concatenate([fpad, feas[..., :-1]], axis=-1)
+    interior = np.gradient(safe, grid, axis=-1) if len(grid) > 1 else np.zeros_like(safe)
+    m = np.where(has_l & has_r, interior, np.where(has_r, right, np.where(has_l, left, 0.0)))
+    m = np.where(feas, m, 0.0)
+    return np.moveaxis(m, -1, ax)
+
+
+def _value_child_read(tg, wlists, Rn, dR, V_arr, M_arr):
+    """Continuation read of a carried value array: the expectation over the
+    target's discrete states folded into the value and marginal rows (sum of
+    w * row over the nodes with a non-zero weight), then one read at R'(A)
+    on the target's Euler grid (``egm/continuation.py:551-674, 1460-1520``)."""
+    spec = tg.spec
+    names = [a.name for a in spec.states]
+    ax = names.index(tg.value_euler)
+    grid = spec.state(tg.value_euler).grid.to_numpy()
+    V = np.moveaxis(np.asarray(V_arr, dtype=np.float64).reshape(spec.state_shape), ax, -1)
+    M = np.moveaxis(np.asarray(M_arr, dtype=np.float64).reshape(spec.state_shape), ax, -1)
+    fv = np.zeros(len(grid))
+    fm = np.zeros(len(grid))
+    for combo in itertools.product(*[range(len(w)) for w in wlists]):
+        w = 1.0
+        for wl, j in zip(wlists, combo):
+            w *= wl[j]
+        if w == 0.0:
+            continue
+        with np.errstate(all="ignore"):
+            fv = fv + w * V[combo]
+            fm = fm + w * M[combo]
+    with np.errstate(all="ignore"):
+        val = read_row(Rn, grid, fv, fm)
+        mar = read_row(Rn, grid, fm)
+        mar = np.where(np.isneginf(val), 0.0, mar * dR)
+    return val, mar
+
+
+def _weight_lists(tg, dstates, procs, env, tr):
+    """Weights of each discrete state of a target: the process row, the
+    Markov row or the one-hot deterministic law."""
+    wlists = []
+    for ax in dstates:
+        law = tg.disc_laws[ax.name]
+        if law.kind == "process":
+            P = procs[law.source_process][1]
+            wlists.append(P[env[("state", law.source_process)], :])
+        elif law.kind == "markov":
+            wlists.append(np.array([float(_eval(x, env, tr)) for x in law.expr.items]))
+        else:
+            k = int(_eval(law.expr, env, tr))
+            w = np.zeros(ax.size)
+            w[min(max(k, 0), ax.size - 1)] = 1.0
+            wlists.append(w)
+    return wlists
+
+
+def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R, value_mu=None):
+    """Rows of V_d on the state grid and carry rows for one EGM regime.
+    `value_mu` holds the marginal-value rows of the targets read as value
+    arrays (terminal / grid-search regimes)."""
     tr = er.tracer
     procs = _process_tables(er.spec, res)
     beta = float(_eval(er.beta, {}, tr))
@@ -129,23 +220,17 @@ def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R):
                 continue
             # joint distribution over the target's discrete states
             dstates = [a for a in tg.spec.states if a.kind != "continuous"]
-            wlists = []
-            for ax in dstates:
-                law = tg.disc_laws[ax.name]
-                if law.kind == "process":
-                    P = procs[law.source_process][1]
-                    wlists.append(P[env[("state", law.source_process)], :])
-                elif law.kind == "markov":
-                    wlists.append(np.array([float(_eval(x, env, tr)) for x in law.expr.items]))
-                else:
-                    k = int(_eval(law.expr, env, tr))
-                    w = np.zeros(ax.size)
-                    w[min(max(k, 0), ax.size - 1)] = 1.0
-                    wlists.append(w)
+            wlists = _weight_lists(tg, dstates, procs, env, tr)
             envA = dict(env)
             envA[("egm", "A")] = A
             Rn = np.broadcast_to(np.asarray(_eval(tg.next_R, envA, tr), dtype=np.float64), A.shape)
             dR = np.broadcast_to(np.asarray(_eval(tg.dR_dA, envA, tr), dtype=np.float64), A.shape)
+            if tg.is_value:
+                val, mar = _value_child_read(tg, wlists, Rn, dR, V_next[tg.spec.name], value_mu[tg.spec.name])
+                with np.errstate(all="ignore"):
+                    EV = EV + p * val
+                    EMU = EMU + p * mar
+                continue
             num_v = np.zeros_like(A)
             num_m = np.zeros_like(A)
             den = 0.0
@@ -287,7 +372,13 @@ def solve(model, params):
             if is_egm(s) and not s.terminal:
                 er = trace_egm_regime(s, specs, res, targets)
                 grid_R = s.state(er.E).grid.to_numpy()
-                Vs, cr, _ = egm_step(er, specs, res, period, age, carry.get(period + 1, {}), V.get(period + 1, {}), grid_R)
+                vmu = {
+                    t.spec.name: value_carry_marginal(t.spec, t.value_euler, V[period + 1][t.spec.name], specs, res,
+                                                      period + 1, float(model.ages.values[period + 1]))
+                    for t in er.targets if t.is_value and not t.unreachable
+                }
+                Vs, cr, _ = egm_step(er, specs, res, period, age, carry.get(period + 1, {}), V.get(period + 1, {}),
+                                     grid_R, vmu)
                 V[period][s.name] = Vs
                 carry[period][s.name] = cr
             else:

@@ -318,23 +318,24 @@ __device__ __forceinline__ int lcm_categorical(const double* p, double u) {
 // slopes dp, limited by Fritsch & Carlson (1980); it falls back to linear
 // where a slope or endpoint is not finite.  The slope row itself is read
 // linearly.  L is the number of valid (non-NaN) leading entries.
-__device__ __forceinline__ void lcm_row_read(const double* __restrict__ xp, const double* __restrict__ fp,
-                                             const double* __restrict__ dp, int L, double xq,
-                                             double& val, double& slope_val) {
-  if (L <= 0) { val = slope_val = LCM_NAN; return; }
-  if (L == 1) { val = fp[0]; slope_val = dp ? dp[0] : LCM_NAN; return; }
-  int lo = 0, hi = L;  // first index with xp > xq
+// Index of the last node at or below xq (-1 below the first node): a binary
+// search for the first node above xq.
+__device__ __forceinline__ int lcm_row_bracket(const double* __restrict__ xp, int L, double xq) {
+  int lo = 0, hi = L;
   while (lo < hi) { const int mid = (lo + hi) >> 1; if (xp[mid] > xq) hi = mid; else lo = mid + 1; }
-  const int idx = lo - 1;
-  if (idx >= L - 1) { val = fp[L - 1]; slope_val = dp ? dp[L - 1] : LCM_NAN; return; }
-  const int b = idx < 0 ? 0 : idx;
-  const double x0 = xp[b], x1 = xp[b + 1], f0 = fp[b], f1 = fp[b + 1];
+  return lo - 1;
+}
+
+// The read on one bracket [x0, x1] (node values f0, f1, node slopes d0, d1
+// when has_dp) of a row whose bracket index is idx (-1: below the first node;
+// the bracket is then the first one) and idx <= L - 2.
+__device__ __forceinline__ void lcm_bracket_read(double x0, double x1, double f0, double f1, double d0, double d1,
+                                                 bool has_dp, int idx, double xq, double& val, double& slope_val) {
   const double h = x1 - x0;
   const double t = h > 0.0 ? (xq - x0) / h : 0.0;
   double v = h > 0.0 ? f0 + t * (f1 - f0) : f1;
   double s = LCM_NAN;
-  if (dp) {
-    const double d0 = dp[b], d1 = dp[b + 1];
+  if (has_dp) {
     s = h > 0.0 ? d0 + t * (d1 - d0) : d1;
     if (lcm_isfinite(f0) && lcm_isfinite(f1) && lcm_isfinite(d0) && lcm_isfinite(d1) && h > 0.0 && idx >= 0) {
       const double delta = (f1 - f0) / h;
@@ -356,4 +357,16 @@ __device__ __forceinline__ void lcm_row_read(const double* __restrict__ xp, cons
   if (idx >= 0 && (neg0 || neg1) && !((xq == x0) && lcm_isfinite(f0)) && !((xq == x1) && lcm_isfinite(f1))) v = -LCM_INF;
   val = v;
   slope_val = s;
+}
+
+__device__ __forceinline__ void lcm_row_read(const double* __restrict__ xp, const double* __restrict__ fp,
+                                             const double* __restrict__ dp, int L, double xq,
+                                             double& val, double& slope_val) {
+  if (L <= 0) { val = slope_val = LCM_NAN; return; }
+  if (L == 1) { val = fp[0]; slope_val = dp ? dp[0] : LCM_NAN; return; }
+  const int idx = lcm_row_bracket(xp, L, xq);
+  if (idx >= L - 1) { val = fp[L - 1]; slope_val = dp ? dp[L - 1] : LCM_NAN; return; }
+  const int b = idx < 0 ? 0 : idx;
+  lcm_bracket_read(xp[b], xp[b + 1], fp[b], fp[b + 1], dp ? dp[b] : 0.0, dp ? dp[b + 1] : 0.0, dp != nullptr, idx, xq,
+                   val, slope_val);
 }

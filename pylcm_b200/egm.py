@@ -61,6 +61,37 @@ class EgmTarget:
     # no law for one of the target's states: the source cannot reach the
     # target; a non-zero probability toward it poisons the continuation (NaN)
     unreachable: bool = False
+    # a target solved without the endogenous grid (terminal or grid search):
+    # its carry is its value array on its own state grid with the marginal
+    # value of its Euler state (``value_euler``) beside it
+    value_euler: str | None = None
+
+    @property
+    def is_value(self) -> bool:
+        return self.value_euler is not None
+
+
+def value_child_euler(tg: RegimeSpec) -> str:
+    """The Euler state of a target that publishes its value array as a carry
+    (``regime_building/processing.py:1270-1386``): the first declared state,
+    which must be continuous; further continuous (passive) states are not
+    carried here; a terminal target has no actions and no process states
+    (its marginal value is the gradient of its utility)."""
+    first = tg.state(next(iter(tg.user.states)))
+    cont = [a for a in tg.states if a.kind == "continuous"]
+    if first.kind != "continuous":
+        raise ModelInitializationError(
+            f"DCEGM target {tg.name!r}: its first state must be its continuous (Euler) state"
+        )
+    if len(cont) > 1:
+        raise ModelInitializationError(
+            f"DCEGM target {tg.name!r}: passive continuous states in a carried value are not supported"
+        )
+    if tg.terminal and (tg.actions or any(a.kind == "process" for a in tg.states)):
+        raise ModelInitializationError(
+            f"terminal DCEGM target {tg.name!r} must have no actions and no process states"
+        )
+    return first.name
 
 
 @dataclasses.dataclass
@@ -170,8 +201,7 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
         if not tg.states:
             tgs.append(EgmTarget(tg, probs[tg.rid], {}, None, None))
             continue
-        if not is_egm(tg):
-            raise ModelInitializationError(f"DCEGM target {tname!r} must be a DCEGM regime or stateless")
+        euler = tg.user.liquid.state if is_egm(tg) else value_child_euler(tg)
         laws = {}
         nextR = None
         src_states = {a.name for a in spec.states}
@@ -192,7 +222,7 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
                 continue
             law = spec.functions[fname]
             val = t.trace(fname)
-            if ax.name == tg.user.liquid.state:
+            if ax.name == euler:
                 nextR = ir.const(val)
             elif isinstance(law, MarkovTransition):
                 laws[ax.name] = NextState("markov", val)
@@ -201,7 +231,8 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
         if unreachable or nextR is None:
             tgs.append(EgmTarget(tg, probs[tg.rid], {}, None, None, unreachable=True))
             continue
-        tgs.append(EgmTarget(tg, probs[tg.rid], laws, nextR, ir.diff(nextR, A_VAR)))
+        tgs.append(EgmTarget(tg, probs[tg.rid], laws, nextR, ir.diff(nextR, A_VAR),
+                             value_euler=None if is_egm(tg) else euler))
     sav = np.asarray(solver.savings_grid.to_numpy(), dtype=np.float64)
     nc = int(solver.n_constrained_points)
     ratio = (1.0 / CONSTRAINED_OFFSET_FRACTION) ** (1.0 / max(nc - 1, 1))

@@ -72,6 +72,8 @@ class EgmKernels:
                 self.W_T.append({})
             elif t.next_R is None:
                 self.W_T.append({"scalar": take()})
+            elif t.is_value:
+                self.W_T.append({"tv": take(), "tm": take(), "tg": take(), "tn": take()})
             else:
                 self.W_T.append({"rg": take(), "rv": take(), "mu": take(), "nk": take(), "npad": take(), "taste": take()})
         self.n_words = w
@@ -91,6 +93,78 @@ class EgmKernels:
             lines.append(f"const int dc_{a.name} = rrem % {a.size}; rrem /= {a.size};")
             prov[id(ir.var(kind, a.name, "i"))] = f"dc_{a.name}"
         return prov
+
+    def _weights(self, body: list, ti: int, t, names: dict) -> list:
+        """Emit the weight vector of every discrete state of target `t`
+        (process row, Markov row or one-hot deterministic law)."""
+        wl_names = []
+        for ax in [a for a in t.spec.states if a.kind != "continuous"]:
+            law = t.disc_laws[ax.name]
+            arr = f"w_{ti}_{ax.name}"
+            wl_names.append((ax, arr))
+            body.append(f"    double {arr}[{ax.size}];")
+            if law.kind == "process":
+                off, shape = self.param_off[proc_P_name(law.source_process)]
+                body.append(
+                    f"    for (int q = 0; q < {ax.size}; ++q) {arr}[q] = PV[{off} + dc_{law.source_process} * {shape[1]} + q];"
+                )
+            elif law.kind == "markov":
+                for q, v in enumerate(names[("m", ax.name)]):
+                    body.append(f"    {arr}[{q}] = (double)({v});")
+            else:
+                de = names[("d", ax.name)]
+                body.append(f"    {{ const int kk = min(max((int)({de}), 0), {ax.size - 1});")
+                body.append(f"      for (int q = 0; q < {ax.size}; ++q) {arr}[q] = (q == kk) ? 1.0 : 0.0; }}")
+        return wl_names
+
+    def _value_read(self, body: list, ti: int, t, names: dict, w: dict) -> None:
+        """Continuation read of a target that carries its value array (a
+        terminal or grid-search regime) on its own state grid, the Euler
+        state's marginal value beside it (``egm/terminal.py:76-330``).  All
+        rows share the grid, so the expectation over the target's discrete
+        states folds into the rows before one read, as the reference folds a
+        value-only child's node axes (``egm/continuation.py:551-674``: the
+        weighted sums w * row over the nodes, a zero weight contributing
+        nothing; an integer-indexed deterministic state is the one-hot case);
+        the value read is the limited cubic Hermite with the marginal row as
+        node slopes, the marginal read linear, pinned to zero where the value
+        read is -inf, times dR'/dA (``continuation.py:1460-1520``)."""
+        tg = t.spec
+        body.append(f"    const double Rn = (double)({names['R']}); const double dR = (double)({names['dR']});")
+        wl_names = self._weights(body, ti, t, names)
+        body.append(f"    const double* TV = lcm_wp<const double>(it, {w['tv']});")
+        body.append(f"    const double* TM = lcm_wp<const double>(it, {w['tm']});")
+        body.append(f"    const double* TG = lcm_wp<const double>(it, {w['tg']});")
+        body.append(f"    const int tn = lcm_wi(it, {w['tn']});")
+        body.append("    const int ix = tn > 1 ? lcm_row_bracket(TG, tn, Rn) : 0;")
+        body.append("    const int b0 = tn > 1 ? (ix < 0 ? 0 : (ix > tn - 2 ? tn - 2 : ix)) : 0;")
+        body.append("    const int b1 = tn > 1 ? b0 + 1 : 0;")
+        body.append("    double f0 = 0.0, f1 = 0.0, g0 = 0.0, g1 = 0.0;")
+        J = 1
+        for ax, _ in wl_names:
+            J *= ax.size
+        body.append(f"    for (int jc = 0; jc < {J}; ++jc) {{")
+        body.append("      int jr = jc; double wt = 1.0;")
+        for ax, arr in reversed(wl_names):
+            body.append(f"      const int jn_{ax.name} = jr % {ax.size}; jr /= {ax.size}; wt *= {arr}[jn_{ax.name}];")
+        body.append("      (void)jr;")
+        body.append("      if (wt == 0.0) continue;")
+        # flat index into the target's value array (states in declaration
+        # order, the Euler axis tn long)
+        i0 = i1 = "(i64)0"
+        for ax in tg.states:
+            if ax.name == t.value_euler:
+                i0, i1 = f"({i0}) * tn + b0", f"({i1}) * tn + b1"
+            else:
+                i0, i1 = f"({i0}) * {ax.size} + jn_{ax.name}", f"({i1}) * {ax.size} + jn_{ax.name}"
+        body.append(f"      const i64 i0 = {i0}, i1 = {i1};")
+        body.append("      f0 += wt * TV[i0]; f1 += wt * TV[i1]; g0 += wt * TM[i0]; g1 += wt * TM[i1];")
+        body.append("    }")
+        body.append("    double vr, mr;")
+        body.append("    if (tn <= 1) { vr = f0; mr = g0; }")
+        body.append("    else if (ix >= tn - 1) { vr = f1; mr = g1; }")
+        body.append("    else lcm_bracket_read(TG[b0], TG[b1], f0, f1, g0, g1, true, ix, Rn, vr, mr);")
+        body.append("    EV += p * vr; EMU += p * (vr == -LCM_INF ? 0.0 : mr * dR);")
 
     def _source(self) -> str:
         er = self.er
@@ -152,32 +226,15 @@ class EgmKernels:
                 body.append("    EV = LCM_NAN;  // probability toward a target this regime cannot reach")
             elif t.next_R is None:
                 body.append(f"    EV += lcm_zs(p, *lcm_wp<const double>(it, {w['scalar']}));")
+            elif t.is_value:
+                self._value_read(body, ti, t, tnames[ti], w)
             else:
                 tg = t.spec
                 Re = tnames[ti]["R"]
                 dRe = tnames[ti]["dR"]
                 body.append(f"    const double Rn = (double)({Re}); const double dR = (double)({dRe});")
-                # weights per target discrete axis
                 dstates = [a for a in tg.states if a.kind != "continuous"]
-                wl_names = []
-                for ax in dstates:
-                    law = t.disc_laws[ax.name]
-                    arr = f"w_{ti}_{ax.name}"
-                    wl_names.append((ax, arr))
-                    body.append(f"    double {arr}[{ax.size}];")
-                    if law.kind == "process":
-                        off, shape = self.param_off[proc_P_name(law.source_process)]
-                        body.append(
-                            f"    for (int q = 0; q < {ax.size}; ++q) {arr}[q] = PV[{off} + dc_{law.source_process} * {shape[1]} + q];"
-                        )
-                    elif law.kind == "markov":
-                        vs = tnames[ti][("m", ax.name)]
-                        for q, v in enumerate(vs):
-                            body.append(f"    {arr}[{q}] = (double)({v});")
-                    else:
-                        de = tnames[ti][("d", ax.name)]
-                        body.append(f"    {{ const int kk = min(max((int)({de}), 0), {ax.size - 1});")
-                        body.append(f"      for (int q = 0; q < {ax.size}; ++q) {arr}[q] = (q == kk) ? 1.0 : 0.0; }}")
+                wl_names = self._weights(body, ti, t, tnames[ti])
                 nd_t = 1
                 for a in tg.actions:
                     if a.kind != "continuous":
@@ -366,6 +423,103 @@ class EgmKernels:
             ap(f"    best = lcm_logsum<double, {nd}>(vd, lam);")
         ap(f"    lcm_wp<double>(it, {self.W_V})[(i64)srow * ng + gi] = best;")
         ap(f"    lcm_wp<int>(it, {self.W_POL})[(i64)srow * ng + gi] = barg;")
+        ap("  }")
+        ap("}")
+        return "\n".join(L)
+
+
+class ValueCarryKernel:
+    """The marginal-value rows of a target that carries its value array into
+    a DC-EGM parent (``egm/terminal.py:76-330``), one thread per state of the
+    target, written in the value array's layout:
+
+    - terminal target: the derivative of its utility with respect to the
+      Euler state at the grid node (the reference's ``jax.grad``; here
+      :func:`pylcm_b200.ir.diff`), zero where the value is -inf;
+    - grid-search target: the value array's slope along the Euler grid --
+      NumPy's second-order non-uniform stencil where both neighbours are
+      feasible, the one-sided difference toward the one feasible neighbour,
+      zero without one or at an infeasible state (``terminal.py:272-314``).
+    """
+
+    def __init__(self, spec, euler: str, U=None, param_off=None) -> None:
+        self.spec = spec
+        self.euler = euler
+        self.terminal = U is not None
+        self.param_off = param_off or {}
+        self.U = U
+        self.W_P, self.W_PERIOD, self.W_AGE, self.W_V, self.W_M, self.W_G, self.W_NG = range(7)
+        self.n_words = 7
+        self.src = self._source()
+        self.key = "lcm_vmu_" + hashlib.sha1(self.src.encode()).hexdigest()[:24]
+
+    def name(self) -> str:
+        return f"lcm_vmu_{self.spec.name}"
+
+    def _source(self) -> str:
+        spec = self.spec
+        L: list[str] = [device_header(), _EXTRA_DEVICE]
+        ap = L.append
+        ap(f'extern "C" __global__ void __launch_bounds__(256) {self.name()}(const i64* __restrict__ items, '
+           "const int* __restrict__ tile_prefix, int n_items, int n_tiles) {")
+        ap("  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {")
+        ap("    const int item = lcm_find_item(tile_prefix, n_items, tile);")
+        ap(f"    const i64* __restrict__ it = items + (i64)item * {self.n_words};")
+        ap(f"    const double* __restrict__ PV = lcm_wp<const double>(it, {self.W_P});")
+        ap(f"    const int period = lcm_wi(it, {self.W_PERIOD}); const double age = lcm_wd(it, {self.W_AGE});")
+        ap("    (void)period; (void)age; (void)PV;")
+        ap(f"    const double* __restrict__ V = lcm_wp<const double>(it, {self.W_V});")
+        ap(f"    double* __restrict__ M = lcm_wp<double>(it, {self.W_M});")
+        ap(f"    const double* __restrict__ G = lcm_wp<const double>(it, {self.W_G});")
+        ap(f"    const int ng = lcm_wi(it, {self.W_NG});")
+        ap("    const i64 e = (i64)(tile - tile_prefix[item]) * 256 + (int)threadIdx.x;")
+        n_other = 1
+        for a in spec.states:
+            if a.name != self.euler:
+                n_other *= a.size
+        ap(f"    if (e >= (i64){n_other} * ng) continue;")
+        # decode the flat state index (declaration order, last fastest)
+        ap("    i64 rem = e; i64 se = 1; (void)se;")
+        after = True
+        for a in reversed(spec.states):
+            size = "ng" if a.name == self.euler else str(a.size)
+            ap(f"    const int c_{a.name} = (int)(rem % {size}); rem /= {size};")
+            if a.name == self.euler:
+                after = False
+            elif after:
+                ap(f"    se *= {a.size};")
+        ap(f"    const int gi = c_{self.euler};")
+        ap("    const double v = V[e];")
+        if self.terminal:
+            prov = {id(ir.var("period", "period", "i")): "period", id(ir.var("age", "age", "f")): "age"}
+            for a in spec.states:
+                if a.name == self.euler:
+                    ap(f"    const double sv_{a.name} = G[gi];")
+                    prov[id(ir.var("state", a.name, "f"))] = f"sv_{a.name}"
+                elif a.kind == "continuous":
+                    raise TracingError("passive continuous states are not carried")
+                else:
+                    prov[id(ir.var("state", a.name, "i"))] = f"c_{a.name}"
+            em = Emitter("double", self.param_off, prov, "u")
+            de = em.emit(ir.diff(self.U, ir.var("state", self.euler, "f")))
+            for ln in em.lines:
+                ap("    " + ln)
+            ap(f"    M[e] = (v == -LCM_INF) ? 0.0 : (double)({de});")
+        else:
+            ap("    const bool fe = lcm_isfinite(v);")
+            ap("    const bool hl = gi > 0 && lcm_isfinite(V[e - se]);")
+            ap("    const bool hr = gi < ng - 1 && lcm_isfinite(V[e + se]);")
+            ap("    double m = 0.0;")
+            ap("    if (fe && hl && hr) {")
+            ap("      const double hs = G[gi] - G[gi - 1], hd = G[gi + 1] - G[gi];")
+            ap("      const double a = -hd / (hs * (hd + hs)), b = (hd - hs) / (hs * hd), c = hs / (hd * (hd + hs));")
+            ap("      m = a * V[e - se] + b * v + c * V[e + se];")
+            ap("    } else if (fe && hr) {")
+            ap("      m = (V[e + se] - v) / (G[gi + 1] - G[gi]);")
+            ap("    } else if (fe && hl) {")
+            ap("      m = (v - V[e - se]) / (G[gi] - G[gi - 1]);")
+            ap("    }")
+            ap("    M[e] = m;")
         ap("  }")
         ap("}")
         return "\n".join(L)

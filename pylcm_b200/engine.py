@@ -206,6 +206,22 @@ class SolveEngine:
             self._kernels[key] = ek
         return ek
 
+    def value_carry_kernel(self, spec: RegimeSpec, euler: str, params):
+        """The marginal-value kernel of a terminal or grid-search regime that
+        a DC-EGM regime reads as a carried value array."""
+        from pylcm_b200.egm_codegen import ValueCarryKernel
+
+        key = ("vmu", spec.name)
+        vk = self._kernels.get(key)
+        if vk is None:
+            if spec.terminal:
+                rk = self.kernels(spec, (), params)
+                vk = ValueCarryKernel(spec, euler, rk.tr.U, rk.param_off)
+            else:
+                vk = ValueCarryKernel(spec, euler)
+            self._kernels[key] = vk
+        return vk
+
     def module(self, rk: RegimeKernels):
         from pylcm_b200.runtime import get_context
 
@@ -333,6 +349,20 @@ class SolvePlan:
             self.egm[s.name]["ws"] = torch.empty(max(wb, 8), dtype=torch.uint8, device=dev)
             self.egm[s.name]["wb"] = wb
 
+        # marginal-value rows of the terminal / grid-search regimes DC-EGM
+        # regimes read as carried value arrays (two-slot ring by period parity)
+        self.vmu: dict[str, Any] = {}
+        self._vck: dict[str, Any] = {}
+        self._vmu_need: set = set()
+        for period, s, targets, ek in egm_steps:
+            for t in ek.er.targets:
+                if not t.is_value or t.unreachable:
+                    continue
+                self._vmu_need.add((t.spec.name, period + 1))
+                if t.spec.name not in self.vmu:
+                    self.vmu[t.spec.name] = torch.zeros((2, n, t.spec.n_states), dtype=torch.float64, device=dev)
+                    self._vck[t.spec.name] = eng.value_carry_kernel(t.spec, t.value_euler, params_list[0])
+
         # EV buffers per (source, target set, target)
         for period, s, targets, rk in step_list:
             if not isinstance(rk, RegimeKernels):
@@ -377,6 +407,8 @@ class SolvePlan:
                 self._egm_launches(rk, period, s, targets, float(ages[period]), resolvers, b)
                 continue
             self._gs_launches(b, rk, period, s, targets, (s.name, targets))
+            if (s.name, period) in self._vmu_need:
+                self._vmu_launch(b, s, targets, period)
         self.launches = b.launches
         self._rec = b
         for rk in {id(l.module): l.module for l in self.launches if l.kind != "fues"}.values():
@@ -502,6 +534,29 @@ class SolvePlan:
         base, inst, step = self._geom(("pol" if pol else "V", name), (self.pol if pol else self.V)[name], 1)
         slots = np.array([self.slot[name][int(p)] for p in periods], dtype=np.int64)
         return base + inst[None, :] + slots[:, None] * step
+
+    def _mptrs_many(self, name: str, periods: np.ndarray) -> np.ndarray:
+        """(periods, instances) device addresses of a carried value array's
+        marginal-value rows (a two-slot ring indexed by period parity)."""
+        base, inst, step = self._geom(("vmu", name), self.vmu[name], 0)
+        return base + inst[None, :] + (np.asarray(periods, dtype=np.int64)[:, None] % 2) * step
+
+    def _vmu_launch(self, b: "_Records", s: RegimeSpec, targets, period: int) -> None:
+        """Marginal-value rows of regime `s` at `period`, from its value array."""
+        vk = self._vck[s.name]
+        n = self.n
+        pa = np.array([period], dtype=np.int64)
+        pbuf = self.params[(s.name, targets)]
+        grid = self.sgrid[s.name][[a.name for a in s.states].index(vk.euler)]
+        rows = np.zeros((n, vk.n_words), dtype=np.int64)
+        rows[:, vk.W_P] = pbuf.data_ptr() + self._ar * pbuf.stride(0) * pbuf.element_size()
+        rows[:, vk.W_PERIOD] = period
+        rows[:, vk.W_AGE] = self._age_words(pa)[0]
+        rows[:, vk.W_V] = self._vptrs_many(s.name, pa)[0]
+        rows[:, vk.W_M] = self._mptrs_many(s.name, pa)[0]
+        rows[:, vk.W_G] = grid.data_ptr()
+        rows[:, vk.W_NG] = grid.numel()
+        b.add("egm", vk, vk.name(), rows, [math.ceil(s.n_states / 256)] * n, 256, 0, period)
 
     def _cptrs_many(self, name: str, field: str, periods: np.ndarray) -> np.ndarray:
         """(periods, instances) device addresses of a DC-EGM carry field
@@ -686,6 +741,16 @@ class SolvePlan:
                     if i == 0:
                         out["carry"].append((w["scalar"], t.spec.name, None))
                     continue
+                if t.is_value:
+                    tgrid = self.sgrid[t.spec.name][[a.name for a in t.spec.states].index(t.value_euler)]
+                    r[w["tv"]] = self.V[t.spec.name][i, tslot].data_ptr()
+                    r[w["tm"]] = self.vmu[t.spec.name][(period + 1) % 2, i].data_ptr()
+                    r[w["tg"]] = tgrid.data_ptr()
+                    r[w["tn"]] = tgrid.numel()
+                    if i == 0:
+                        out["carry"].append((w["tv"], t.spec.name, None))
+                        out["carry"].append((w["tm"], t.spec.name, "vmu"))
+                    continue
                 if i == 0:
                     for f in ("rg", "rv", "mu", "nk"):
                         out["carry"].append((w[f], t.spec.name, f))
@@ -730,7 +795,12 @@ class SolvePlan:
         G[:, :, ek.W_V] = self._vptrs_many(name, pa)
         G[:, :, ek.W_POL] = self._vptrs_many(name, pa, pol=True)
         for w, tname, f in tm["carry"]:
-            G[:, :, w] = self._vptrs_many(tname, pa + 1) if f is None else self._cptrs_many(tname, f, pa + 1)
+            if f is None:
+                G[:, :, w] = self._vptrs_many(tname, pa + 1)
+            elif f == "vmu":
+                G[:, :, w] = self._mptrs_many(tname, pa + 1)
+            else:
+                G[:, :, w] = self._cptrs_many(tname, f, pa + 1)
         F = np.repeat(tm["fues"][None], P, axis=0)
         for w, f in ((4, "rg"), (5, "rc"), (6, "rv"), (7, "nk")):
             F[:, :, w] = self._cptrs_many(name, f, pa)
@@ -738,7 +808,7 @@ class SolvePlan:
         g.update({"index": {int(p): k for k, p in enumerate(pa)}, "rows": G, "fues": F})
         tw = [(ek.W_TASTE, s)]
         for t, w in zip(ek.er.targets, ek.W_T):
-            if not t.unreachable and t.next_R is not None:
+            if not t.unreachable and t.next_R is not None and not t.is_value:
                 tw.append((w["taste"], t.spec))
         g["taste_words"] = tw
         return g

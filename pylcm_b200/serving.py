@@ -86,15 +86,19 @@ def solve_bytes(eng: SolveEngine) -> int:
     T x states value (float64) and policy (int32) arrays per regime, the
     expectation tables (float64, plus float32 copies in the single-precision
     search), the action tables, the DC-EGM carry rows (two-period ring) and
-    candidates."""
+    candidates, and the marginal-value rows of regimes DC-EGM reads as value
+    arrays."""
     from pylcm_b200.egm import is_egm
 
     specs = eng.specs
     fp32 = eng.precision == "fp32"
+    any_egm = any(is_egm(s) and not s.terminal for s in specs)
     b = 0
     for s in specs:
         slots = max(len(s.active_periods), 1)
         b += slots * s.n_states * (8 + 4)
+        if any_egm and not is_egm(s) and any(a.kind == "continuous" for a in s.states):
+            b += 2 * s.n_states * 8  # marginal-value rows of a carried value array
         if is_egm(s) and not s.terminal:
             n_rows = 1
             for a in s.states + s.actions:

@@ -548,3 +548,161 @@ def ijrs_params(taste_scale=0.2):
         "working_life": {"taste_shocks": {"scale": taste_scale}},
         "retirement": {"next_wealth": {"labor_income": 0.0}},
     }
+
+
+def _ijrs_savings(wealth, consumption):
+    return wealth - consumption
+
+
+def _ijrs_next_wealth_from_savings(savings, labor_income, interest_rate, floor):
+    return jnp.maximum((1.0 + interest_rate) * savings + labor_income, floor)
+
+
+def _ijrs_inverse_mu(marginal_continuation, rho):
+    return marginal_continuation ** (-1.0 / rho)
+
+
+def ijrs_dcegm_model(savings_points=None):
+    """The DC-EGM twin: the same model with both living regimes solved by
+    DC-EGM on the fixture run's savings grid (uniform, 500 points on
+    [0, 50]) unless `savings_points` is given; the terminal regimes carry
+    their utility and its wealth gradient."""
+    from pylcm_b200 import (
+        ConsumptionSavingsRegime, ExtremeValueTasteShocks, IrregSpacedGrid, LinSpacedGrid, LiquidMargin,
+        LogSpacedGrid,
+    )
+    from pylcm_b200.solvers import DCEGM
+
+    sav = LinSpacedGrid(start=0.0, stop=50.0, n_points=500) if savings_points is None else \
+        IrregSpacedGrid(points=tuple(savings_points))
+    solver = DCEGM(savings_grid=sav)
+    margin = LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings")
+    wealth = IrregSpacedGrid(points=ijrs_wealth_points())
+    cons = LogSpacedGrid(start=0.001, stop=50.0, n_points=400)
+    alive = lambda age: age <= IJRS_LAST_ALIVE_AGE  # noqa: E731
+    working = ConsumptionSavingsRegime(
+        transition=_ijrs_nr_working, states={"wealth": wealth},
+        actions={"work_choice": DiscreteGrid(IjrsWork), "consumption": cons},
+        taste_shocks=ExtremeValueTasteShocks(), active=alive,
+        state_transitions={"wealth": _ijrs_next_wealth_from_savings},
+        functions={"utility": _ijrs_u_work, "is_working": _ijrs_is_working, "labor_income": _ijrs_labor_income,
+                   "savings": _ijrs_savings, "inverse_marginal_utility": _ijrs_inverse_mu},
+        solver=solver, liquid=margin,
+    )
+    retired = ConsumptionSavingsRegime(
+        transition=_ijrs_nr_retired, states={"wealth": wealth}, actions={"consumption": cons}, active=alive,
+        state_transitions={"wealth": _ijrs_next_wealth_from_savings},
+        functions={"utility": _ijrs_u_ret, "savings": _ijrs_savings, "inverse_marginal_utility": _ijrs_inverse_mu},
+        solver=solver, liquid=margin,
+    )
+    done_w = Regime(transition=None, states={"wealth": wealth}, functions={"utility": _ijrs_u_done_working})
+    done_r = Regime(transition=None, states={"wealth": wealth}, functions={"utility": _ijrs_u_done_retired})
+    return Model(regimes={"working_life": working, "retirement": retired, "done_from_working": done_w,
+                          "done_retired": done_r},
+                 ages=AgeGrid(start=IJRS_MIN_AGE, stop=IJRS_MIN_AGE + IJRS_N_PERIODS - 1, step="Y"),
+                 regime_id_class=IjrsRegimeId)
+
+
+# --------------------------------------------------------------------------
+# DC-EGM into value arrays: a DC-EGM regime with a Markov health state whose
+# targets are a grid-search regime (wealth x health) and a terminal regime
+# (bequest over wealth x health); both are read as carried value arrays, the
+# Markov health law folded into their rows.  The grids start at zero wealth,
+# where nothing is affordable (-inf values at the first node).
+# --------------------------------------------------------------------------
+@categorical(ordered=False)
+class VcRegimeId:
+    working: int
+    retired: int
+    done: int
+
+
+VC_N_PERIODS = 6
+
+
+def _vc_crra(c, rho):
+    return (c ** (1.0 - rho) - 1.0) / (1.0 - rho)
+
+
+def _vc_u_work(consumption, work_choice, health, rho, disutility):
+    return _vc_crra(consumption, rho) - jnp.where(work_choice == IjrsWork.work, disutility, 0.0) \
+        - 0.2 * (health == Health.bad)
+
+
+def _vc_u_ret(consumption, health, rho):
+    return _vc_crra(consumption, rho) - 0.2 * (health == Health.bad)
+
+
+def _vc_u_done(wealth, health, rho, weight):
+    return weight * (1.0 + 0.5 * (health == Health.good)) * _vc_crra(wealth + 1.0, rho)
+
+
+def _vc_savings(wealth, consumption):
+    return wealth - consumption
+
+
+def _vc_next_wealth_work(savings, work_choice, health, interest_rate, wage):
+    earn = jnp.where(work_choice == IjrsWork.work, wage * (0.6 + 0.4 * (health == Health.good)), 0.0)
+    return (1.0 + interest_rate) * savings + earn
+
+
+def _vc_next_wealth_ret(wealth, consumption, interest_rate):
+    return (1.0 + interest_rate) * (wealth - consumption)
+
+
+def _vc_next_health(health, p_stay_good, p_recover):
+    good = health == Health.good
+    p_good = jnp.where(good, p_stay_good, p_recover)
+    return jnp.array([1.0 - p_good, p_good])
+
+
+def _vc_inverse_mu(marginal_continuation, rho):
+    return marginal_continuation ** (-1.0 / rho)
+
+
+def _vc_budget(consumption, wealth):
+    return consumption <= wealth
+
+
+def _vc_nr_working(work_choice, age):
+    return jnp.where(age >= VC_N_PERIODS - 2, VcRegimeId.done,
+                     jnp.where(work_choice == IjrsWork.retire, VcRegimeId.retired, VcRegimeId.working))
+
+
+def _vc_nr_retired(age):
+    return jnp.where(age >= VC_N_PERIODS - 2, VcRegimeId.done, VcRegimeId.retired)
+
+
+def value_children_model(taste=False, n_wealth=60, n_savings=80):
+    from pylcm_b200 import ConsumptionSavingsRegime, ExtremeValueTasteShocks, LiquidMargin
+    from pylcm_b200.solvers import DCEGM
+
+    wealth = LinSpacedGrid(start=0.0, stop=40.0, n_points=n_wealth)
+    cons = LinSpacedGrid(start=0.05, stop=40.0, n_points=120)
+    health = DiscreteGrid(Health)
+    alive = lambda age: age <= VC_N_PERIODS - 2  # noqa: E731
+    working = ConsumptionSavingsRegime(
+        transition=_vc_nr_working, states={"health": health, "wealth": wealth},
+        actions={"work_choice": DiscreteGrid(IjrsWork), "consumption": cons},
+        taste_shocks=ExtremeValueTasteShocks() if taste else None, active=alive,
+        state_transitions={"wealth": _vc_next_wealth_work, "health": MarkovTransition(_vc_next_health)},
+        functions={"utility": _vc_u_work, "savings": _vc_savings, "inverse_marginal_utility": _vc_inverse_mu},
+        solver=DCEGM(savings_grid=LinSpacedGrid(start=0.0, stop=40.0, n_points=n_savings)),
+        liquid=LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings"),
+    )
+    retired = Regime(
+        transition=_vc_nr_retired, states={"wealth": wealth, "health": health}, actions={"consumption": cons},
+        active=alive, state_transitions={"wealth": _vc_next_wealth_ret, "health": MarkovTransition(_vc_next_health)},
+        constraints={"budget": _vc_budget}, functions={"utility": _vc_u_ret},
+    )
+    done = Regime(transition=None, states={"wealth": wealth, "health": health}, functions={"utility": _vc_u_done})
+    return Model(regimes={"working": working, "retired": retired, "done": done},
+                 ages=AgeGrid(start=0, stop=VC_N_PERIODS - 1, step="Y"), regime_id_class=VcRegimeId)
+
+
+def value_children_params(taste_scale=None, p_stay_good=0.9):
+    p = {"discount_factor": 0.95, "rho": 2.0, "disutility": 0.3, "interest_rate": 0.04, "wage": 3.0,
+         "p_stay_good": p_stay_good, "p_recover": 0.4, "weight": 2.0}
+    if taste_scale is not None:
+        p["working"] = {"taste_shocks": {"scale": taste_scale}}
+    return p

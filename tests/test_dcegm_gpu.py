@@ -81,3 +81,19 @@ def test_dcegm_simulation_matches_oracle(taste):
         np.testing.assert_allclose(res.periods[p]["value"], ora[p]["value"], rtol=1e-9, atol=1e-9, equal_nan=True)
         for name in ("consumption", "labor_supply"):
             np.testing.assert_allclose(res.periods[p]["actions"][name], ora[p]["actions"][name], equal_nan=True)
+
+
+@pytest.mark.parametrize("taste", [None, 0.1])
+def test_dcegm_reads_grid_search_and_terminal_value_arrays(taste):
+    """DC-EGM regime whose targets are a grid-search regime and a terminal
+    regime over wealth x Markov health: both carried as value arrays (the
+    grid-search one with its finite-difference wealth slope, the terminal
+    one with its utility gradient), the health law folded into the rows;
+    -inf values at zero wealth."""
+    model = M.value_children_model(taste=taste is not None)
+    for params in (M.value_children_params(taste), M.value_children_params(taste, p_stay_good=0.7)):
+        V = model.solve(params=params, log_level="off")
+        Vo, _ = oracle_solve(model, params)
+        for p in Vo:
+            for r in Vo[p]:
+                assert rel_err(V[p][r], Vo[p][r]) < 1e-10, (p, r)
