@@ -16,7 +16,6 @@ from __future__ import annotations
 
 from typing import Sequence
 
-import numpy as np
 
 from pylcm_b200.engine import SolveEngine, SolvePlan
 
@@ -46,11 +45,6 @@ class BatchSolver:
         self._host_pol = {
             r: torch.empty(tuple(v.shape), dtype=torch.int32, pin_memory=True) for r, v in self.plan.pol.items()
         }
-        self._rk_for = {}
-        for key in self._pkeys:
-            name, targets = key
-            spec = next(s for s in self.engine.specs if s.name == name)
-            self._rk_for[key] = self.engine.kernels(spec, targets, template_params, self.n)
         if use_graph:
             self.plan.capture()
 
@@ -59,12 +53,9 @@ class BatchSolver:
         """Host-side packing of parameter vectors (float64, plan layout)."""
         if len(params_list) != self.n:
             raise ValueError(f"expected {self.n} parameter sets, got {len(params_list)}")
-        out = {}
-        for key in self._pkeys:
-            rk = self._rk_for[key]
-            rows = [rk.tr.pack_params(rk.tr.values_for(self.engine.resolver(p))) for p in params_list]
-            out[key] = np.stack(rows)
-        return out
+        resolvers = [self.engine.resolver(p) for p in params_list]
+        memo: dict = {}
+        return {key: self.plan._pack_many[key](resolvers, memo) for key in self._pkeys}
 
     def upload(self, packed: dict, non_blocking: bool = True) -> int:
         """Copy packed parameters host->device; returns bytes copied."""

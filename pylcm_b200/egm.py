@@ -281,5 +281,10 @@ def _pack_for(self, resolver):
     return tr.pack_params(tr.values_for(resolver))
 
 
+def _pack_many(self, resolvers, memo=None):
+    return _as_traced(self).pack_many(resolvers, memo)
+
+
 EgmRegime.tracer_layout = _tracer_layout
 EgmRegime.pack_for = _pack_for
+EgmRegime.pack_many = _pack_many

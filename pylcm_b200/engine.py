@@ -293,9 +293,11 @@ class SolvePlan:
         by = {s.name: s for s in specs}
         self.params: dict[tuple, Any] = {}
         self._packers: dict[tuple, Any] = {}  # params key -> packer(resolver) -> float64 vector
+        self._pack_many: dict[tuple, Any] = {}  # params key -> packer(resolvers, memo) -> rows
         self.ev: dict[tuple, tuple] = {}
         step_list: list[tuple[int, RegimeSpec, tuple, Any]] = []
         egm_steps: list = []
+        pack_memo: dict = {}  # parameter columns shared by a regime's target sets
         for period in range(T - 1, -1, -1):
             for s in specs:
                 if period not in s.active_periods:
@@ -307,17 +309,19 @@ class SolvePlan:
                 if is_egm(s) and not s.terminal:
                     ek = eng.egm_kernels(s, targets, params_list[0])
                     if key not in self.params:
-                        vecs = [ek.er.pack_for(r) for r in resolvers]
-                        self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                        vecs = ek.er.pack_many(resolvers, pack_memo)
+                        self.params[key] = torch.as_tensor(vecs, dtype=torch.float64, device=dev)
                         self._packers[key] = ek.er.pack_for
+                        self._pack_many[key] = ek.er.pack_many
                     egm_steps.append((period, s, targets, ek))
                     step_list.append((period, s, targets, ek))
                     continue
                 rk = eng.kernels(s, targets, params_list[0], n)
                 if key not in self.params:
-                    vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in resolvers]
-                    self.params[key] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                    vecs = rk.tr.pack_many(resolvers, pack_memo)
+                    self.params[key] = torch.as_tensor(vecs, dtype=torch.float64, device=dev)
                     self._packers[key] = lambda r, tr=rk.tr: tr.pack_params(tr.values_for(r))
+                    self._pack_many[key] = rk.tr.pack_many
                 step_list.append((period, s, targets, rk))
         # DC-EGM buffers: carry rows per active period, scratch per regime
         self.egm: dict[str, dict] = {}
@@ -639,9 +643,9 @@ class SolvePlan:
             rk = eng.kernels(s, targets, self.params_list[0], n)
             pkey = (s.name, targets, "gs")
             if pkey not in self.params:
-                vecs = [rk.tr.pack_params(rk.tr.values_for(r)) for r in self.resolvers]
-                self.params[pkey] = torch.as_tensor(np.stack(vecs), dtype=torch.float64, device=dev)
+                self.params[pkey] = torch.as_tensor(rk.tr.pack_many(self.resolvers), dtype=torch.float64, device=dev)
                 self._packers[pkey] = lambda r, tr=rk.tr: tr.pack_params(tr.values_for(r))
+                self._pack_many[pkey] = rk.tr.pack_many
             for t in rk.targets:
                 if t.scalar or not (t.needs_contraction or fp32):
                     continue

@@ -24,7 +24,7 @@ import dataclasses
 import inspect
 import math
 from collections.abc import Mapping
-from typing import Any, Callable
+from typing import Any, Callable, Sequence
 
 import numpy as np
 
@@ -334,6 +334,70 @@ class TracedRegime:
                     f"parameter {flat} has shape {v.shape}, expected {self.param_values[flat].shape}"
                 )
             out[flat] = v
+        return out
+
+    def pack_many(self, resolvers: Sequence["ParamResolver"], memo: dict | None = None) -> np.ndarray:
+        """Packed vectors of many parameter sets, one row each: the same
+        numbers as ``pack_params(values_for(r))`` row by row, gathered one
+        parameter (column) at a time.  `memo` shares the gathered columns
+        between the traces of one regime (one per target set) packing the same
+        resolvers; process tables are computed once per distinct set of
+        process parameters."""
+        cached = self.__dict__.get("_layout_cache")
+        if cached is None:
+            cached = self.__dict__["_layout_cache"] = self.param_layout()
+        layout, total = cached
+        n = len(resolvers)
+        out = np.zeros((n, max(total, 1)), dtype=np.float64)
+        memo = {} if memo is None else memo
+        name = self.spec.name
+        for flat in self.param_order:
+            off, shape = layout[flat]
+            src = self.param_sources[flat]
+            key = (name, *src)
+            col = memo.get(key)
+            if col is None:
+                if src[0] == "arg":
+                    vals = []
+                    for r in resolvers:
+                        ok, val = r.find(name, src[1], src[2])
+                        if not ok:
+                            raise InvalidParamsError(f"regime {name!r}: missing parameter {src[2]!r} of {src[1]!r}")
+                        vals.append(val)
+                elif src[0] == "proc_field":
+                    ax = self.spec.state(src[1])
+                    vals = [float(r.process_params(name, src[1], ax.grid)[src[2]]) for r in resolvers]
+                else:
+                    ax = self.spec.state(src[1])
+                    tables: dict = memo.setdefault(("__proc_tables__", name, src[1]), {})
+                    vals = []
+                    for r in resolvers:
+                        pp = r.process_params(name, src[1], ax.grid)
+                        tk = tuple((k, np.asarray(v, dtype=np.float64).tobytes()) for k, v in sorted(pp.items()))
+                        tab = tables.get(tk)
+                        if tab is None:
+                            tab = tables[tk] = (
+                                np.asarray(ax.grid.compute_gridpoints(**pp), dtype=np.float64),
+                                np.asarray(ax.grid.compute_transition_probs(**pp), dtype=np.float64),
+                            )
+                        vals.append(tab[0 if src[0] == "proc_nodes" else 1])
+                try:
+                    col = np.asarray(vals, dtype=np.float64)
+                except ValueError:
+                    col = None
+                want = (n, *np.shape(self.param_values[flat]))
+                if col is None or col.shape != want:
+                    bad = next(
+                        (np.shape(v) for v in vals if np.shape(v) != np.shape(self.param_values[flat])), None
+                    )
+                    raise InvalidParamsError(
+                        f"parameter {flat} has shape {bad}, expected {np.shape(self.param_values[flat])}"
+                    )
+                col = col.reshape(n, -1)
+                memo[key] = col
+            width = max(1, col.shape[1])
+            if col.shape[1]:
+                out[:, off : off + width] = col
         return out
 
     def pack_params(self, values: dict | None = None) -> np.ndarray:
