@@ -175,22 +175,28 @@ def run_ours(args) -> dict:
     # ---- end to end through the public batch API (host params -> host V)
     torch.cuda.synchronize()
     e2e_ms = []
+    phases = []
     h2d = d2h = 0
     for k in range(max(1, min(args.steps, 3))):
         flush_l2(torch, flush)
         torch.cuda.synchronize()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
+        ev4 = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         t0 = time.perf_counter()
-        s0.record(stream)
         pk = fast.pack(params)
+        t1 = time.perf_counter()
+        ev4[0].record(stream)
         h2d = fast.upload(pk)
+        ev4[1].record(stream)
         fast.run()
+        ev4[2].record(stream)
         d2h = fast.download(policy=False)
-        s1.record(stream)
+        ev4[3].record(stream)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        phases.append(((t1 - t0) * 1e3, ev4[0].elapsed_time(ev4[1]), ev4[1].elapsed_time(ev4[2]),
+                       ev4[2].elapsed_time(ev4[3])))
     e2e_value = args.batch / (statistics.median(e2e_ms) / 1e3) * world
+    ph = np.median(np.asarray(phases), axis=0)
 
     # ---- kernel-level timing of the dominant kernel (kernel a), eager, events
     plan = fast.plan
@@ -354,6 +360,8 @@ def run_ours(args) -> dict:
             "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h),
             "api": "pylcm_b200.batch.BatchSolver pack+upload+run+download (host params -> host V)",
+            "phases_ms": {"pack_host": float(ph[0]), "h2d": float(ph[1]), "run": float(ph[2]),
+                          "d2h": float(ph[3])},
         },
         "gpu_launches": fast.gpu_launches * args.steps,
         "roofline": {
