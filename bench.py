@@ -187,9 +187,8 @@ def run_ours(args) -> dict:
         ev4[0].record(stream)
         h2d = fast.upload(pk)
         ev4[1].record(stream)
-        fast.run()
         ev4[2].record(stream)
-        d2h = fast.download(policy=False)
+        d2h = fast.run_download(policy=False)  # per-period copies overlap the compute
         ev4[3].record(stream)
         torch.cuda.synchronize()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
@@ -359,9 +358,8 @@ def run_ours(args) -> dict:
             "unit": UNIT,
             "h2d_bytes_per_step": int(h2d),
             "d2h_bytes_per_step": int(d2h),
-            "api": "pylcm_b200.batch.BatchSolver pack+upload+run+download (host params -> host V)",
-            "phases_ms": {"pack_host": float(ph[0]), "h2d": float(ph[1]), "run": float(ph[2]),
-                          "d2h": float(ph[3])},
+            "api": "pylcm_b200.batch.BatchSolver pack+upload+run_download (host params -> host V)",
+            "phases_ms": {"pack_host": float(ph[0]), "h2d": float(ph[1]), "run_and_overlapped_d2h": float(ph[3])},
         },
         "gpu_launches": fast.gpu_launches * args.steps,
         "roofline": {

@@ -23,6 +23,8 @@
  *                           src/_lcm/egm/upper_envelope/fues.py:151-338.
  *   lcmx_count_nonfinite <- the per-period NaN/Inf diagnostics,
  *                           backward_induction.py:205-236.
+ *   lcmx_copy_rows_d2h   <- the device->host read of a period's value
+ *                           arrays (the `np.asarray` of the returned V).
  *
  * Conventions: every pointer argument that names array data is a DEVICE
  * pointer; sizes are element counts; `stream` is a cudaStream_t (NULL = the
@@ -149,6 +151,14 @@ int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const double* polic
  * (+-inf), which the caller zeroes. */
 int lcmx_count_nonfinite(lcmx_ctx* ctx, const double* x, long long n,
                          unsigned long long* counts_dev, void* stream);
+
+/* Asynchronous strided device->host copy of `rows` rows of `row_bytes` bytes:
+ * row r goes from src + r * src_pitch (device) to dst + r * dst_pitch (host;
+ * page-locked for the copy to overlap kernels).  Used to read one period's
+ * slice of every instance's value array while later periods compute.  The
+ * one exception to the device-pointer convention: `dst` is a HOST pointer. */
+int lcmx_copy_rows_d2h(lcmx_ctx* ctx, void* dst, size_t dst_pitch, const void* src, size_t src_pitch,
+                       size_t row_bytes, size_t rows, void* stream);
 
 #ifdef __cplusplus
 }

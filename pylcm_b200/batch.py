@@ -84,13 +84,73 @@ class BatchSolver:
                 nbytes += v.numel() * 4
         return nbytes
 
+    def run_download(self, policy: bool = False) -> int:
+        """Run the backward induction and copy its results to the pinned host
+        arrays, each period's slice of every value (and policy) array read on
+        a copy stream as soon as that period's launches are done -- the copies
+        of late periods overlap the computation of the early ones.  Launches
+        are issued eagerly, period by period, on the current stream, which
+        waits for the copies at the end.  Returns the bytes copied."""
+        from pylcm_b200.runtime import get_context
+
+        torch = self.torch
+        plan = self.plan
+        ctx = get_context(self.engine.device)
+        if plan._prepared is None:
+            plan._prepared = plan._prepare()
+        comp = torch.cuda.current_stream(plan.dev)
+        copy = self.__dict__.get("_copy_stream")
+        if copy is None:
+            copy = self._copy_stream = torch.cuda.Stream(plan.dev)
+        by_period: dict[int, list] = {}
+        for s in self.engine.specs:
+            for period, k in plan.slot[s.name].items():
+                by_period.setdefault(period, []).append((s, k))
+        nbytes = 0
+        launches = plan.launches
+        i = 0
+        while i < len(launches):
+            period = launches[i].period
+            while i < len(launches) and launches[i].period == period:
+                plan._prepared[i](comp.cuda_stream)
+                i += 1
+            ev = torch.cuda.Event()
+            ev.record(comp)
+            copy.wait_event(ev)
+            for s, k in by_period.pop(period, []):
+                nbytes += self._copy_slot(ctx, s, k, policy, copy.cuda_stream)
+        # periods without launches of their own (none in a solve plan)
+        for period, items in by_period.items():
+            ev = torch.cuda.Event()
+            ev.record(comp)
+            copy.wait_event(ev)
+            for s, k in items:
+                nbytes += self._copy_slot(ctx, s, k, policy, copy.cuda_stream)
+        comp.wait_stream(copy)
+        return nbytes
+
+    def _copy_slot(self, ctx, s, k: int, policy: bool, stream: int) -> int:
+        """Copy slot k (one period) of every instance's value (and policy)
+        array of regime `s`: n rows of n_states entries, strided by the slots."""
+        nbytes = 0
+        arrays = [(self.plan.V[s.name], self._host_V[s.name])]
+        if policy:
+            arrays.append((self.plan.pol[s.name], self._host_pol[s.name]))
+        for dev_t, host_t in arrays:
+            es = dev_t.element_size()
+            row = dev_t.shape[2] * es
+            pitch = dev_t.stride(0) * es
+            off = k * dev_t.stride(1) * es
+            ctx.copy_rows_d2h(host_t.data_ptr() + off, pitch, dev_t.data_ptr() + off, pitch, row, dev_t.shape[0], stream)
+            nbytes += row * dev_t.shape[0]
+        return nbytes
+
     def solve(self, params_list: Sequence, return_policy: bool = False):
         """Solve `params_list` (len == batch_size); returns per-instance
         ``{period: {regime: V}}`` host arrays (and policies)."""
         packed = self.pack(params_list)
         self.upload(packed)
-        self.run()
-        self.download(policy=return_policy)
+        self.run_download(policy=return_policy)
         self.torch.cuda.current_stream().synchronize()
         return self.results(return_policy)
 

@@ -393,6 +393,17 @@ extern "C" int lcmx_count_nonfinite(lcmx_ctx* ctx, const double* x, long long n,
   return LCMX_OK;
 }
 
+extern "C" int lcmx_copy_rows_d2h(lcmx_ctx* ctx, void* dst, size_t dst_pitch, const void* src, size_t src_pitch,
+                                  size_t row_bytes, size_t rows, void* stream) {
+  if (!ctx || (rows > 0 && (!dst || !src)) || row_bytes > dst_pitch || row_bytes > src_pitch)
+    return set_err(ctx, LCMX_ERR_ARGS, "lcmx_copy_rows_d2h: bad args");
+  if (rows == 0 || row_bytes == 0) return LCMX_OK;
+  cudaError_t e = cudaMemcpy2DAsync(dst, dst_pitch, src, src_pitch, row_bytes, rows, cudaMemcpyDeviceToHost,
+                                    (cudaStream_t)stream);
+  if (e != cudaSuccess) return set_err(ctx, LCMX_ERR_LAUNCH, std::string("copy_rows_d2h: ") + cudaGetErrorString(e));
+  return LCMX_OK;
+}
+
 // error helper shared with the other translation units of this library
 int lcmx_set_error_from(lcmx_ctx* ctx, int code, const std::string& msg) { return set_err(ctx, code, msg); }
 

@@ -31,6 +31,7 @@ EXPORTED = (
     "lcmx_fues_scan",
     "lcmx_fues_scan_static",
     "lcmx_fues_step",
+    "lcmx_copy_rows_d2h",
 )
 
 
@@ -78,6 +79,8 @@ def load_library() -> ctypes.CDLL:
             "lcmx_simulate": ([vp, cp, ctypes.POINTER(LaunchArgs), ctypes.c_ulonglong, vp], ip),
             "lcmx_egm_step": ([vp, cp, ctypes.POINTER(LaunchArgs), vp], ip),
             "lcmx_count_nonfinite": ([vp, vp, ctypes.c_longlong, vp, vp], ip),
+            "lcmx_copy_rows_d2h": ([vp, vp, ctypes.c_size_t, vp, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_size_t, vp],
+                                   ip),
             "lcmx_fues_workspace_bytes": ([ip, ip], ctypes.c_size_t),
             "lcmx_fues_scan": (
                 [vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp, ctypes.c_size_t, vp],
@@ -132,6 +135,11 @@ class Context:
 
     def count_nonfinite(self, ptr: int, n: int, counts_ptr: int, stream: int) -> None:
         self.check(self.lib.lcmx_count_nonfinite(self.h, ptr, n, counts_ptr, stream))
+
+    def copy_rows_d2h(self, dst: int, dst_pitch: int, src: int, src_pitch: int, row_bytes: int, rows: int,
+                      stream: int) -> None:
+        """Strided device->host copy (host `dst` page-locked for overlap)."""
+        self.check(self.lib.lcmx_copy_rows_d2h(self.h, dst, dst_pitch, src, src_pitch, row_bytes, rows, stream))
 
     def fues_step(self, items: int, prefix: int, n_items: int, n_rows: int, max_n_in: int, stream: int) -> None:
         """FUES of the rows of several candidate blocks (device item records)."""

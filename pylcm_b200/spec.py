@@ -198,6 +198,11 @@ def _is_leaf(v: Any) -> bool:
     return not isinstance(v, Mapping)
 
 
+# process object id -> (process, fixed parameters, runtime parameter names);
+# the entry keeps the process alive so that its id stays its own
+_PROC_FIELDS: dict[int, tuple] = {}
+
+
 class ParamResolver:
     """Looks up a function argument's value in user params / fixed params."""
 
@@ -232,8 +237,11 @@ class ParamResolver:
         return dict(out)
 
     def _process_params(self, regime: str, state: str, proc: _Process) -> dict:
-        out = dict(proc.fixed_params)
-        for name in proc.runtime_param_names:
+        ent = _PROC_FIELDS.get(id(proc))
+        if ent is None or ent[0] is not proc:
+            ent = _PROC_FIELDS[id(proc)] = (proc, dict(proc.fixed_params), tuple(proc.runtime_param_names))
+        out = dict(ent[1])
+        for name in ent[2]:
             found = False
             for src in self.sources:
                 for holder in (src.get(regime), src):
@@ -365,22 +373,26 @@ class TracedRegime:
                             raise InvalidParamsError(f"regime {name!r}: missing parameter {src[2]!r} of {src[1]!r}")
                         vals.append(val)
                 elif src[0] == "proc_field":
-                    ax = self.spec.state(src[1])
-                    vals = [float(r.process_params(name, src[1], ax.grid)[src[2]]) for r in resolvers]
+                    pps = self._process_params_of(resolvers, src[1], memo)
+                    vals = [float(pp[src[2]]) for pp in pps]
                 else:
+                    # one table per distinct set of process parameters
                     ax = self.spec.state(src[1])
+                    tk_key = ("__proc_table_keys__", name, src[1])
+                    keys = memo.get(tk_key)
                     tables: dict = memo.setdefault(("__proc_tables__", name, src[1]), {})
-                    vals = []
-                    for r in resolvers:
-                        pp = r.process_params(name, src[1], ax.grid)
-                        tk = tuple((k, np.asarray(v, dtype=np.float64).tobytes()) for k, v in sorted(pp.items()))
-                        tab = tables.get(tk)
-                        if tab is None:
-                            tab = tables[tk] = (
-                                np.asarray(ax.grid.compute_gridpoints(**pp), dtype=np.float64),
-                                np.asarray(ax.grid.compute_transition_probs(**pp), dtype=np.float64),
-                            )
-                        vals.append(tab[0 if src[0] == "proc_nodes" else 1])
+                    if keys is None:
+                        keys = []
+                        for pp in self._process_params_of(resolvers, src[1], memo):
+                            tk = tuple((k, np.asarray(v, dtype=np.float64).tobytes()) for k, v in sorted(pp.items()))
+                            if tk not in tables:
+                                tables[tk] = (
+                                    np.asarray(ax.grid.compute_gridpoints(**pp), dtype=np.float64),
+                                    np.asarray(ax.grid.compute_transition_probs(**pp), dtype=np.float64),
+                                )
+                            keys.append(tk)
+                        memo[tk_key] = keys
+                    vals = [tables[tk][0 if src[0] == "proc_nodes" else 1] for tk in keys]
                 try:
                     col = np.asarray(vals, dtype=np.float64)
                 except ValueError:
@@ -399,6 +411,15 @@ class TracedRegime:
             if col.shape[1]:
                 out[:, off : off + width] = col
         return out
+
+    def _process_params_of(self, resolvers, state: str, memo: dict) -> list:
+        """Process parameters of `state` for every resolver (memoised)."""
+        key = ("__proc_params__", self.spec.name, state)
+        pps = memo.get(key)
+        if pps is None:
+            ax = self.spec.state(state)
+            pps = memo[key] = [r.process_params(self.spec.name, state, ax.grid) for r in resolvers]
+        return pps
 
     def pack_params(self, values: dict | None = None) -> np.ndarray:
         values = self.param_values if values is None else values

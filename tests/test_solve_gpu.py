@@ -153,3 +153,39 @@ def test_launch_shape_keeps_the_fp64_bars(case, lanes, sb):
                 g = np.asarray(gaps[p][r]).reshape(a.shape)
                 sel = g > 1e-9
                 np.testing.assert_array_equal(P2[p][r].cpu().numpy()[sel], P1[p][r].cpu().numpy()[sel])
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batch_solver_overlapped_download_equals_the_device_arrays(precision):
+    """`BatchSolver.solve` reads each period's value and policy slices on a
+    copy stream while later periods compute; the host arrays equal the
+    device arrays and the graph-replay + whole-array download path."""
+    import torch
+
+    from pylcm_b200.batch import BatchSolver
+
+    model = M.stochastic_model(6, 60, 80)
+    ps = [M.stochastic_params(beta=b, crra=c) for b, c in ((0.95, 2.0), (0.9, 3.0), (0.97, 1.5))]
+    bs = BatchSolver(model, len(ps), precision, template_params=ps[0])
+    Vs, Ps = bs.solve(ps, return_policy=True)
+    for r, v in bs.plan.V.items():
+        assert torch.equal(torch.nan_to_num(bs._host_V[r], nan=5.0), torch.nan_to_num(v.cpu(), nan=5.0))
+        assert torch.equal(bs._host_pol[r], bs.plan.pol[r].cpu())
+    keep = [{p: {r: np.array(a) for r, a in d.items()} for p, d in V.items()} for V in Vs]
+    for h in bs._host_V.values():
+        h.zero_()
+    bs.upload(bs.pack(ps))
+    bs.run()
+    bs.download(policy=True)
+    torch.cuda.synchronize()
+    for i, V in enumerate(bs.results()):
+        for p in V:
+            for r in V[p]:
+                assert np.array_equal(V[p][r], keep[i][p][r], equal_nan=True)
+    if precision == "fp32":
+        return  # single solves may take another launch shape (last-ulp differences)
+    for i, p_ in enumerate(ps):
+        V1, _ = model.engine(precision).solve(p_)
+        for per in V1:
+            for r in V1[per]:
+                assert np.array_equal(V1[per][r].cpu().numpy(), keep[i][per][r], equal_nan=True)
