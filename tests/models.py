@@ -706,3 +706,79 @@ def value_children_params(taste_scale=None, p_stay_good=0.9):
     if taste_scale is not None:
         p["working"] = {"taste_shocks": {"scale": taste_scale}}
     return p
+
+
+# --------------------------------------------------------------------------
+# DC-EGM with an AR(1) income process (Tauchen): the DC-EGM regime's rows
+# include the process state; its targets are itself and a grid-search
+# regime over (wealth, income), the process law's transition-matrix row
+# folded into the carried value array.
+# --------------------------------------------------------------------------
+@categorical(ordered=False)
+class EpRegimeId:
+    working: int
+    retired: int
+    dead: int
+
+
+EP_N_PERIODS = 6
+
+
+def _ep_u_work(consumption, work_choice, rho, disutility):
+    return _vc_crra(consumption, rho) - jnp.where(work_choice == IjrsWork.work, disutility, 0.0)
+
+
+def _ep_u_ret(consumption, rho):
+    return _vc_crra(consumption, rho)
+
+
+def _ep_next_wealth_work(savings, work_choice, income, interest_rate, wage):
+    return (1.0 + interest_rate) * savings + jnp.where(work_choice == IjrsWork.work, wage * jnp.exp(income), 0.0)
+
+
+def _ep_next_wealth_ret(wealth, consumption, interest_rate, pension):
+    return (1.0 + interest_rate) * (wealth - consumption) + pension
+
+
+def _ep_nr_working(work_choice, age):
+    return jnp.where(age >= EP_N_PERIODS - 2, EpRegimeId.dead,
+                     jnp.where(work_choice == IjrsWork.retire, EpRegimeId.retired, EpRegimeId.working))
+
+
+def _ep_nr_retired(age):
+    return jnp.where(age >= EP_N_PERIODS - 2, EpRegimeId.dead, EpRegimeId.retired)
+
+
+def egm_process_model(taste=False, n_wealth=50, n_savings=60):
+    from pylcm_b200 import ConsumptionSavingsRegime, ExtremeValueTasteShocks, LiquidMargin
+    from pylcm_b200.solvers import DCEGM
+
+    wealth = LinSpacedGrid(start=0.0, stop=40.0, n_points=n_wealth)
+    cons = LinSpacedGrid(start=0.05, stop=40.0, n_points=100)
+    income = TauchenAR1Process(n_points=5, gauss_hermite=False, n_std=2.0)
+    alive = lambda age: age <= EP_N_PERIODS - 2  # noqa: E731
+    working = ConsumptionSavingsRegime(
+        transition=_ep_nr_working, states={"wealth": wealth, "income": income},
+        actions={"work_choice": DiscreteGrid(IjrsWork), "consumption": cons},
+        taste_shocks=ExtremeValueTasteShocks() if taste else None, active=alive,
+        state_transitions={"wealth": _ep_next_wealth_work},
+        functions={"utility": _ep_u_work, "savings": _vc_savings, "inverse_marginal_utility": _vc_inverse_mu},
+        solver=DCEGM(savings_grid=LinSpacedGrid(start=0.0, stop=40.0, n_points=n_savings)),
+        liquid=LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings"),
+    )
+    retired = Regime(
+        transition=_ep_nr_retired, states={"wealth": wealth, "income": income}, actions={"consumption": cons},
+        active=alive, state_transitions={"wealth": _ep_next_wealth_ret},
+        constraints={"budget": _vc_budget}, functions={"utility": _ep_u_ret},
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(regimes={"working": working, "retired": retired, "dead": dead},
+                 ages=AgeGrid(start=0, stop=EP_N_PERIODS - 1, step="Y"), regime_id_class=EpRegimeId)
+
+
+def egm_process_params(taste_scale=None, rho=0.9):
+    p = {"discount_factor": 0.95, "rho": 2.0, "disutility": 0.4, "interest_rate": 0.04, "wage": 2.0,
+         "pension": 0.5, "income": {"rho": rho, "sigma": 0.2, "mu": 0.0}}
+    if taste_scale is not None:
+        p["working"] = {"taste_shocks": {"scale": taste_scale}}
+    return p

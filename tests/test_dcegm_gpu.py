@@ -127,3 +127,32 @@ def test_simulation_through_value_array_targets_matches_oracle(taste):
         np.testing.assert_allclose(res.periods[p]["value"], ora[p]["value"], rtol=1e-9, atol=1e-9, equal_nan=True)
         for name in ("consumption", "work_choice"):
             np.testing.assert_allclose(res.periods[p]["actions"][name], ora[p]["actions"][name], equal_nan=True)
+
+
+@pytest.mark.parametrize("taste", [None, 0.1])
+def test_dcegm_with_an_income_process_matches_oracle(taste):
+    """DC-EGM rows over an AR(1) income process (Tauchen transition rows as
+    the weights of its own carry and of a grid-search target's value array),
+    solve and simulation against the oracle."""
+    from oracle.simulate import simulate as oracle_simulate
+
+    model = M.egm_process_model(taste=taste is not None)
+    for params in (M.egm_process_params(taste), M.egm_process_params(taste, rho=0.5)):
+        V = model.solve(params=params, log_level="off")
+        Vo, _ = oracle_solve(model, params)
+        for p in Vo:
+            for r in Vo[p]:
+                assert rel_err(V[p][r], Vo[p][r]) < 1e-10, (p, r)
+    n = 64
+    rng = np.random.default_rng(8)
+    rid = {s.name: s.rid for s in model.regime_specs}
+    ic = {"wealth": rng.uniform(0.5, 30, n), "income": rng.normal(0.0, 0.3, n), "age": np.zeros(n),
+          "regime_id": np.where(rng.uniform(size=n) < 0.7, rid["working"], rid["retired"])}
+    res = model.simulate(params=params, initial_conditions=ic, seed=4)
+    ora = oracle_simulate(model, params, ic, seed=4)
+    for p in ora:
+        np.testing.assert_array_equal(res.periods[p]["regime_id"], ora[p]["regime_id"])
+        for name in ("wealth", "income"):
+            np.testing.assert_allclose(res.periods[p]["states"][name], ora[p]["states"][name], rtol=1e-9, atol=1e-9,
+                                       equal_nan=True)
+        np.testing.assert_allclose(res.periods[p]["value"], ora[p]["value"], rtol=1e-9, atol=1e-9, equal_nan=True)
