@@ -136,14 +136,15 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
                 cont_arg = Qd.argmax(axis=2)
                 Qc = Qd.max(axis=2)
                 noise = np.stack([scale * (rng.gumbel(64 + d) - EULER_GAMMA) for d in range(nd)], axis=1)
-                noisy = np.where(np.isfinite(Qc), Qc + noise, -np.inf)
+                noisy = Qc + noise  # -inf stays -inf, a NaN cell is NaN (argmax: first NaN)
                 dstar = noisy.argmax(axis=1)
                 aa = dstar * nc + cont_arg[np.arange(len(sel)), dstar]
                 v = Qc[np.arange(len(sel)), dstar]
             else:
+                # argmax_and_max (argmax.py:55-69): the first feasible action at
+                # the max; a NaN max, or no feasible action, matches none: 0
                 v = Qm.max(axis=1)
                 aa = ((Qm == v[:, None]) & F).argmax(axis=1)
-                aa = np.where(np.isfinite(v) | np.isnan(v), aa, 0)
             val[sel] = v
             ashape = tuple(a.size for a in spec.actions)
             aidx = np.unravel_index(aa, ashape) if spec.actions else ()

@@ -305,6 +305,7 @@ class TargetPlan:
     w_sizes: int = -1
     w_coord: int = -1
     w_scalar: int = -1
+    w_vraw: int = -1
     unreachable: bool = False  # no law for one of the target's states
 
     @property
@@ -436,6 +437,9 @@ class RegimeKernels:
                 t.w_ev32 = take()
                 t.w_sizes = take(len(t.spec.states))
                 t.w_coord = take(3 * len(t.cont_pos))
+                # the target's value array itself (node-by-node reads in the
+                # simulation, for process values outside the process grid)
+                t.w_vraw = take()
         self.n_words = max(w, 1)
 
     # -------------------------------------------------------------- source
@@ -459,6 +463,73 @@ class RegimeKernels:
         return f"lcm_expect_{self.tag}_{t.spec.name}"
 
     # ..................................................................
+    def _sim_extrapolated_expectation(self, ti, t, T, E, blend, proc_names, dn, mk) -> list[str]:
+        """Simulation, process value outside its grid: the transition row is
+        the extrapolation of the two bracketing rows (a weight may be
+        negative), and blending the two contracted rows is then not the
+        reference's expectation wherever a node's value is infinite.  Redo it
+        node by node as the reference does (``processing.py:2780-2839``,
+        ``Q_and_F.py:1145-1209``): per combination of the target's stochastic
+        states, the interpolated value times the product of the node weights
+        (a zero weight ignoring a non-finite value), over the sum of the
+        weights."""
+        spec = self.spec
+        tg = t.spec
+        L = [f"if (!(PT[{blend}] >= 0.0 && PT[{blend}] <= 1.0)) {{"]
+        L.append(f"  {T} num = ({T})0, den = ({T})0;")
+        cblk = "1"
+        for pos in t.cont_pos:
+            cblk = f"{cblk} * C.n{ti}_{pos}"
+        # nested loops over the stochastic axes
+        depth = 0
+        for pos in t.stoch_pos:
+            ax = tg.states[pos]
+            L.append("  " * (depth + 1) + f"for (int j{pos} = 0; j{pos} < {ax.size}; ++j{pos}) {{")
+            depth += 1
+        ind = "  " * (depth + 1)
+        wexpr = f"({T})1"
+        for pos in t.stoch_pos:
+            ax = tg.states[pos]
+            law = t.laws[ax.name]
+            if law.kind == "process":
+                off, shape = self.param_off[proc_P_name(law.source_process)]
+                pi = proc_names.index(law.source_process)
+                L.append(ind + f"const {T} w{pos} = lcm_zs(({T})1 - ({T})PT[{pi}], ({T})PV[{off} + PLO[{pi}] * {shape[1]} + j{pos}])"
+                         f" + lcm_zs(({T})PT[{pi}], ({T})PV[{off} + (PLO[{pi}] + 1) * {shape[1]} + j{pos}]);")
+            else:
+                items = mk[(ti, pos)]
+                L.append(ind + f"{T} w{pos} = ({T})0;")
+                for q, v in enumerate(items):
+                    L.append(ind + f"if (j{pos} == {q}) w{pos} = ({T})({v});")
+            wexpr = f"{wexpr} * w{pos}" if wexpr != f"({T})1" else f"w{pos}"
+        L.append(ind + f"const {T} w = {wexpr};")
+        # flat index of the node row (non-continuous axes in declaration order)
+        flat = "(i64)0"
+        for pos, ax in enumerate(tg.states):
+            if ax.kind == "continuous":
+                continue
+            if pos in t.stoch_pos:
+                flat = f"({flat}) * {ax.size} + j{pos}"
+            else:
+                sz = f"C.n{ti}_{pos}"
+                flat = f"({flat}) * {sz} + min(max((int)({dn[(ti, pos)]}), 0), {sz} - 1)"
+        L.append(ind + f"const double* vrow = C.vr{ti} + ({flat}) * ({cblk});")
+        if len(t.cont_pos) == 0:
+            L.append(ind + f"const {T} v = ({T})vrow[0];")
+        elif len(t.cont_pos) == 1:
+            L.append(ind + f"const {T} v = lcm_interp1<{T}, double>(vrow, C.n{ti}_{t.cont_pos[0]}, c0);")
+        else:
+            L.append(ind + f"const {T} v = lcm_interp2<{T}, double>(vrow, C.n{ti}_{t.cont_pos[0]}, "
+                           f"C.n{ti}_{t.cont_pos[1]}, c0, c1);")
+        L.append(ind + "den = den + w;")
+        L.append(ind + "num = num + ((w == 0 && !lcm_isfinite(v)) ? w * 0 : w * v);")
+        for _ in t.stoch_pos:
+            depth -= 1
+            L.append("  " * (depth + 1) + "}")
+        L.append(f"  ev = num / (den > 0 ? den : ({T})1);")
+        L.append("}")
+        return L
+
     def _affine_laws(self) -> dict:
         """Continuous next-state laws that are affine in the one continuous
         action they read: {(target, state position): (law at action 0,
@@ -607,6 +678,8 @@ class RegimeKernels:
                 continue
             ap(f"  const E* ev{ti};")
             loads.append(f"ev{ti} = lcm_evsel<E>::get(it, {t.w_ev64}, {t.w_ev32});")
+            ap(f"  const double* vr{ti};")
+            loads.append(f"vr{ti} = lcm_wp<const double>(it, {t.w_vraw});")
             for pos in t.det_pos + t.cont_pos:
                 ap(f"  int n{ti}_{pos};")
                 loads.append(f"n{ti}_{pos} = lcm_wi(it, {t.w_sizes + pos});")
@@ -682,6 +755,7 @@ class RegimeKernels:
             sel = [(ti, t) for ti, t in enumerate(self.targets) if tsel < 0 or ti == tsel]
             pnames, dn, xn, affine_names = {}, {}, {}, {}
             rid_name = e.emit(self.tr.regime_id) if (det and tsel < 0) else None
+            mk = {}
             for ti, t in sel:
                 if not det:
                     pnames[ti] = e.emit(t.prob)
@@ -689,6 +763,11 @@ class RegimeKernels:
                     continue
                 for pos in t.det_pos:
                     dn[(ti, pos)] = e.emit(t.laws[t.spec.states[pos].name].expr)
+                if sim and any(kind == "state" and name in proc_names for kind, name, _ in t.key_vars):
+                    for pos in t.stoch_pos:
+                        law = t.laws[t.spec.states[pos].name]
+                        if law.kind == "markov":
+                            mk[(ti, pos)] = [e.emit(x) for x in law.expr.items]
                 for pos in t.cont_pos:
                     if not sim and (ti, pos) in self._affine:
                         x0, g, cv = self._affine[(ti, pos)]
@@ -775,6 +854,7 @@ class RegimeKernels:
                         # off-grid process value: blend the two bracketing node rows
                         # (the reference interpolates the transition-matrix rows)
                         inner.append(f"ev = lcm_zs(({T})1 - ({T})PT[{blend}], ev) + lcm_zs(({T})PT[{blend}], evh);")
+                        inner += self._sim_extrapolated_expectation(ti, t, T, E, blend, proc_names, dn, mk)
                     out += ["    " + s for s in inner]
                 if det:
                     out.append("    ce = ev;")
@@ -1295,17 +1375,26 @@ class RegimeKernels:
         ap("    if (lane != 0) continue;")
         if taste:
             ap(f"    const double scale = lcm_wd(it, {self.W_TASTE});")
-            ap("    int dstar = -1; double bn = -lcm_lim<double>::inf(); double vstar = -lcm_lim<double>::inf();")
+            # the reference (max_Q_over_a.py:268-297): per discrete cell the
+            # first argmax of the masked Q row (a NaN first, an all -inf row
+            # its first action), then the first argmax of max + noise over
+            # the cells (a NaN cell first)
+            ap("    int dstar = -1, dnan = -1; double bn = -lcm_lim<double>::inf(); double vstar = -lcm_lim<double>::inf();")
             ap(f"    for (int d = 0; d < {ND}; ++d) {{")
-            ap("      if (bd[d].idx < 0) continue;")
-            ap("      const double noisy = bd[d].v + scale * (rng.gumbel(64u + (u32)d) - 0.5772156649015329);")
-            ap("      if (dstar < 0 || noisy > bn) { bn = noisy; dstar = d; vstar = bd[d].v; }")
+            ap("      const double qc = bd[d].nan ? lcm_lim<double>::nan() : (bd[d].idx < 0 ? -lcm_lim<double>::inf() : bd[d].v);")
+            ap("      const double noisy = qc + scale * (rng.gumbel(64u + (u32)d) - 0.5772156649015329);")
+            ap("      if (dnan < 0 && noisy != noisy) dnan = d;")
+            ap("      if (dstar < 0 || noisy > bn) { bn = noisy; dstar = d; vstar = qc; }")
             ap("    }")
+            ap("    if (dnan >= 0) { dstar = dnan; vstar = lcm_lim<double>::nan(); }")
             ap("    int aa = 0;")
-            ap(f"    for (int d = 0; d < {ND}; ++d) if (d == dstar) aa = bd[d].idx;")
-            ap("    const double value = dstar < 0 ? -lcm_lim<double>::inf() : vstar;")
+            ap(f"    for (int d = 0; d < {ND}; ++d) if (d == dstar) "
+               "aa = bd[d].nan ? bd[d].nan - 1 : ((bd[d].idx < 0 || !(bd[d].v > -lcm_lim<double>::inf())) ? d * n_ac : bd[d].idx);")
+            ap("    const double value = vstar;")
         else:
-            ap("    const int aa = best.idx < 0 ? 0 : best.idx;")
+            # argmax_and_max (argmax.py:55-69): a NaN maximum matches no
+            # entry, so the first action
+            ap("    const int aa = (best.nan || best.idx < 0) ? 0 : best.idx;")
             ap("    const double value = best.nan ? lcm_lim<double>::nan() : (best.idx < 0 ? -lcm_lim<double>::inf() : best.v);")
         ap(f"    lcm_wp<double>(it, {self.SW_VAL})[s] = value;")
         ap(f"    lcm_wp<int>(it, {self.SW_AIDX})[s] = aa;")

@@ -148,16 +148,16 @@ __device__ __forceinline__ T lcm_interp2(const S* __restrict__ blk, int n0, int 
 template <typename T> struct LcmBest {
   T v;
   int idx;   // -1: no feasible action seen yet
-  int nan;   // a feasible action produced NaN
+  int nan;   // 0, or 1 + the smallest index of a feasible action whose Q is NaN
   __device__ __forceinline__ void init() { v = -lcm_lim<T>::inf(); idx = -1; nan = 0; }
   __device__ __forceinline__ void push(T q, int a) {
-    if (q != q) { nan = 1; return; }
+    if (q != q) { if (!nan) nan = a + 1; return; }
     if (idx < 0 || q > v) { v = q; idx = a; }
   }
   // merge with another partial result over a disjoint action set; ties go to
   // the smaller flat index, so the result equals the sequential first argmax.
   __device__ __forceinline__ void merge(T ov, int oidx, int onan) {
-    nan |= onan;
+    nan = (nan == 0) ? onan : ((onan == 0 || nan < onan) ? nan : onan);
     if (oidx < 0) return;
     if (idx < 0 || ov > v || (ov == v && oidx < idx)) { v = ov; idx = oidx; }
   }

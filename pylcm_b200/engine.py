@@ -503,6 +503,9 @@ class SolvePlan:
                     r[t.w_ev32] = 0
                     if i == 0:
                         out["tv"].append((t.w_ev64, t.spec.name))
+                r[t.w_vraw] = tV[i, tslot].data_ptr()
+                if i == 0:
+                    out["tv"].append((t.w_vraw, t.spec.name))
                 for k, ax in enumerate(t.spec.states):
                     r[t.w_sizes + k] = ax.size
                 for ci, pos in enumerate(t.cont_pos):
