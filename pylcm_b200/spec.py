@@ -198,11 +198,6 @@ def _is_leaf(v: Any) -> bool:
     return not isinstance(v, Mapping)
 
 
-# process object id -> (process, fixed parameters, runtime parameter names);
-# the entry keeps the process alive so that its id stays its own
-_PROC_FIELDS: dict[int, tuple] = {}
-
-
 class ParamResolver:
     """Looks up a function argument's value in user params / fixed params."""
 
@@ -237,11 +232,14 @@ class ParamResolver:
         return dict(out)
 
     def _process_params(self, regime: str, state: str, proc: _Process) -> dict:
-        ent = _PROC_FIELDS.get(id(proc))
-        if ent is None or ent[0] is not proc:
-            ent = _PROC_FIELDS[id(proc)] = (proc, dict(proc.fixed_params), tuple(proc.runtime_param_names))
-        out = dict(ent[1])
-        for name in ent[2]:
+        # the process's fixed parameters and runtime parameter names, kept on
+        # the (frozen) process object itself
+        ent = proc.__dict__.get("_lcm_param_fields")
+        if ent is None:
+            ent = (dict(proc.fixed_params), tuple(proc.runtime_param_names))
+            object.__setattr__(proc, "_lcm_param_fields", ent)
+        out = dict(ent[0])
+        for name in ent[1]:
             found = False
             for src in self.sources:
                 for holder in (src.get(regime), src):
