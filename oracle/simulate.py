@@ -190,6 +190,14 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
                             x = float(pp["mu"]) + float(pp["sigma"]) * rng.normal(1 + k)
                         elif cls == "LogNormalIIDProcess":
                             x = np.exp(float(pp["mu"]) + float(pp["sigma"]) * rng.normal(1 + k))
+                        elif cls in ("TauchenNormalMixtureAR1Process", "NormalMixtureIIDProcess"):
+                            # mixture innovation (``ar1.py:306-320``, ``iid.py:290-300``):
+                            # component 1 with probability p1, then its normal
+                            c1 = rng.uniform(128 + k) < float(pp["p1"])
+                            z = rng.normal(1 + k)
+                            eps = np.where(c1, float(pp["mu1"]) + float(pp["sigma1"]) * z,
+                                           float(pp["mu2"]) + float(pp["sigma2"]) * z)
+                            x = eps if cls == "NormalMixtureIIDProcess" else float(pp["mu"]) + float(pp["rho"]) * y + eps
                         else:
                             x = float(pp["start"]) + (float(pp["stop"]) - float(pp["start"])) * rng.uniform(1 + k)
                     newS[ax.name][sel[m]] = np.asarray(x)[m]

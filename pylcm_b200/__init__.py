@@ -32,8 +32,10 @@ from pylcm_b200.model import Model
 from pylcm_b200.processes import (
     LogNormalIIDProcess,
     NormalIIDProcess,
+    NormalMixtureIIDProcess,
     RouwenhorstAR1Process,
     TauchenAR1Process,
+    TauchenNormalMixtureAR1Process,
     UniformIIDProcess,
 )
 from pylcm_b200.regime import (
@@ -68,11 +70,13 @@ __all__ = [
     "Model",
     "ModelInitializationError",
     "NormalIIDProcess",
+    "NormalMixtureIIDProcess",
     "PyLCMError",
     "Regime",
     "RegimeInitializationError",
     "RouwenhorstAR1Process",
     "TauchenAR1Process",
+    "TauchenNormalMixtureAR1Process",
     "TracingError",
     "UniformIIDProcess",
     "categorical",

@@ -1243,7 +1243,8 @@ class RegimeKernels:
         precision), the first lane records value and action and draws the next
         regime and next states with the Philox stream of (seed, subject,
         period, stream id).  Stream ids: 0 regime draw, 1 + k the k-th state of
-        the drawn target, 64 + d the taste shock of discrete choice d.
+        the drawn target, 64 + d the taste shock of discrete choice d, 128 + k
+        the mixture component of the k-th state (normal-mixture processes).
         """
         from pylcm_b200.spec import proc_field_name, proc_grid_name
 
@@ -1474,6 +1475,12 @@ class RegimeKernels:
                             ap(f"      {dst} = exp({fld('mu')} + {fld('sigma')} * rng.normal({stream}));")
                         elif cls == "UniformIIDProcess":
                             ap(f"      {dst} = {fld('start')} + ({fld('stop')} - {fld('start')}) * rng.uniform({stream});")
+                        elif cls in ("TauchenNormalMixtureAR1Process", "NormalMixtureIIDProcess"):
+                            # component 1 with probability p1 (its own stream), then its normal
+                            ar = f"{fld('mu')} + {fld('rho')} * pv_{src} + " if cls.startswith("Tauchen") else ""
+                            ap(f"      {{ const bool c1 = rng.uniform({128 + k}u) < {fld('p1')};")
+                            ap(f"        const double z = rng.normal({stream});")
+                            ap(f"        {dst} = {ar}(c1 ? {fld('mu1')} + {fld('sigma1')} * z : {fld('mu2')} + {fld('sigma2')} * z); }}")
                         else:
                             raise TracingError(f"no simulation draw for process {cls}")
                 ap("    }")

@@ -248,5 +248,99 @@ class LogNormalIIDProcess(_Process):
         return _equal_spaced_normal_probs(mu, sigma, float(kw["n_std"]), n)
 
 
+def _mixture_cdf(x, p1: float, mu1: float, sigma1: float, mu2: float, sigma2: float) -> np.ndarray:
+    """CDF of the two-component normal mixture p1 N(mu1, sigma1^2) + (1 - p1) N(mu2, sigma2^2)."""
+    return p1 * ndtr((x - mu1) / sigma1) + (1.0 - p1) * ndtr((x - mu2) / sigma2)
+
+
+def _mixture_moments(p1: float, mu1: float, sigma1: float, mu2: float, sigma2: float) -> tuple[float, float]:
+    """Mean and variance of the two-component normal mixture."""
+    mean = p1 * mu1 + (1.0 - p1) * mu2
+    var = p1 * (sigma1**2 + mu1**2) + (1.0 - p1) * (sigma2**2 + mu2**2) - mean**2
+    return mean, var
+
+
+_MIX_FIELDS = ("p1", "mu1", "sigma1", "mu2", "sigma2")
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
+class TauchenNormalMixtureAR1Process(_Process):
+    """AR(1) y' = mu + rho y + eps with eps a two-component normal mixture,
+    discretised by Tauchen's binning with the mixture CDF (Fella, Gallipoli &
+    Pan 2019, eq. 21; ``ar1.py:206-320``): equally spaced nodes around the
+    long-run mean (mu + E[eps]) / (1 - rho), n_std unconditional standard
+    deviations wide; row i bins the innovation x_j - mu - rho x_i over
+    half-steps, the outer bins open-ended."""
+
+    rho: float | None = None
+    mu: float | None = None
+    n_std: float | None = None
+    p1: float | None = None
+    mu1: float | None = None
+    sigma1: float | None = None
+    mu2: float | None = None
+    sigma2: float | None = None
+    is_ar1: ClassVar[bool] = True
+
+    def _nodes(self, kw) -> tuple[np.ndarray, float]:
+        rho, mu, n_std = float(kw["rho"]), float(kw["mu"]), float(kw["n_std"])
+        mean, var = _mixture_moments(*(float(kw[f]) for f in _MIX_FIELDS))
+        std_y = np.sqrt(var / (1 - rho**2))
+        lrm = (mu + mean) / (1 - rho)
+        x_max = n_std * std_y
+        x = np.linspace(lrm - x_max, lrm + x_max, self.n_points)
+        return x, (2 * x_max) / (self.n_points - 1)
+
+    def compute_gridpoints(self, **kw) -> np.ndarray:
+        return self._nodes(kw)[0]
+
+    def compute_transition_probs(self, **kw) -> np.ndarray:
+        x, step = self._nodes(kw)
+        rho, mu = float(kw["rho"]), float(kw["mu"])
+        mix = [float(kw[f]) for f in _MIX_FIELDS]
+        z = x[None, :] - mu - rho * x[:, None]
+        upper = _mixture_cdf(z + 0.5 * step, *mix)
+        lower = _mixture_cdf(z - 0.5 * step, *mix)
+        P = upper - lower
+        P[:, 0] = upper[:, 0]
+        P[:, -1] = 1 - lower[:, -1]
+        return P
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
+class NormalMixtureIIDProcess(_Process):
+    """IID draws from a two-component normal mixture (``iid.py:211-300``):
+    equally spaced nodes n_std mixture standard deviations around the mixture
+    mean, bin probabilities from the mixture CDF over half-steps (the outer
+    bins open-ended), the same row for every current node."""
+
+    n_std: float | None = None
+    p1: float | None = None
+    mu1: float | None = None
+    sigma1: float | None = None
+    mu2: float | None = None
+    sigma2: float | None = None
+
+    def _nodes(self, kw) -> tuple[np.ndarray, float]:
+        n_std = float(kw["n_std"])
+        mean, var = _mixture_moments(*(float(kw[f]) for f in _MIX_FIELDS))
+        std = np.sqrt(var)
+        x = np.linspace(mean - n_std * std, mean + n_std * std, self.n_points)
+        return x, (2 * n_std * std) / (self.n_points - 1)
+
+    def compute_gridpoints(self, **kw) -> np.ndarray:
+        return self._nodes(kw)[0]
+
+    def compute_transition_probs(self, **kw) -> np.ndarray:
+        x, step = self._nodes(kw)
+        mix = [float(kw[f]) for f in _MIX_FIELDS]
+        upper = _mixture_cdf(x + 0.5 * step, *mix)
+        lower = _mixture_cdf(x - 0.5 * step, *mix)
+        w = upper - lower
+        w[0] = upper[0]
+        w[-1] = 1 - lower[-1]
+        return np.broadcast_to(w, (self.n_points, self.n_points)).copy()
+
+
 def is_process(grid: object) -> bool:
     return isinstance(grid, _Process)

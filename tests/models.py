@@ -782,3 +782,50 @@ def egm_process_params(taste_scale=None, rho=0.9):
     if taste_scale is not None:
         p["working"] = {"taste_shocks": {"scale": taste_scale}}
     return p
+
+
+# --------------------------------------------------------------------------
+# normal-mixture processes: an AR(1) income with mixture innovations, or an
+# IID mixture income, as the process state of a grid-search regime
+# --------------------------------------------------------------------------
+MIX_N_PERIODS = 5
+
+
+def _mix_u(consumption, rho):
+    return (consumption ** (1.0 - rho) - 1.0) / (1.0 - rho)
+
+
+def _mix_next_wealth(wealth, consumption, income, interest_rate):
+    return (1.0 + interest_rate) * (wealth - consumption) + jnp.exp(income)
+
+
+def _mix_budget(consumption, wealth):
+    return consumption <= wealth
+
+
+def _mix_nr(age):
+    return jnp.where(age >= MIX_N_PERIODS - 2, AliveDeadId.dead, AliveDeadId.alive)
+
+
+def mixture_model(kind="ar1", n_wealth=40, n_cons=60):
+    from pylcm_b200 import NormalMixtureIIDProcess, TauchenNormalMixtureAR1Process
+
+    proc = TauchenNormalMixtureAR1Process(n_points=5) if kind == "ar1" else NormalMixtureIIDProcess(n_points=4)
+    alive = Regime(
+        active=lambda age: age <= MIX_N_PERIODS - 2,
+        states={"wealth": LinSpacedGrid(start=0.5, stop=20.0, n_points=n_wealth), "income": proc},
+        state_transitions={"wealth": _mix_next_wealth},
+        actions={"consumption": LinSpacedGrid(start=0.1, stop=20.0, n_points=n_cons)},
+        transition=_mix_nr, constraints={"budget": _mix_budget}, functions={"utility": _mix_u},
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(regimes={"alive": alive, "dead": dead}, regime_id_class=AliveDeadId,
+                 ages=AgeGrid(start=0, stop=MIX_N_PERIODS - 1, step="Y"))
+
+
+def mixture_params(kind="ar1", p1=0.8):
+    if kind == "ar1":
+        inc = {"rho": 0.8, "mu": 0.0, "n_std": 2.5, "p1": p1, "mu1": 0.05, "sigma1": 0.1, "mu2": -0.2, "sigma2": 0.3}
+    else:
+        inc = {"n_std": 2.0, "p1": p1, "mu1": -0.3, "sigma1": 0.1, "mu2": 0.3, "sigma2": 0.2}
+    return {"discount_factor": 0.95, "rho": 2.0, "interest_rate": 0.03, "income": inc}
