@@ -468,6 +468,7 @@ class RegimeKernels:
         the extrapolation of the two bracketing rows (a weight may be
         negative), and blending the two contracted rows is then not the
         reference's expectation wherever a node's value is infinite.  Redo it
+        (and, for a target reached with several process laws, always do it)
         node by node as the reference does (``processing.py:2780-2839``,
         ``Q_and_F.py:1145-1209``): per combination of the target's stochastic
         states, the interpolated value times the product of the node weights
@@ -475,7 +476,8 @@ class RegimeKernels:
         weights."""
         spec = self.spec
         tg = t.spec
-        L = [f"if (!(PT[{blend}] >= 0.0 && PT[{blend}] <= 1.0)) {{"]
+        # blend None: always (targets reached with several process laws)
+        L = ["{"] if blend is None else [f"if (!(PT[{blend}] >= 0.0 && PT[{blend}] <= 1.0)) {{"]
         L.append(f"  {T} num = ({T})0, den = ({T})0;")
         cblk = "1"
         for pos in t.cont_pos:
@@ -797,10 +799,14 @@ class RegimeKernels:
                     inner: list[str] = []
                     key = "0"
                     key_hi = None
+                    # two or more process laws: the simulation takes the
+                    # node-by-node expectation (each process row interpolated
+                    # at its own value), not a blend of contracted rows
+                    multi = sim and sum(1 for kd, nm, _ in t.key_vars if kd == "state" and nm in proc_names) > 1
                     for kind, name, size in t.key_vars:
                         if sim and kind == "state" and name in proc_names:
-                            if key_hi is not None:
-                                raise TracingError("simulation supports one process key per target")
+                            if multi:
+                                continue
                             pi = proc_names.index(name)
                             key_hi = f"({key}) * {size} + PLO[{pi}] + 1"
                             key = f"({key}) * {size} + PLO[{pi}]"
@@ -836,7 +842,10 @@ class RegimeKernels:
                         else:
                             cc = f"lcm_coord_irreg<{T}>(({T})({x}), C.p{ti}_{ci}, C.n{ti}_{pos})"
                         inner.append(f"{T} c{ci} = {cc};")
-                    rows = [("row", off)] + ([("rowh", off_hi)] if off_hi is not None else [])
+                    rows = [] if multi else [("row", off)] + ([("rowh", off_hi)] if off_hi is not None else [])
+                    if multi:
+                        inner.append(f"{T} ev = ({T})0;")
+                        inner += self._sim_extrapolated_expectation(ti, t, T, E, None, proc_names, dn, mk)
                     for rname, roff in rows:
                         ev_name = "ev" if rname == "row" else "evh"
                         inner.append(f"const {E}* {rname} = C.ev{ti} + (i64)({roff}) * ({cblk});")

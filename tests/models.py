@@ -807,14 +807,23 @@ def _mix_nr(age):
     return jnp.where(age >= MIX_N_PERIODS - 2, AliveDeadId.dead, AliveDeadId.alive)
 
 
+def _mix_next_wealth_two(wealth, consumption, income, shock, interest_rate):
+    return (1.0 + interest_rate) * (wealth - consumption) + jnp.exp(income) + 0.1 * shock
+
+
 def mixture_model(kind="ar1", n_wealth=40, n_cons=60):
+    """kind "ar1" / "iid": one mixture income process; "two": the AR(1)
+    mixture income and an IID normal shock (two process states)."""
     from pylcm_b200 import NormalMixtureIIDProcess, TauchenNormalMixtureAR1Process
 
-    proc = TauchenNormalMixtureAR1Process(n_points=5) if kind == "ar1" else NormalMixtureIIDProcess(n_points=4)
+    proc = NormalMixtureIIDProcess(n_points=4) if kind == "iid" else TauchenNormalMixtureAR1Process(n_points=5)
+    states = {"wealth": LinSpacedGrid(start=0.5, stop=20.0, n_points=n_wealth), "income": proc}
+    if kind == "two":
+        states["shock"] = NormalIIDProcess(n_points=3, gauss_hermite=False)
     alive = Regime(
         active=lambda age: age <= MIX_N_PERIODS - 2,
-        states={"wealth": LinSpacedGrid(start=0.5, stop=20.0, n_points=n_wealth), "income": proc},
-        state_transitions={"wealth": _mix_next_wealth},
+        states=states,
+        state_transitions={"wealth": _mix_next_wealth_two if kind == "two" else _mix_next_wealth},
         actions={"consumption": LinSpacedGrid(start=0.1, stop=20.0, n_points=n_cons)},
         transition=_mix_nr, constraints={"budget": _mix_budget}, functions={"utility": _mix_u},
     )
@@ -824,8 +833,11 @@ def mixture_model(kind="ar1", n_wealth=40, n_cons=60):
 
 
 def mixture_params(kind="ar1", p1=0.8):
-    if kind == "ar1":
-        inc = {"rho": 0.8, "mu": 0.0, "n_std": 2.5, "p1": p1, "mu1": 0.05, "sigma1": 0.1, "mu2": -0.2, "sigma2": 0.3}
-    else:
+    if kind == "iid":
         inc = {"n_std": 2.0, "p1": p1, "mu1": -0.3, "sigma1": 0.1, "mu2": 0.3, "sigma2": 0.2}
-    return {"discount_factor": 0.95, "rho": 2.0, "interest_rate": 0.03, "income": inc}
+    else:
+        inc = {"rho": 0.8, "mu": 0.0, "n_std": 2.5, "p1": p1, "mu1": 0.05, "sigma1": 0.1, "mu2": -0.2, "sigma2": 0.3}
+    out = {"discount_factor": 0.95, "rho": 2.0, "interest_rate": 0.03, "income": inc}
+    if kind == "two":
+        out["shock"] = {"mu": 0.0, "sigma": 1.0, "n_std": 2.0}
+    return out

@@ -55,13 +55,16 @@ def test_iid_mixture_tables():
     np.testing.assert_allclose(P[0], w, rtol=1e-12)
 
 
-def _ic(n):
+def _ic(n, kind="ar1"):
     rng = np.random.default_rng(2)
-    return {"wealth": rng.uniform(1, 15, n), "income": rng.normal(0, 0.3, n), "age": np.zeros(n),
-            "regime_id": np.zeros(n, dtype=int)}
+    ic = {"wealth": rng.uniform(1, 15, n), "income": rng.normal(0, 0.3, n), "age": np.zeros(n),
+          "regime_id": np.zeros(n, dtype=int)}
+    if kind == "two":
+        ic["shock"] = rng.normal(0, 1.5, n)
+    return ic
 
 
-@pytest.mark.parametrize("kind", ["ar1", "iid"])
+@pytest.mark.parametrize("kind", ["ar1", "iid", "two"])
 def test_oracle_solves_and_simulates_a_mixture_model(kind):
     from oracle.grid_search import solve
     from oracle.simulate import simulate
@@ -69,13 +72,13 @@ def test_oracle_solves_and_simulates_a_mixture_model(kind):
     model = M.mixture_model(kind)
     V, _ = solve(model, M.mixture_params(kind))
     assert all(np.isfinite(np.asarray(v)).all() for d in V.values() for v in d.values())
-    out = simulate(model, M.mixture_params(kind), _ic(40), seed=5)
+    out = simulate(model, M.mixture_params(kind), _ic(40, kind), seed=5)
     inc = np.concatenate([out[p]["states"]["income"] for p in range(1, M.MIX_N_PERIODS - 1)])
     assert np.isfinite(inc).all() and inc.std() > 0
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["ar1", "iid"])
+@pytest.mark.parametrize("kind", ["ar1", "iid", "two"])
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_gpu_mixture_model_solve_matches_oracle(precision, kind):
     from oracle.grid_search import solve
@@ -90,18 +93,20 @@ def test_gpu_mixture_model_solve_matches_oracle(precision, kind):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kind", ["ar1", "iid"])
+@pytest.mark.parametrize("kind", ["ar1", "iid", "two"])
 def test_gpu_mixture_model_simulation_matches_oracle(kind):
+    """"two": a target reached with two process laws, whose simulated
+    expectation is taken node by node."""
     from oracle.simulate import simulate
 
     model = M.mixture_model(kind)
     params = M.mixture_params(kind)
-    ic = _ic(64)
+    ic = _ic(64, kind)
     res = model.simulate(params=params, initial_conditions=ic, seed=5)
     ora = simulate(model, params, ic, seed=5)
     for p in ora:
         np.testing.assert_array_equal(res.periods[p]["regime_id"], ora[p]["regime_id"])
-        for name in ("wealth", "income"):
+        for name in ("wealth", "income") + (("shock",) if kind == "two" else ()):
             np.testing.assert_allclose(res.periods[p]["states"][name], ora[p]["states"][name], rtol=1e-9, atol=1e-9,
                                        equal_nan=True)
         np.testing.assert_allclose(res.periods[p]["value"], ora[p]["value"], rtol=1e-9, atol=1e-9, equal_nan=True)
