@@ -62,6 +62,30 @@ def grid_coordinate(grid, values: np.ndarray) -> np.ndarray:
             lower = np.exp(a + sl * lo)
             upper = np.exp(a + sl * (lo + 1))
             return lo + (v - lower) / (upper - lower)
+    if kind == "piece":
+        # ``piecewise.py:107-118, 178-188``: the segment by searchsorted(side="right")
+        # over the effective starts of segments 1..k-1, plus its offset
+        bnds = [seg.effective_bounds() for seg in grid.segments]
+        ns = np.array([int(seg.n_points) for seg in grid.segments])
+        offs = np.concatenate([[0], np.cumsum(ns[:-1])])
+        seg_i = np.searchsorted(np.array([a for a, _ in bnds[1:]]), v, side="right")
+        out = np.empty_like(v)
+        for k, ((a, b), n) in enumerate(zip(bnds, ns)):
+            m = seg_i == k
+            if not m.any():
+                continue
+            if grid.log:
+                a_l, b_l = np.log(a), np.log(b)
+                sl = (b_l - a_l) / (n - 1)
+                with np.errstate(all="ignore"):
+                    c = (np.log(v[m]) - a_l) / sl
+                    lo = np.floor(c)
+                    lower = np.exp(a_l + sl * lo)
+                    upper = np.exp(a_l + sl * (lo + 1))
+                    out[m] = offs[k] + lo + (v[m] - lower) / (upper - lower)
+            else:
+                out[m] = offs[k] + (v[m] - a) / ((b - a) / (n - 1))
+        return out
     if kind == "irreg":
         pts = grid.to_numpy()
         n = len(pts)
@@ -99,7 +123,7 @@ def interp_rows(rows: np.ndarray, coords: list[np.ndarray]) -> np.ndarray:
     shape = rows.shape[-d:]
     data = []
     for c, n in zip(coords, shape):
-        lo = np.clip(np.floor(c), 0, n - 2).astype(np.int64)
+        lo = np.clip(np.nan_to_num(np.floor(c), nan=0.0), 0, n - 2).astype(np.int64)  # NaN: any index, NaN weight
         wu = c - lo
         wl = 1 - wu
         data.append(((lo, wl), (lo + 1, wu)))
@@ -485,7 +509,7 @@ def _expected_next_value(spec, tgt, resolver, ev, V_next, procs, sidx_of, aidx_o
     cdata = []
     for p, c in zip(cont_pos, coords):
         n = shape[p]
-        lo = np.clip(np.floor(c), 0, n - 2).astype(np.int64)
+        lo = np.clip(np.nan_to_num(np.floor(c), nan=0.0), 0, n - 2).astype(np.int64)  # NaN: any index, NaN weight
         wu = c - lo
         cdata.append(((lo, 1 - wu), (lo + 1, wu)))
     node_ranges = [range(len(ws)) for _, ws in stoch_axes]

@@ -26,6 +26,9 @@ from pylcm_b200.grids import (
     IrregSpacedGrid,
     LinSpacedGrid,
     LogSpacedGrid,
+    PiecewiseGridSegment,
+    PiecewiseLinSpacedGrid,
+    PiecewiseLogSpacedGrid,
     categorical,
 )
 from pylcm_b200.model import Model
@@ -66,6 +69,9 @@ __all__ = [
     "LiquidMargin",
     "LogNormalIIDProcess",
     "LogSpacedGrid",
+    "PiecewiseGridSegment",
+    "PiecewiseLinSpacedGrid",
+    "PiecewiseLogSpacedGrid",
     "MarkovTransition",
     "Model",
     "ModelInitializationError",

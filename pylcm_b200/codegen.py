@@ -549,6 +549,8 @@ class RegimeKernels:
             if t.scalar:
                 continue
             for pos in t.cont_pos:
+                if t.spec.states[pos].grid.kind != "lin":
+                    continue  # the coordinate is affine in the law only on a linear grid
                 x = ir.const(t.laws[t.spec.states[pos].name].expr)
                 if not isinstance(x, ir.Expr):
                     continue
@@ -690,6 +692,10 @@ class RegimeKernels:
                 if t.spec.states[pos].grid.kind == "irreg":
                     ap(f"  const double* p{ti}_{ci};")
                     loads.append(f"p{ti}_{ci} = lcm_wp<const double>(it, {w0 + 2});")
+                elif t.spec.states[pos].grid.kind == "piece":
+                    ap(f"  const double* p{ti}_{ci}; int k{ti}_{ci}, g{ti}_{ci};")
+                    loads.append(f"p{ti}_{ci} = lcm_wp<const double>(it, {w0 + 2}); "
+                                 f"k{ti}_{ci} = lcm_wi(it, {w0 + 1}); g{ti}_{ci} = lcm_wi(it, {w0});")
                 else:
                     ap(f"  T a{ti}_{ci}, b{ti}_{ci};")
                     loads.append(f"a{ti}_{ci} = (T)lcm_wd(it, {w0}); b{ti}_{ci} = (T)lcm_wd(it, {w0 + 1});")
@@ -839,6 +845,8 @@ class RegimeKernels:
                             cc = f"lcm_coord_lin<{T}>(({T})({x}), C.a{ti}_{ci}, C.b{ti}_{ci})"
                         elif kind == "log":
                             cc = f"lcm_coord_log<{T}>(({T})({x}), C.a{ti}_{ci}, C.b{ti}_{ci})"
+                        elif kind == "piece":
+                            cc = f"lcm_coord_piece<{T}>(({T})({x}), C.p{ti}_{ci}, C.k{ti}_{ci}, C.g{ti}_{ci})"
                         else:
                             cc = f"lcm_coord_irreg<{T}>(({T})({x}), C.p{ti}_{ci}, C.n{ti}_{pos})"
                         inner.append(f"{T} c{ci} = {cc};")

@@ -109,6 +109,22 @@ __device__ __forceinline__ T lcm_coord_irreg(T x, const double* __restrict__ pts
   return (T)low + (x - pl) / (pu - pl);
 }
 
+// Coordinate on a piecewise grid of k segments (piecewise.py:107-118,
+// 178-188): the segment is the count of breakpoints (effective starts of
+// segments 1..k-1) at or below x; inside it the linear or logarithmic
+// coordinate, plus the segment's offset.  tab = [breakpoints (k-1) | start
+// (k) | scale (k) | offset (k)], start/scale as lcm_coord_lin's or
+// lcm_coord_log's arguments.
+template <typename T>
+__device__ __forceinline__ T lcm_coord_piece(T x, const double* __restrict__ tab, int k, int is_log) {
+  int seg = 0;
+  for (int i = 0; i < k - 1; ++i) seg += ((double)x >= tab[i]) ? 1 : 0;
+  const double* st = tab + (k - 1);
+  const T local = is_log ? lcm_coord_log<T>(x, (T)st[seg], (T)st[k + seg])
+                         : lcm_coord_lin<T>(x, (T)st[seg], (T)st[k + seg]);
+  return (T)st[2 * k + seg] + local;
+}
+
 // 1-D linear read with extrapolation; `row` is contiguous.
 template <typename T, typename S>
 __device__ __forceinline__ T lcm_interp1(const S* __restrict__ row, int n, T c) {

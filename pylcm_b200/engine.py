@@ -518,6 +518,10 @@ class SolvePlan:
                     elif kind == "log":
                         r[base] = _f2w(a)
                         r[base + 1] = _f2w(bb)
+                    elif kind == "piece":
+                        r[base] = int(a)  # 1: log-spaced segments
+                        r[base + 1] = int(bb)  # segments
+                        r[base + 2] = self._coord_table(t.spec, pos).data_ptr()
                     else:
                         r[base + 2] = self.sgrid[t.spec.name][pos].data_ptr()
             recs.append(r)
@@ -526,6 +530,15 @@ class SolvePlan:
         out["tiles"] = [math.ceil(s.n_states / spt)] * n
         out["atab_tiles"] = [math.ceil(s.n_actions / 256)] * n
         return out
+
+    def _coord_table(self, spec: RegimeSpec, pos: int):
+        """Device copy of a piecewise grid's coordinate table (one per plan)."""
+        tabs = self.__dict__.setdefault("_ctabs", {})
+        key = (spec.name, pos)
+        if key not in tabs:
+            tab = spec.states[pos].grid.coordinate_table()
+            tabs[key] = self.torch.as_tensor(tab, dtype=self.torch.float64, device=self.dev)
+        return tabs[key]
 
     # ---- device addresses of slot-indexed buffers, per instance
     def _geom(self, key, t, slot_axis: int):

@@ -841,3 +841,66 @@ def mixture_params(kind="ar1", p1=0.8):
     if kind == "two":
         out["shock"] = {"mu": 0.0, "sigma": 1.0, "n_std": 2.0}
     return out
+
+
+# --------------------------------------------------------------------------
+# wealth grids of every continuous kind (irregular, log-spaced, piecewise
+# linear, piecewise log) with an affine next-wealth law that leaves the grid
+# at the top (extrapolation) and a Markov health state
+# --------------------------------------------------------------------------
+GK_N_PERIODS = 5
+
+
+def _gk_u(consumption, health):
+    return jnp.log(consumption) - 0.1 * (health == Health.bad)
+
+
+def _gk_next_wealth(wealth, consumption, health, interest_rate, income):
+    return (1.0 + interest_rate) * (wealth - consumption) + income * jnp.where(health == Health.good, 1.0, 0.5)
+
+
+def _gk_next_health(health):
+    p_good = jnp.where(health == Health.good, 0.9, 0.4)
+    return jnp.array([1.0 - p_good, p_good])
+
+
+def _gk_budget(consumption, wealth):
+    return consumption <= wealth
+
+
+def _gk_nr(age):
+    return jnp.where(age >= GK_N_PERIODS - 2, AliveDeadId.dead, AliveDeadId.alive)
+
+
+def grid_kinds_model(kind):
+    from pylcm_b200 import (
+        IrregSpacedGrid, LogSpacedGrid, PiecewiseGridSegment, PiecewiseLinSpacedGrid, PiecewiseLogSpacedGrid,
+    )
+
+    cons = LinSpacedGrid(start=0.5, stop=60.0, n_points=80)
+    if kind == "irreg":
+        wealth = IrregSpacedGrid(points=tuple(1.0 + 59.0 * (i / 39) ** 2 for i in range(40)))
+    elif kind == "log":
+        wealth = LogSpacedGrid(start=1.0, stop=60.0, n_points=40)
+    elif kind == "piece_lin":
+        wealth = PiecewiseLinSpacedGrid(segments=(PiecewiseGridSegment("[1, 10)", 20),
+                                                  PiecewiseGridSegment("[10, 60]", 20)))
+        cons = PiecewiseLinSpacedGrid(segments=(PiecewiseGridSegment("[0.5, 5]", 40),
+                                                PiecewiseGridSegment("(5, 60]", 40)))
+    else:
+        wealth = PiecewiseLogSpacedGrid(segments=(PiecewiseGridSegment("[1, 10]", 15),
+                                                  PiecewiseGridSegment("(10, 60]", 25)))
+    alive = Regime(
+        active=lambda age: age <= GK_N_PERIODS - 2,
+        states={"health": DiscreteGrid(Health), "wealth": wealth},
+        state_transitions={"wealth": _gk_next_wealth, "health": MarkovTransition(_gk_next_health)},
+        actions={"consumption": cons},
+        transition=_gk_nr, constraints={"budget": _gk_budget}, functions={"utility": _gk_u},
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(regimes={"alive": alive, "dead": dead}, regime_id_class=AliveDeadId,
+                 ages=AgeGrid(start=0, stop=GK_N_PERIODS - 1, step="Y"))
+
+
+def grid_kinds_params():
+    return {"discount_factor": 0.95, "interest_rate": 0.04, "income": 8.0}

@@ -38,6 +38,8 @@ CASES = {
     "retirement": (lambda: M.retirement_model(5), M.retirement_params),
     "stochastic": (lambda: M.stochastic_model(4, 20, 20), M.stochastic_params),
     "hc": (lambda: M.hc_model(3, 10, 4, 4, 8), lambda: M.hc_params(0, 4)),
+    **{f"grid_{k}": (lambda k=k: M.grid_kinds_model(k), M.grid_kinds_params)
+       for k in ("irreg", "log", "piece_lin", "piece_log")},
 }
 
 

@@ -50,3 +50,41 @@ def test_grid_coordinates():
     v = np.array([0.5, 1.0, 2.0, 7.0, 9.0, -1.0])
     np.testing.assert_allclose(grid_coordinate(irr, v), [0.5, 1.0, 1.5, 3.0, 3.5, -1.0], rtol=1e-15)
     np.testing.assert_allclose(np.interp(v[:4], irr.to_numpy(), np.arange(4.0)), grid_coordinate(irr, v[:4]))
+
+
+def test_piecewise_grid_coordinates():
+    """Inside a segment the coordinate is the segment's own (linear or
+    logarithmic) coordinate plus the segment's offset; beyond the last node
+    the last segment's spacing continues (``piecewise.py:107-118, 178-188``)."""
+    from pylcm_b200 import PiecewiseGridSegment as S
+    from pylcm_b200 import PiecewiseLinSpacedGrid, PiecewiseLogSpacedGrid
+
+    g = PiecewiseLinSpacedGrid(segments=(S("[1, 4)", 4), S("[4, 10]", 4)))
+    pts = g.to_numpy()
+    assert len(g) == 8 and pts[3] < 4.0 == pts[4]
+    v = np.array([1.0, 2.5, 4.0, 5.0, 10.0, 12.0, 0.0])
+    np.testing.assert_allclose(grid_coordinate(g, v), [0.0, 1.5, 4.0, 4.5, 7.0, 8.0, -1.0], rtol=1e-14, atol=1e-14)
+    h = PiecewiseLogSpacedGrid(segments=(S("[0.1, 10)", 3), S("[10, 1000]", 3)))
+    v = np.array([1.0, 10.0, 100.0, 1000.0])
+    np.testing.assert_allclose(grid_coordinate(h, v), [1.0, 3.0, 4.0, 5.0], rtol=1e-12, atol=1e-12)
+    # inside segments: the irregular-grid coordinate on the same points
+    from pylcm_b200 import IrregSpacedGrid
+
+    irr = IrregSpacedGrid(points=tuple(h.to_numpy()))
+    v = np.array([0.2, 0.5, 3.0, 20.0, 500.0])
+    np.testing.assert_allclose(grid_coordinate(h, v), grid_coordinate(irr, v), rtol=1e-12)
+
+
+def test_piecewise_grid_rejects_gaps_and_overlaps():
+    import pytest
+
+    from pylcm_b200 import PiecewiseGridSegment as S
+    from pylcm_b200 import PiecewiseLinSpacedGrid, PiecewiseLogSpacedGrid
+    from pylcm_b200.exceptions import GridInitializationError
+
+    for segs in ((S("[1, 4)", 4), S("[5, 10]", 4)), (S("[1, 4]", 4), S("[4, 10]", 4)), (S("[1, 4)", 1),),
+                 (S("1, 4", 3),)):
+        with pytest.raises(GridInitializationError):
+            PiecewiseLinSpacedGrid(segments=segs)
+    with pytest.raises(GridInitializationError):
+        PiecewiseLogSpacedGrid(segments=(S("[0, 4]", 3),))
