@@ -73,6 +73,20 @@ def main() -> None:
             if src.exists():
                 arr = np.genfromtxt(src, delimiter=",")
                 np.save(OUT / f"analytical_{kind}__{what}.npy", arr)
+    # the mortality example's stored float64 simulation (4 subjects from wealth
+    # 100 at age 40; its survival path is one draw of the reference's stream)
+    mort = pd.read_pickle(data / "regression_tests" / "f64" / "mortality_simulation.pkl")
+    np.savez(
+        OUT / "mortality_simulation.npz",
+        subject_id=mort["subject_id"].to_numpy(np.int64),
+        period=mort["period"].to_numpy(np.int64),
+        regime=mort["regime_name"].astype(str).to_numpy().astype("U"),
+        value=mort["value"].to_numpy(np.float64),
+        wealth=mort["wealth"].to_numpy(np.float64),
+        consumption=mort["consumption"].to_numpy(np.float64),
+        labor_supply=mort["labor_supply"].astype(str).to_numpy().astype("U"),
+        age=mort["age"].to_numpy(np.float64),
+    )
     # the independent `dcegm` package's solution of the IJRS retirement model
     # with taste shocks (the reference's cross-check fixture)
     df = pd.read_csv(data / "dcegm_reference" / "ijrs_taste_shocks_reference.csv")

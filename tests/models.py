@@ -904,3 +904,82 @@ def grid_kinds_model(kind):
 
 def grid_kinds_params():
     return {"discount_factor": 0.95, "interest_rate": 0.04, "income": 8.0}
+
+
+# --------------------------------------------------------------------------
+# mortality model (restating the reference's lcm_examples/mortality.py):
+# working life, retirement and death, 10-year periods from age 40,
+# survival probabilities indexed by period in Markov regime transitions
+# --------------------------------------------------------------------------
+@categorical(ordered=False)
+class MortalityRegimeId:
+    working_life: int
+    retirement: int
+    dead: int
+
+
+MORTALITY_LAST_AGE = 70
+
+
+def _mo_u_work(consumption, is_working, disutility_of_work):
+    return jnp.log(consumption) - jnp.where(is_working, disutility_of_work, 0.0)
+
+
+def _mo_u_ret(consumption):
+    return jnp.log(consumption)
+
+
+def _mo_income(is_working, wage):
+    return jnp.where(is_working, wage, 0.0)
+
+
+def _mo_is_working(labor_supply):
+    return labor_supply == LaborSupply.work
+
+
+def _mo_next_wealth(wealth, consumption, labor_income, interest_rate):
+    return (1 + interest_rate) * (wealth - consumption) + labor_income
+
+
+def _mo_nr_working(labor_supply, period, survival_probs):
+    sp = survival_probs[period]
+    retire = labor_supply == LaborSupply.retire
+    return jnp.array([jnp.where(retire, 0.0, sp), jnp.where(retire, sp, 0.0), 1 - sp])
+
+
+def _mo_nr_retired(period, survival_probs):
+    sp = survival_probs[period]
+    return jnp.array([0.0, sp, 1 - sp])
+
+
+def _mo_budget(consumption, wealth):
+    return consumption <= wealth
+
+
+def mortality_model():
+    wealth = LinSpacedGrid(start=1, stop=400, n_points=100)
+    cons = LinSpacedGrid(start=1, stop=400, n_points=500)
+    alive = lambda age: age < MORTALITY_LAST_AGE  # noqa: E731
+    working = Regime(
+        actions={"labor_supply": DiscreteGrid(LaborSupply), "consumption": cons},
+        states={"wealth": wealth}, state_transitions={"wealth": _mo_next_wealth},
+        constraints={"borrowing_constraint": _mo_budget}, transition=MarkovTransition(_mo_nr_working),
+        functions={"utility": _mo_u_work, "labor_income": _mo_income, "is_working": _mo_is_working}, active=alive,
+    )
+    retired = Regime(
+        transition=MarkovTransition(_mo_nr_retired), actions={"consumption": cons}, states={"wealth": wealth},
+        state_transitions={"wealth": _mo_next_wealth}, constraints={"borrowing_constraint": _mo_budget},
+        functions={"utility": _mo_u_ret}, active=alive,
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(regimes={"working_life": working, "retirement": retired, "dead": dead},
+                 ages=AgeGrid(start=40, stop=MORTALITY_LAST_AGE, step="10Y"), regime_id_class=MortalityRegimeId)
+
+
+def mortality_params():
+    """The reference's defaults for 4 periods: survival 0.98, 0.82, then 0."""
+    return {
+        "discount_factor": 0.95, "interest_rate": 0.05, "survival_probs": np.array([0.98, 0.82, 0.0]),
+        "working_life": {"utility": {"disutility_of_work": 0.5}, "labor_income": {"wage": 10.0}},
+        "retirement": {"next_wealth": {"labor_income": 0.0}},
+    }
