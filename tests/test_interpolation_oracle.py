@@ -88,3 +88,28 @@ def test_piecewise_grid_rejects_gaps_and_overlaps():
             PiecewiseLinSpacedGrid(segments=segs)
     with pytest.raises(GridInitializationError):
         PiecewiseLogSpacedGrid(segments=(S("[0, 4]", 3),))
+
+
+def test_piecewise_device_table_reproduces_the_coordinate():
+    """The table the kernels read for a piecewise grid ([breakpoints | starts |
+    scales | offsets]), evaluated the way the device does, gives the oracle's
+    coordinate."""
+    from pylcm_b200 import PiecewiseGridSegment as S
+    from pylcm_b200 import PiecewiseLinSpacedGrid, PiecewiseLogSpacedGrid
+
+    rng = np.random.default_rng(4)
+    for grid in (PiecewiseLinSpacedGrid(segments=(S("[1, 4)", 7), S("[4, 10]", 5), S("(10, 30]", 9))),
+                 PiecewiseLogSpacedGrid(segments=(S("[0.1, 10]", 6), S("(10, 1000]", 8)))):
+        tab = grid.coordinate_table()
+        k = len(grid.segments)
+        v = rng.uniform(0.05, 1200.0 if grid.log else 35.0, 500)
+        seg = (v[:, None] >= tab[: k - 1][None, :]).sum(axis=1)
+        st, sc, off = tab[k - 1: 2 * k - 1], tab[2 * k - 1: 3 * k - 1], tab[3 * k - 1:]
+        if grid.log:
+            c = (np.log(v) - st[seg]) / sc[seg]
+            lo = np.floor(c)
+            lower, upper = np.exp(st[seg] + sc[seg] * lo), np.exp(st[seg] + sc[seg] * (lo + 1))
+            local = lo + (v - lower) / (upper - lower)
+        else:
+            local = (v - st[seg]) * sc[seg]
+        np.testing.assert_allclose(off[seg] + local, grid_coordinate(grid, v), rtol=1e-12, atol=1e-12)
