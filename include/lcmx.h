@@ -138,9 +138,13 @@ int lcmx_fues_step(lcmx_ctx* ctx, const void* items, const int* tile_prefix, int
  * such as an XLA FFI custom-call handler).  No counterpart in the reference.
  * Scratch is an 8 MiB file-scope device array per device, so
  * lcmx_fues_workspace_bytes(n_rows, n_in) must not exceed 8 MiB (larger calls
- * return LCMX_ERR_ARGS).  The first call on a device resolves the array's
+ * return LCMX_ERR_ARGS).  Rows of up to 4096 candidates are staged in shared
+ * memory and leave the array unused; longer rows (up to 8192) keep their
+ * sorted copy in it.  The first call on a device resolves the array's
  * address (make it before any stream capture); all calls share the array, so
- * calls that overlap on the GPU race.  Allocates nothing. */
+ * calls that overlap on the GPU race.  The call makes the context's device
+ * current while it runs and restores the caller's current device before it
+ * returns.  Allocates nothing. */
 int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
                           const double* savings, int n_rows, int n_in, double jump_thresh,
                           double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,

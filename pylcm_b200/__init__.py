@@ -14,6 +14,8 @@ from pylcm_b200.exceptions import (
     GridInitializationError,
     InvalidInitialConditionsError,
     InvalidParamsError,
+    InvalidRegimeTransitionProbabilitiesError,
+    InvalidStateTransitionProbabilitiesError,
     InvalidValueFunctionError,
     KernelError,
     ModelInitializationError,
@@ -62,6 +64,8 @@ __all__ = [
     "GridSearch",
     "InvalidInitialConditionsError",
     "InvalidParamsError",
+    "InvalidRegimeTransitionProbabilitiesError",
+    "InvalidStateTransitionProbabilitiesError",
     "InvalidValueFunctionError",
     "IrregSpacedGrid",
     "KernelError",

@@ -796,7 +796,13 @@ extern "C" int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* p
 // * Set-up: the first call on a device, with that device current, looks up
 //   the array's device address with cudaGetSymbolAddress (in host code the
 //   symbol is only a host-side stand-in, not a device address) and caches it
-//   for that device.  Make that first call before any stream capture.
+//   for that device.  Make that first call before any stream capture.  Each
+//   call makes the context's device current for the lookup and the launch and
+//   then restores the caller's current device.
+// * Which rows touch the array: rows of up to 4096 candidates are staged in
+//   shared memory and leave it unused; rows of 4097..8192 candidates go
+//   through the global-workspace kernel, whose per-row sorted copy lives in
+//   the array.
 // * Sharing: every call uses the same array, which keeps the last call's
 //   contents.  Nothing in it has to start at zero (each row's sorted copy is
 //   written in full before it is read), but calls that overlap on the GPU
@@ -829,24 +835,36 @@ extern "C" int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const do
   if (n_rows == 0) return LCMX_OK;
   const int dev = lcmx_ctx_device_of(ctx);
   if (dev < 0 || dev >= 64) return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan_static: device ordinal >= 64");
-  cudaError_t e = cudaSetDevice(dev);
-  if (e != cudaSuccess) return lcmx_set_error_from(ctx, LCMX_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  // The context's device is made current for the symbol lookup and the
+  // launch; the caller's current device is put back before every return.
+  int prev = -1;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e != cudaSuccess) return lcmx_set_error_from(ctx, LCMX_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  if (prev != dev) {
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return lcmx_set_error_from(ctx, LCMX_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  }
+  int rc = LCMX_OK;
+  std::string err;
   double* work = nullptr;
   {
     std::lock_guard<std::mutex> g(g_static_mu);
     if (!g_static_ptr[dev]) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_fues_static_scratch);
-      if (e != cudaSuccess || !p)
-        return lcmx_set_error_from(ctx, LCMX_ERR_CUDA,
-                                   std::string("cudaGetSymbolAddress(static FUES scratch): ") + cudaGetErrorString(e));
-      g_static_ptr[dev] = static_cast<double*>(p);
+      if (e != cudaSuccess || !p) {
+        rc = LCMX_ERR_CUDA;
+        err = std::string("cudaGetSymbolAddress(static FUES scratch): ") + cudaGetErrorString(e);
+      } else {
+        g_static_ptr[dev] = static_cast<double*>(p);
+      }
     }
     work = g_static_ptr[dev];
   }
-  std::string err;
-  int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
-                       n_out, n_kept, work, (cudaStream_t)stream, err);
+  if (rc == LCMX_OK)
+    rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
+                     n_out, n_kept, work, (cudaStream_t)stream, err);
+  if (prev != dev) cudaSetDevice(prev);
   if (rc) return lcmx_set_error_from(ctx, rc, err);
   return LCMX_OK;
 }

@@ -236,10 +236,16 @@ class SolveEngine:
     def plan(self, params_list: Sequence) -> "SolvePlan":
         return SolvePlan(self, list(params_list))
 
-    def solve(self, params) -> tuple[dict, dict]:
+    def solve(self, params, collect_carries: bool = False):
+        """(V, policy) of one parameter set; with ``collect_carries`` also
+        each period's DC-EGM carry rows (see
+        ``SolvePlan.run_collecting_carries``) as a third element."""
         plan = self.plan([params])
-        plan.run()
-        return plan.result(0)
+        if not collect_carries:
+            plan.run()
+            return plan.result(0)
+        carries = plan.run_collecting_carries()
+        return (*plan.result(0), carries)
 
     def solve_batch(self, params_list: Sequence) -> list[tuple[dict, dict]]:
         plan = self.plan(params_list)
@@ -922,6 +928,40 @@ class SolvePlan:
             self._prepared = self._prepare()
         for launch in self._prepared:
             launch(stream)
+
+    def run_collecting_carries(self) -> dict:
+        """Issue every launch on the current stream and keep a copy of each
+        period's DC-EGM carry rows before the two-slot ring overwrites them.
+
+        Returns ``{period: {regime: {"rg", "rc", "rv", "mu", "nk"}}}`` with
+        device tensors of shape (instances, rows, n_pad) (``nk``: (instances,
+        rows)): the refined endogenous grid, policy, value and marginal utility
+        of every discrete-state x discrete-action row and its kept count, the
+        arrays the reference publishes as ``EGMSimPolicy``
+        (``src/_lcm/egm/published_policy.py:76-120``)."""
+        stream = self.torch.cuda.current_stream(self.dev).cuda_stream
+        if self._prepared is None:
+            self._prepared = self._prepare()
+        egm_at: dict[int, list] = {}
+        for p_, s_, _ in self._egm_steps:
+            egm_at.setdefault(p_, []).append(s_.name)
+        out: dict[int, dict] = {}
+
+        def snap(period):
+            for name in egm_at.get(period, ()):
+                b = self.egm[name]
+                slot = period % 2
+                out.setdefault(period, {})[name] = {f: b[f][slot].clone() for f in ("rg", "rc", "rv", "mu", "nk")}
+
+        cur = None
+        for l, launch in zip(self.launches, self._prepared):
+            if cur is not None and l.period != cur:
+                snap(cur)
+            cur = l.period
+            launch(stream)
+        if cur is not None:
+            snap(cur)
+        return dict(sorted(out.items()))
 
     def run_period_inputs(self, period: int, stream: int) -> None:
         """Re-issue the expectation and action-table launches of one period

@@ -21,6 +21,15 @@ class InvalidParamsError(PyLCMError):
     """The params passed to solve/simulate do not match the model."""
 
 
+class InvalidRegimeTransitionProbabilitiesError(PyLCMError):
+    """Regime transition probabilities are non-finite, outside [0, 1], do not
+    sum to one, or reach a regime that is inactive next period."""
+
+
+class InvalidStateTransitionProbabilitiesError(PyLCMError):
+    """A stochastic state transition returned an invalid probability row."""
+
+
 class InvalidValueFunctionError(PyLCMError):
     """A solved value function contains NaN."""
 

@@ -983,3 +983,56 @@ def mortality_params():
         "working_life": {"utility": {"disutility_of_work": 0.5}, "labor_income": {"wage": 10.0}},
         "retirement": {"next_wealth": {"labor_income": 0.0}},
     }
+
+
+# --------------------------------------------------------------------------
+# regime-transition mass: survival probabilities scaled by a `mass` factor,
+# for the continuation's mass check (the reference's
+# ``Q_and_F.py:1401-1432``: CE / mass where |mass - 1| <= 1e-3 and no weight
+# is negative, NaN otherwise) and the transition validation
+# --------------------------------------------------------------------------
+@categorical(ordered=False)
+class MassRegimeId:
+    alive: int
+    dead: int
+
+
+def _mass_u(consumption):
+    return jnp.log(consumption)
+
+
+def _mass_next_wealth(wealth, consumption, interest_rate):
+    return (1 + interest_rate) * (wealth - consumption) + 5.0
+
+
+def _mass_budget(consumption, wealth):
+    return consumption <= wealth
+
+
+def _mass_nr(wealth, period, p_survive, mass, threshold, last_alive_period):
+    # nobody survives into the last period (the alive regime is inactive
+    # there); the distortion applies only above `threshold` wealth, so part
+    # of the state grid keeps a proper distribution
+    p = jnp.where(period < last_alive_period, p_survive, 0.0)
+    m = jnp.where(wealth > threshold, mass, 1.0)
+    return jnp.array([p * m, (1.0 - p) * m])
+
+
+def mass_model(n_periods: int = 4, n_wealth: int = 30, n_cons: int = 40):
+    wealth = LinSpacedGrid(start=1, stop=50, n_points=n_wealth)
+    cons = LinSpacedGrid(start=1, stop=50, n_points=n_cons)
+    last = n_periods - 1
+    alive = Regime(
+        actions={"consumption": cons}, states={"wealth": wealth},
+        state_transitions={"wealth": _mass_next_wealth}, constraints={"borrowing_constraint": _mass_budget},
+        transition=MarkovTransition(_mass_nr), functions={"utility": _mass_u},
+        active=lambda age, last=last: age < last,
+    )
+    dead = Regime(transition=None, functions={"utility": lambda: 0.0})
+    return Model(regimes={"alive": alive, "dead": dead}, ages=AgeGrid(start=0, stop=last, step="Y"),
+                 regime_id_class=MassRegimeId, fixed_params={"last_alive_period": last - 1})
+
+
+def mass_params(mass=1.0, p_survive=0.9, threshold=25.0):
+    return {"discount_factor": 0.95, "interest_rate": 0.03, "p_survive": p_survive, "mass": mass,
+            "threshold": threshold}
