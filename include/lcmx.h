@@ -14,7 +14,9 @@
  *                           max_Q_over_a program, max_Q_over_a.py:30-191).
  *   lcmx_expectation     <- the continuation expectation inside Q_and_F,
  *                           src/_lcm/regime_building/Q_and_F.py:466-681 and
- *                           _expectation_over_stochastic_nodes :1145-1209.
+ *                           _expectation_over_stochastic_nodes :1145-1209
+ *                           (also the tcgen05 form of the single-precision
+ *                           search table, 3xTF32 with FP32 accumulation).
  *   lcmx_simulate        <- the per-period simulation step,
  *                           src/_lcm/simulation/simulate.py:465-668.
  *   lcmx_egm_step        <- the DC-EGM per-period core,
@@ -87,6 +89,14 @@ int lcmx_module_destroy(lcmx_module* mod);
 /* Resident CTAs per SM of `kernel` at the given block size / dynamic smem. */
 int lcmx_occupancy(lcmx_module* mod, const char* kernel, int block, int smem_bytes,
                    int* blocks_per_sm);
+
+/* Read the int status word `name` (a __device__ global) of a module: 0 when
+ * every bounded device-side wait of its kernels completed; the tensor-core
+ * expectation sets its word "lcm_status" to 1 when a wait gave up.  A module
+ * without the word reports 0.  Synchronous (waits for the device); `reset`
+ * clears a non-zero word.  No counterpart in the reference: its XLA programs
+ * have no bounded waits to report. */
+int lcmx_module_status(lcmx_module* mod, const char* name, int* value, int reset);
 
 /* Kernel (a): fused Q_and_F + max/argmax over actions for a batch of
  * (solve instance, regime, period) items; writes V (double) and the flat

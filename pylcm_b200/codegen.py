@@ -50,6 +50,12 @@ def device_header() -> str:
     return (KERNEL_DIR / "lcm_device.cuh").read_text()
 
 
+def tc_header() -> str:
+    """The tcgen05 expectation (lcm_tc.cuh), for modules with a tensor-core
+    form of kernel (b)."""
+    return (KERNEL_DIR / "lcm_tc.cuh").read_text()
+
+
 # ---------------------------------------------------------------------------
 # expression emission
 # ---------------------------------------------------------------------------
@@ -445,9 +451,14 @@ class RegimeKernels:
     # -------------------------------------------------------------- source
     def source(self) -> str:
         parts = [device_header(), _EXTRA_DEVICE, self._bellman_source()]
+        tc = [t for t in self.targets if self.tc_ok(t)]
+        if tc:
+            parts.insert(1, tc_header())
         for t in self.targets:
             if not t.scalar and (t.needs_contraction or self.precision == "fp32"):
                 parts.append(self._expect_source(t))
+        for t in tc:
+            parts.append(self._expect_tc_source(t))
         return "\n".join(parts)
 
     def e_words_for(self, t: TargetPlan) -> int:
@@ -564,6 +575,47 @@ class RegimeKernels:
                 x0 = ir.substitute(x, cv, 0.0)
                 out[(ti, pos)] = (x0, g, cv)
         return out
+
+    def inner_flops(self) -> dict:
+        """Floating-point operations of one (state, action) evaluation of
+        kernel (a)'s inner loop, counted from the traced IR: every
+        floating-point node that depends on a continuous action and on the
+        state (the part not hoisted to the per-tile, per-state or per-action
+        phases) -- arithmetic, comparisons and selects count one, a
+        transcendental one (its special-function unit work is not expanded) --
+        plus, per target reached with a continuous state, the grid coordinate
+        (2 per continuous axis), the multilinear read (2^d - 1 lerps of 2
+        flops, 3 for d = 2 with the two interpolation weights), and the Bellman
+        combination Q = U + beta CE and the running maximum (3)."""
+        spec = self.spec
+        dn = {a.name for a in spec.actions if a.kind != "continuous"}
+        seen: set[int] = set()
+        n_arith = n_trans = 0
+        stack = [r for r in self._roots() if isinstance(r, ir.Expr)]
+        while stack:
+            n = stack.pop()
+            if id(n) in seen or n.op in ("const", "var", "param"):
+                continue
+            seen.add(id(n))
+            d = n.deps()
+            if not (any(k == "state" for k, _ in d) and any(k == "action" and nm not in dn for k, nm in d)):
+                continue
+            if n.dtype == "f" or n.op == "cmp":
+                if n.op == "un":
+                    n_trans += 1
+                else:
+                    n_arith += 1
+            stack.extend(a for a in n.args if isinstance(a, ir.Expr))
+        per_target = []
+        for t in self.targets:
+            if t.scalar or t.unreachable or not t.cont_pos:
+                continue
+            dim = len(t.cont_pos)
+            per_target.append(2 * dim + (2 * (2 ** dim - 1) if dim == 1 else 2 * (2 ** dim - 1) + 2))
+        # a deterministic regime transition reads one target per evaluation
+        interp = (max(per_target) if self.tr.regime_id is not None else sum(per_target)) if per_target else 0
+        total = n_arith + n_trans + interp + 3
+        return {"ir_arith": n_arith, "ir_transcendental": n_trans, "interpolation": interp, "total": total}
 
     def _roots(self):
         """Root IR nodes the per-(state, action) code needs."""
@@ -1507,6 +1559,106 @@ class RegimeKernels:
 
 
     # ------------------------------------------------------------------ (b)
+    def _weight_fill(self, t: TargetPlan, block: int) -> list[str]:
+        """Lines that fill the item's weight table W[k * J + j] (double, in
+        shared memory) with a stride of `block` threads; they read the item
+        words PV (3), period (4) and age (5) through `PV`, `period`, `age`."""
+        tg = t.spec
+        K, J = t.K, t.J
+        L = [f"for (int e = threadIdx.x; e < {K * J}; e += {block}) {{",
+             f"  const int k = e / {J}; const int j = e % {J};",
+             "  int kr = k;"]
+        for kind, kname, size in reversed(t.key_vars):
+            L.append(f"  const int key_{kind}_{kname} = kr % {size}; kr /= {size};")
+        L.append("  int jr = j;")
+        for pos in reversed(t.stoch_pos):
+            ax = tg.states[pos]
+            L.append(f"  const int jn_{ax.name} = jr % {ax.size}; jr /= {ax.size};")
+        prov = {
+            id(ir.var("period", "period", "i")): "period",
+            id(ir.var("age", "age", "f")): "age",
+        }
+        for kind, kname, size in t.key_vars:
+            prov[id(ir.var(kind, kname, "i"))] = f"key_{kind}_{kname}"
+        e = Emitter("double", self.param_off, prov, "w")
+        factors = []
+        for pos in t.stoch_pos:
+            ax = tg.states[pos]
+            law = t.laws[ax.name]
+            if law.kind == "process":
+                off, shape = self.param_off[proc_P_name(law.source_process)]
+                n = shape[0]
+                factors.append(f"PV[{off} + key_state_{law.source_process} * {n} + jn_{ax.name}]")
+            else:
+                # select item j of the Markov vector
+                exprs = [e.emit(x) for x in law.expr.items]
+                sel = exprs[-1]
+                for q in range(len(exprs) - 2, -1, -1):
+                    sel = f"(jn_{ax.name} == {q} ? (double)({exprs[q]}) : {sel})"
+                factors.append(f"(double)({sel})")
+        L += ["  " + s_ for s_ in e.lines]
+        prod = factors[0] if factors else "1.0"
+        for f_ in factors[1:]:
+            prod = f"({prod}) * ({f_})"
+        L.append(f"  W[e] = {prod};")
+        L.append("}")
+        return L
+
+    # ..................................................................
+    # tensor-core form of kernel (b) (single-precision search table)
+    TC_MAX_J = 64
+    TC_MAX_K = 256
+
+    def tc_ok(self, t: TargetPlan) -> bool:
+        """The single-precision search table of target `t` comes from the
+        tcgen05 kernel: a contraction whose V' rows are the target's
+        stochastic node combinations (no deterministic discrete axis), with at
+        most 64 nodes and 256 weight rows."""
+        return (self.precision == "fp32" and not t.scalar and not t.unreachable and t.needs_contraction
+                and not t.det_pos and t.J <= self.TC_MAX_J and t.K <= self.TC_MAX_K)
+
+    def expect_tc_name(self, t: TargetPlan) -> str:
+        return f"lcm_expect_tc_{self.tag}_{t.spec.name}"
+
+    @staticmethod
+    def tc_shape(K: int, J: int) -> dict:
+        """Padded sizes and shared memory of the tensor-core expectation (the
+        host-side twin of LcmTcShape in lcm_tc.cuh)."""
+        JP = (J + 7) // 8 * 8
+        NP = (K + 15) // 16 * 16
+        ncol = 32 if NP <= 32 else 64 if NP <= 64 else 128 if NP <= 128 else 256
+        dyn = 2 * 128 * JP * 4 + 2 * NP * JP * 4 + 128
+        static = K * J * 8 + K * 4 + 8 + 4 + 4 + 64
+        # at most 512 / ncol CTAs per SM so that every CTA's tensor-memory
+        # allocation succeeds at once: pad the dynamic shared memory so that
+        # no more CTAs fit (228 KB per SM, 1 KB reserved per CTA)
+        max_ctas = 512 // ncol
+        per_sm, reserve = 233472, 1024
+        if per_sm // (dyn + static + reserve) > max_ctas:
+            dyn = per_sm // (max_ctas + 1) - static - reserve + 1
+        return {"JP": JP, "NP": NP, "ncol": ncol, "smem": dyn, "max_ctas": max_ctas}
+
+    def _expect_tc_source(self, t: TargetPlan) -> str:
+        """Kernel (b), tensor-core form: EV32 by a 3xTF32 tcgen05 GEMM
+        (lcm_tc_expect in lcm_tc.cuh) with this target's weight table."""
+        name = self.expect_tc_name(t)
+        K, J = t.K, t.J
+        L = [f"// ---- expectation {self.spec.name} -> {t.spec.name} on the tensor cores: K={K} J={J}",
+             f"struct WFill_{name} {{",
+             "  __device__ __forceinline__ void operator()(const i64* __restrict__ it, double* W) const {",
+             "    const double* __restrict__ PV = lcm_wp<const double>(it, 3);",
+             "    const int period = lcm_wi(it, 4);",
+             "    const double age = lcm_wd(it, 5);",
+             "    (void)period; (void)age; (void)PV;"]
+        L += ["    " + s_ for s_ in self._weight_fill(t, 128)]
+        L += ["  }", "};",
+              f'extern "C" __global__ void __launch_bounds__(128) {name}('
+              "const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles) {",
+              f"  lcm_tc_expect<{K}, {J}>(items, tile_prefix, n_items, n_tiles, {8 + len(t.spec.states)}, "
+              f"WFill_{name}{{}});",
+              "}"]
+        return "\n".join(L)
+
     def _expect_source(self, t: TargetPlan) -> str:
         """Kernel (b): contraction of V' over the target's stochastic axes."""
         spec = self.spec
@@ -1544,46 +1696,8 @@ class RegimeKernels:
         ap("    const int n_cols = lcm_wi(it, 7);")
         ap("    (void)period; (void)age;")
         ap("    __syncthreads();")
-        # weight table fill
-        ap(f"    for (int e = threadIdx.x; e < {K * J}; e += {B}) {{")
-        ap(f"      const int k = e / {J}; const int j = e % {J};")
-        # decode k into key vars
-        ap("      int kr = k;")
-        for kind, kname, size in reversed(t.key_vars):
-            ap(f"      const int key_{kind}_{kname} = kr % {size}; kr /= {size};")
-        ap("      int jr = j;")
-        for pos in reversed(stoch):
-            ax = tg.states[pos]
-            ap(f"      const int jn_{ax.name} = jr % {ax.size}; jr /= {ax.size};")
-        prov = {
-            id(ir.var("period", "period", "i")): "period",
-            id(ir.var("age", "age", "f")): "age",
-        }
-        for kind, kname, size in t.key_vars:
-            prov[id(ir.var(kind, kname, "i"))] = f"key_{kind}_{kname}"
-        e = Emitter("double", self.param_off, prov, "w")
-        factors = []
-        for pos in stoch:
-            ax = tg.states[pos]
-            law = t.laws[ax.name]
-            if law.kind == "process":
-                off, shape = self.param_off[proc_P_name(law.source_process)]
-                n = shape[0]
-                factors.append(f"PV[{off} + key_state_{law.source_process} * {n} + jn_{ax.name}]")
-            else:
-                # select item j of the Markov vector
-                exprs = [e.emit(x) for x in law.expr.items]
-                sel = exprs[-1]
-                for q in range(len(exprs) - 2, -1, -1):
-                    sel = f"(jn_{ax.name} == {q} ? (double)({exprs[q]}) : {sel})"
-                factors.append(f"(double)({sel})")
-        for s_ in e.lines:
-            ap("      " + s_)
-        prod = factors[0] if factors else "1.0"
-        for f_ in factors[1:]:
-            prod = f"({prod}) * ({f_})"
-        ap(f"      W[e] = {prod};")
-        ap("    }")
+        for s_ in self._weight_fill(t, B):
+            ap("    " + s_)
         ap("    __syncthreads();")
         ap(f"    for (int k = threadIdx.x; k < {K}; k += {B}) {{")
         ap(f"      double sw = 0.0; for (int j = 0; j < {J}; ++j) sw += W[k * {J} + j];")

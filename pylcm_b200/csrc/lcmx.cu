@@ -39,6 +39,7 @@ struct DriverApi {
   CUresult (*OccupancyMaxActiveBlocksPerMultiprocessor)(int*, CUfunction, int, size_t) = nullptr;
   CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                            CUstream, void**, void**) = nullptr;
+  CUresult (*ModuleGetGlobal)(CUdeviceptr*, size_t*, CUmodule, const char*) = nullptr;
   bool ok = false;
 };
 static DriverApi g_drv;
@@ -61,7 +62,7 @@ static bool drv_init() {
             drv_get("cuModuleUnload", g_drv.ModuleUnload) && drv_get("cuModuleGetFunction", g_drv.ModuleGetFunction) &&
             drv_get("cuFuncSetAttribute", g_drv.FuncSetAttribute) &&
             drv_get("cuOccupancyMaxActiveBlocksPerMultiprocessor", g_drv.OccupancyMaxActiveBlocksPerMultiprocessor) &&
-            drv_get("cuLaunchKernel", g_drv.LaunchKernel);
+            drv_get("cuLaunchKernel", g_drv.LaunchKernel) && drv_get("cuModuleGetGlobal", g_drv.ModuleGetGlobal);
   g_drv.ok = ok;
   return ok;
 }
@@ -342,6 +343,21 @@ static int launch_items(lcmx_module* mod, const char* kernel, const lcmx_launch_
   CUresult r = g_drv.LaunchKernel(f, (unsigned)grid, 1, 1, (unsigned)a->block, 1, 1, (unsigned)a->smem_bytes,
                               (CUstream)stream, params5, nullptr);
   if (r != CUDA_SUCCESS) return set_err(mod->ctx, LCMX_ERR_LAUNCH, std::string("launch ") + kernel + ": " + cu_msg(r));
+  return LCMX_OK;
+}
+
+extern "C" int lcmx_module_status(lcmx_module* mod, const char* name, int* value, int reset) {
+  if (!mod || !name || !value) return set_err(mod ? mod->ctx : nullptr, LCMX_ERR_ARGS, "lcmx_module_status: bad args");
+  *value = 0;
+  CUdeviceptr p = 0;
+  size_t n = 0;
+  CUresult r = g_drv.ModuleGetGlobal(&p, &n, mod->mod, name);
+  if (r == CUDA_ERROR_NOT_FOUND) return LCMX_OK;  // the module has no such word: nothing to report
+  if (r != CUDA_SUCCESS) return set_err(mod->ctx, LCMX_ERR_MODULE, std::string("status word ") + name + ": " + cu_msg(r));
+  if (n < sizeof(int)) return set_err(mod->ctx, LCMX_ERR_MODULE, std::string("status word ") + name + " is too small");
+  cudaError_t e = cudaMemcpy(value, reinterpret_cast<void*>(p), sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && reset && *value) e = cudaMemset(reinterpret_cast<void*>(p), 0, sizeof(int));
+  if (e != cudaSuccess) return set_err(mod->ctx, LCMX_ERR_CUDA, std::string("status word: ") + cudaGetErrorString(e));
   return LCMX_OK;
 }
 

@@ -243,8 +243,10 @@ class SolveEngine:
         plan = self.plan([params])
         if not collect_carries:
             plan.run()
+            plan.check_status()
             return plan.result(0)
         carries = plan.run_collecting_carries()
+        plan.check_status()
         return (*plan.result(0), carries)
 
     def solve_batch(self, params_list: Sequence) -> list[tuple[dict, dict]]:
@@ -632,7 +634,21 @@ class SolvePlan:
             g = self._grp[key] = self._gs_group(rk, s, targets, pkey)
         k = g["index"][period]
         for t, X, tiles in g["expect"]:
-            b.add("expect", rk, rk.expect_name(t), X[k], tiles, 256, 0, period)
+            if rk.tc_ok(t):
+                # single-precision search: the float table comes from the
+                # tensor-core kernel, the double table (the FP64 re-evaluation
+                # and the simulation) from kernel (b) with its float output off
+                X64 = g.setdefault("x64", {}).get(id(t))
+                if X64 is None:
+                    X64 = g["x64"][id(t)] = X.copy()
+                    X64[:, :, 2] = 0
+                b.add("expect", rk, rk.expect_name(t), X64[k], tiles, 256, 0, period)
+                sh = rk.tc_shape(t.K, t.J)
+                ncols = int(X[k][0, 7])
+                b.add("expect_tc", rk, rk.expect_tc_name(t), X[k], [math.ceil(ncols / 128)] * len(tiles), 128,
+                      sh["smem"], period)
+            else:
+                b.add("expect", rk, rk.expect_name(t), X[k], tiles, 256, 0, period)
         rows = g["rows"][k]
         self.records[(period, s.name)] = (rk, rows)
         b.add("atab", rk, rk.atab_name(), rows, g["atab_tiles"], 256, 0, period)
@@ -999,6 +1015,15 @@ class SolvePlan:
     @property
     def gpu_launches(self) -> int:
         return len(self.launches)
+
+    def check_status(self) -> None:
+        """Raise if a bounded device-side wait of this plan's kernels gave up
+        (the tensor-core expectation's mbarrier wait).  Synchronous."""
+        from pylcm_b200.exceptions import KernelError
+
+        for rk in {id(l.module): l.module for l in self.launches if l.kind == "expect_tc"}.values():
+            if rk.module.status(reset=True):
+                raise KernelError(7, f"{rk.key}: a tensor-core wait gave up; its float expectation table is incomplete")
 
     def result(self, i: int) -> tuple[dict, dict]:
         V: dict[int, dict[str, Any]] = {}

@@ -32,6 +32,7 @@ EXPORTED = (
     "lcmx_fues_scan_static",
     "lcmx_fues_step",
     "lcmx_copy_rows_d2h",
+    "lcmx_module_status",
 )
 
 
@@ -88,6 +89,7 @@ def load_library() -> ctypes.CDLL:
             ),
             "lcmx_fues_scan_static": ([vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
             "lcmx_fues_step": ([vp, vp, vp, ip, ip, ip, vp], ip),
+            "lcmx_module_status": ([vp, cp, ctypes.POINTER(ip), ip], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
@@ -170,6 +172,7 @@ class Module:
             "bellman": self.ctx.lib.lcmx_bellman_step,
             "atab": self.ctx.lib.lcmx_bellman_step,
             "expect": self.ctx.lib.lcmx_expectation,
+            "expect_tc": self.ctx.lib.lcmx_expectation,
             "egm": self.ctx.lib.lcmx_egm_step,
         }[kind]
         args = LaunchArgs(items_ptr, prefix_ptr, n_items, n_tiles, grid, block, smem)
@@ -185,6 +188,13 @@ class Module:
 
         launch.keepalive = (args, name)
         return launch
+
+    def status(self, reset: bool = True) -> int:
+        """The module's device status word (0: every bounded wait of its
+        kernels completed).  Synchronous."""
+        v = ctypes.c_int()
+        self.ctx.check(self.ctx.lib.lcmx_module_status(self.h, b"lcm_status", ctypes.byref(v), int(reset)))
+        return v.value
 
     def occupancy(self, kernel: str, block: int, smem: int) -> int:
         n = ctypes.c_int()
