@@ -120,7 +120,10 @@ int lcmx_egm_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* 
 /* Kernel (c), part 2: FUES upper envelope of `n_rows` candidate rows of
  * length n_in (row-major; any order within a row, NaN entries are absent
  * candidates).  `savings` (may be NULL) is each candidate's exogenous savings
- * source.  Outputs are (n_rows x n_out) NaN-padded refined rows in ascending
+ * source.  `n_points_to_scan` bounds the same-segment look-ahead to that many
+ * positions on either side, as FUESEnvelope(n_points_to_scan=...) does
+ * (fues.py:114-128, 1016-1079); <= 0 scans exhaustively (the default).
+ * Outputs are (n_rows x n_out) NaN-padded refined rows in ascending
  * grid order; n_kept[row] > n_out signals overflow (the row holds a valid
  * prefix).  `workspace` must hold lcmx_fues_workspace_bytes(n_rows, n_in)
  * bytes of device memory (rows of up to 4096 candidates are staged in shared
@@ -128,16 +131,17 @@ int lcmx_egm_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* 
 size_t lcmx_fues_workspace_bytes(int n_rows, int n_in);
 int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
                    const double* savings, int n_rows, int n_in, double jump_thresh,
-                   double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
-                   void* workspace, size_t workspace_bytes, void* stream);
+                   int n_points_to_scan, double* grid_out, double* policy_out, double* value_out,
+                   int n_out, int* n_kept, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Kernel (c), part 2, item form: the FUES envelope of the rows of n_items
  * candidate blocks (one per solve instance) in one launch, each row staged in
  * shared memory; same rows as lcmx_fues_scan (fues.py:151-338, one
- * refine_envelope per row).  `items` holds n_items records of 12 64-bit
+ * refine_envelope per row).  `items` holds n_items records of 13 64-bit
  * words: grid, policy, value, savings (0: none), grid_out, policy_out,
- * value_out, n_kept (int32) device pointers, then n_rows, n_in, n_out and
- * jump_thresh (double bits); tile_prefix[i] is the first row of item i and
+ * value_out, n_kept (int32) device pointers, then n_rows, n_in, n_out,
+ * jump_thresh (double bits) and the look-ahead window (<= 0: exhaustive);
+ * tile_prefix[i] is the first row of item i and
  * n_rows the total.  max_n_in (the longest row, at most 4096 candidates)
  * sizes the shared memory.  Needs no workspace. */
 int lcmx_fues_step(lcmx_ctx* ctx, const void* items, const int* tile_prefix, int n_items, int n_rows,
@@ -154,7 +158,7 @@ int lcmx_fues_step(lcmx_ctx* ctx, const void* items, const int* tile_prefix, int
  * address (make it before any stream capture); all calls share the array, so
  * calls that overlap on the GPU race.  The call makes the context's device
  * current while it runs and restores the caller's current device before it
- * returns.  Allocates nothing. */
+ * returns.  The look-ahead is exhaustive.  Allocates nothing. */
 int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
                           const double* savings, int n_rows, int n_in, double jump_thresh,
                           double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,

@@ -309,7 +309,8 @@ def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R, value_mu=N
         cand_c = np.where(dead, np.nan, cand_c)
         cand_v = np.where(dead, np.nan, cand_v)
         cand_s = np.where(dead, np.nan, cand_s)
-        rg, rc, rv, n_kept = refine(cand_g, cand_c, cand_v, cand_s, er.n_pad, er.jump_thresh)
+        rg, rc, rv, n_kept = refine(cand_g, cand_c, cand_v, cand_s, er.n_pad, er.jump_thresh,
+                                    er.scan_window or None)
         envr = dict(env)
         envr[("action", er.C)] = np.where(np.isnan(rc), 1.0, rc)
         with np.errstate(all="ignore"):

@@ -16,7 +16,8 @@ reference implements it in ``src/_lcm/egm/upper_envelope/fues.py``:
   snapped onto a node;
 - the segment test is a jump of |dA/dR| of the implied savings A = R - c above
   ``jump_thresh`` (``_has_policy_jump``, ``fues.py:1082-1131``), the
-  same-segment look-ahead is exhaustive (``fues.py:1016-1079``).
+  same-segment look-ahead is exhaustive by default and bounded to
+  ``n_points_to_scan`` positions when given (``fues.py:114-128, 1016-1079``).
 
 Outputs are NaN-padded rows of length `n_refined` plus the kept count
 (> n_refined signals overflow).
@@ -51,10 +52,13 @@ def _intersect(xa, ya, sa, xb, yb, sb):
     return x, ya + sa * (x - xa)
 
 
-def _find_same_segment(g, p, v, anchor_g, anchor_p, idx, direction, thr):
+def _find_same_segment(g, p, v, anchor_g, anchor_p, idx, direction, thr, window=None):
+    """First candidate on the anchor's segment among positions idx + direction,
+    ..., idx + direction * window (``_find_same_segment_point``,
+    ``fues.py:1016-1079``; window None: every position, ``:114-128``)."""
     n = len(g)
     k = idx + direction
-    while 0 <= k < n:
+    while 0 <= k < n and (window is None or abs(k - idx) <= window):
         if not (math.isnan(g[k]) or math.isnan(v[k])) and not _jump(anchor_g, anchor_p, g[k], p[k], thr):
             return True, g[k], p[k], v[k]
         k += direction
@@ -96,8 +100,10 @@ def sort_and_reduce(grid, policy, value, savings):
     return g, p, v, s
 
 
-def refine(grid, policy, value, savings, n_refined: int, jump_thresh: float = 2.0):
-    """Refined (grid, policy, value) NaN-padded to n_refined, and n_kept."""
+def refine(grid, policy, value, savings, n_refined: int, jump_thresh: float = 2.0, n_points_to_scan=None):
+    """Refined (grid, policy, value) NaN-padded to n_refined, and n_kept.
+    `n_points_to_scan` bounds the same-segment look-ahead (None: exhaustive)."""
+    w = n_points_to_scan
     g, p, v, s = sort_and_reduce(grid, policy, value, savings)
     n = len(g)
     thr = jump_thresh
@@ -112,7 +118,7 @@ def refine(grid, policy, value, savings, n_refined: int, jump_thresh: float = 2.
         node_crossing = valid and switches and gi == gj and vi == vj
         secant = _slope(gj, vj, gi, vi)
         grad_before = _slope(gk, vk, gj, vj)
-        jf, jg, jp, jv = _find_same_segment(g, p, v, gj, pj, idx, 1, thr)
+        jf, jg, jp, jv = _find_same_segment(g, p, v, gj, pj, idx, 1, thr, w)
         if switches and jf:
             below_j = (vi < jv) if gi == jg else (secant < _slope(gi, vi, jg, jv))
         else:
@@ -122,8 +128,8 @@ def refine(grid, policy, value, savings, n_refined: int, jump_thresh: float = 2.
         dropped = dropped and not node_crossing
         if dropped:
             continue
-        ff, fg, fp, fv = _find_same_segment(g, p, v, gi, pi, idx, 1, thr)
-        bf, bg, bp, bv = _find_same_segment(g, p, v, gi, pi, idx, -1, thr)
+        ff, fg, fp, fv = _find_same_segment(g, p, v, gi, pi, idx, 1, thr, w)
+        bf, bg, bp, bv = _find_same_segment(g, p, v, gi, pi, idx, -1, thr, w)
         found = ff or bf
         pg, pp, pv = (fg, fp, fv) if ff else (bg, bp, bv)
         i_slope = _slope(gi, vi, pg, pv)

@@ -89,17 +89,19 @@ __device__ __forceinline__ bool key_less(const Key& a, const Key& b) {
   return a.i < b.i;
 }
 
-// first same-segment candidate from idx in direction dir (warp-cooperative)
+// first same-segment candidate from idx in direction dir among the `window`
+// positions idx + dir, ..., idx + dir * window (warp-cooperative)
 __device__ __forceinline__ bool find_same_segment(const double* g, const double* p, const double* v, int n,
-                                                  double ag, double ap, int idx, int dir, double thr,
+                                                  double ag, double ap, int idx, int dir, double thr, int window,
                                                   double& fg, double& fp, double& fv) {
   const int lane = threadIdx.x & 31;
   for (int base = idx + dir;; base += 32 * dir) {
     if (dir > 0 ? base >= n : base < 0) break;
+    if ((base - idx) * dir > window) break;
     const int k = base + dir * lane;
     bool ok = false;
     double gk = 0.0, pk = 0.0, vk = 0.0;
-    if (k >= 0 && k < n) {
+    if (k >= 0 && k < n && (k - idx) * dir <= window) {
       gk = g[k];
       pk = p[k];
       vk = v[k];
@@ -121,7 +123,7 @@ __device__ __forceinline__ bool find_same_segment(const double* g, const double*
 __global__ void __launch_bounds__(kBlock) fues_kernel(const double* __restrict__ grid, const double* __restrict__ policy,
                                                       const double* __restrict__ value,
                                                       const double* __restrict__ savings, int n_rows, int n_in,
-                                                      double thr, double* __restrict__ grid_out,
+                                                      double thr, int window, double* __restrict__ grid_out,
                                                       double* __restrict__ policy_out, double* __restrict__ value_out,
                                                       int n_out, int* __restrict__ n_kept, double* __restrict__ work) {
   __shared__ int sidx[kMaxSort];
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(kBlock) fues_kernel(const double* __restrict__
         const double secant = slope(gj, vj, gi, vi);
         const double grad_before = slope(gk, vk, gj, vj);
         double jg, jp, jv;
-        const bool jf = find_same_segment(g, p, v, n_in, gj, pj, idx, 1, thr, jg, jp, jv);
+        const bool jf = find_same_segment(g, p, v, n_in, gj, pj, idx, 1, thr, window, jg, jp, jv);
         bool below_j = false;
         if (sw && jf) below_j = (gi == jg) ? (vi < jv) : (secant < slope(gi, vi, jg, jv));
         const bool sav_dec = si < sj;
@@ -236,8 +238,8 @@ __global__ void __launch_bounds__(kBlock) fues_kernel(const double* __restrict__
         dropped = dropped && !node_crossing;
         if (dropped) continue;
         double fg, fp, fv, bg, bp, bv;
-        const bool ff = find_same_segment(g, p, v, n_in, gi, pi, idx, 1, thr, fg, fp, fv);
-        const bool bf = find_same_segment(g, p, v, n_in, gi, pi, idx, -1, thr, bg, bp, bv);
+        const bool ff = find_same_segment(g, p, v, n_in, gi, pi, idx, 1, thr, window, fg, fp, fv);
+        const bool bf = find_same_segment(g, p, v, n_in, gi, pi, idx, -1, thr, window, bg, bp, bv);
         const bool found = ff || bf;
         const double pg = ff ? fg : bg, pp = ff ? fp : bp, pv = ff ? fv : bv;
         const double i_slope = slope(gi, vi, pg, pv);
@@ -314,7 +316,7 @@ __global__ void __launch_bounds__(kBlock) fues_kernel(const double* __restrict__
 // Every value the scan uses is computed with the same operations and
 // operands as in fues_kernel, so the rows are identical.
 constexpr int kSmemMaxN = 4096;
-constexpr int kFuesItemWords = 12;
+constexpr int kFuesItemWords = 13;
 
 __host__ __device__ constexpr size_t fues_smem_bytes(int n) {
   int np2 = 1;
@@ -343,6 +345,7 @@ struct FuesRowIO {
   int n_in;
   int n_out;
   double thr;
+  int window;  // look-ahead positions inspected in each direction
 };
 
 struct FuesContig {
@@ -356,6 +359,7 @@ struct FuesContig {
   int* nk;
   int n_rows, n_in, n_out;
   double thr;
+  int window;
   __device__ __forceinline__ int count() const { return n_rows; }
   __device__ __forceinline__ FuesRowIO row(int r) const {
     FuesRowIO io;
@@ -370,13 +374,15 @@ struct FuesContig {
     io.n_in = n_in;
     io.n_out = n_out;
     io.thr = thr;
+    io.window = window;
     return io;
   }
 };
 
 // item words: 0 grid, 1 policy, 2 value, 3 savings (0: none), 4 grid_out,
 // 5 policy_out, 6 value_out, 7 n_kept (int32), 8 n_rows, 9 n_in, 10 n_out,
-// 11 jump_thresh (double bits); one tile per row
+// 11 jump_thresh (double bits), 12 look-ahead window (<= 0: exhaustive);
+// one tile per row
 struct FuesItems {
   const int64_t* items;
   const int* prefix;
@@ -394,6 +400,7 @@ struct FuesItems {
     io.n_in = (int)it[9];
     io.n_out = (int)it[10];
     io.thr = __longlong_as_double(it[11]);
+    io.window = it[12] > 0 ? (int)it[12] : io.n_in;
     io.G = reinterpret_cast<const double*>(it[0]) + (int64_t)r * io.n_in;
     io.P = reinterpret_cast<const double*>(it[1]) + (int64_t)r * io.n_in;
     io.V = reinterpret_cast<const double*>(it[2]) + (int64_t)r * io.n_in;
@@ -606,7 +613,7 @@ __global__ void __launch_bounds__(kBlock) fues_smem_kernel(Rows rows) {
         double jg = nan, jp = nan, jv = nan;
         bool jf = false;
         if (sw) {
-          jf = find_same_segment(g, p, v, n, gj, pj, idx, 1, thr, jg, jp, jv);
+          jf = find_same_segment(g, p, v, n, gj, pj, idx, 1, thr, io.window, jg, jp, jv);
           if (!drop && jf) drop = (gi == jg) ? (vi < jv) : (get_secant() < slope(gi, vi, jg, jv));
         }
         if (drop && !node_crossing) continue;
@@ -626,8 +633,8 @@ __global__ void __launch_bounds__(kBlock) fues_smem_kernel(Rows rows) {
         const double sc = get_secant();
         const double gb = get_gb();
         double fg, fp, fv, bg, bp, bv;
-        const bool ff = find_same_segment(g, p, v, n, gi, pi, idx, 1, thr, fg, fp, fv);
-        const bool bf = find_same_segment(g, p, v, n, gi, pi, idx, -1, thr, bg, bp, bv);
+        const bool ff = find_same_segment(g, p, v, n, gi, pi, idx, 1, thr, io.window, fg, fp, fv);
+        const bool bf = find_same_segment(g, p, v, n, gi, pi, idx, -1, thr, io.window, bg, bp, bv);
         const bool found = ff || bf;
         const double pg = ff ? fg : bg, pp = ff ? fp : bp, pv = ff ? fv : bv;
         const double i_slope = slope(gi, vi, pg, pv);
@@ -727,14 +734,15 @@ extern "C" size_t lcmx_fues_workspace_bytes(int n_rows, int n_in) {
 }
 
 static int launch_fues(const double* grid, const double* policy, const double* value, const double* savings,
-                       int n_rows, int n_in, double jump_thresh, double* grid_out, double* policy_out,
-                       double* value_out, int n_out, int* n_kept, double* work, cudaStream_t stream,
-                       std::string& err) {
+                       int n_rows, int n_in, double jump_thresh, int window, double* grid_out,
+                       double* policy_out, double* value_out, int n_out, int* n_kept, double* work,
+                       cudaStream_t stream, std::string& err) {
+  if (window <= 0) window = n_in;  // exhaustive look-ahead
   if (n_in <= kSmemMaxN) {
     int rc = fues_smem_attr(err);
     if (rc) return rc;
     FuesContig rows{grid, policy, value, savings, grid_out, policy_out, value_out, n_kept,
-                    n_rows, n_in, n_out, jump_thresh};
+                    n_rows, n_in, n_out, jump_thresh, window};
     fues_smem_kernel<FuesContig><<<fues_grid(n_rows), kBlock, fues_smem_bytes(n_in), stream>>>(rows);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -747,8 +755,8 @@ static int launch_fues(const double* grid, const double* policy, const double* v
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   int grid_n = n_rows < sms * 4 ? n_rows : sms * 4;
-  fues_kernel<<<grid_n, kBlock, 0, stream>>>(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out,
-                                             policy_out, value_out, n_out, n_kept, work);
+  fues_kernel<<<grid_n, kBlock, 0, stream>>>(grid, policy, value, savings, n_rows, n_in, jump_thresh, window,
+                                             grid_out, policy_out, value_out, n_out, n_kept, work);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     err = std::string("fues launch: ") + cudaGetErrorString(e);
@@ -761,8 +769,8 @@ int lcmx_set_error_from(lcmx_ctx* ctx, int code, const std::string& msg);
 
 extern "C" int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
                               const double* savings, int n_rows, int n_in, double jump_thresh,
-                              double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
-                              void* workspace, size_t workspace_bytes, void* stream) {
+                              int n_points_to_scan, double* grid_out, double* policy_out, double* value_out,
+                              int n_out, int* n_kept, void* workspace, size_t workspace_bytes, void* stream) {
   if (!ctx || !grid || !policy || !value || !grid_out || !policy_out || !value_out || !n_kept || n_rows < 0 ||
       n_in < 1 || n_out < 1 || !(jump_thresh > 0.0))
     return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan: bad arguments");
@@ -772,8 +780,9 @@ extern "C" int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* p
   if (!workspace || workspace_bytes < lcmx_fues_workspace_bytes(n_rows, n_in))
     return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_fues_scan: workspace too small");
   std::string err;
-  int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
-                       n_out, n_kept, static_cast<double*>(workspace), (cudaStream_t)stream, err);
+  int rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, n_points_to_scan, grid_out,
+                       policy_out, value_out, n_out, n_kept, static_cast<double*>(workspace), (cudaStream_t)stream,
+                       err);
   if (rc) return lcmx_set_error_from(ctx, rc, err);
   return LCMX_OK;
 }
@@ -862,7 +871,7 @@ extern "C" int lcmx_fues_scan_static(lcmx_ctx* ctx, const double* grid, const do
     work = g_static_ptr[dev];
   }
   if (rc == LCMX_OK)
-    rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out, value_out,
+    rc = launch_fues(grid, policy, value, savings, n_rows, n_in, jump_thresh, 0, grid_out, policy_out, value_out,
                      n_out, n_kept, work, (cudaStream_t)stream, err);
   if (prev != dev) cudaSetDevice(prev);
   if (rc) return lcmx_set_error_from(ctx, rc, err);

@@ -111,6 +111,7 @@ class EgmRegime:
     ratio: float
     n_pad: int
     jump_thresh: float
+    scan_window: int  # FUES same-segment look-ahead (0: exhaustive)
     taste_scale: float | None
     feasible: ir.Expr
     tracer: Any
@@ -254,6 +255,7 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
         ratio=ratio,
         n_pad=n_pad,
         jump_thresh=float(solver.envelope.jump_thresh),
+        scan_window=int(solver.envelope.n_points_to_scan or 0),
         taste_scale=taste,
         feasible=feasible,
         tracer=t,

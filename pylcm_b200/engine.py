@@ -809,10 +809,11 @@ class SolvePlan:
         cg, cc, cv, cs = b["cand"]
         frecs = []
         for i in range(n):
-            fr = np.zeros(12, dtype=np.int64)
+            fr = np.zeros(13, dtype=np.int64)
             fr[0], fr[1], fr[2], fr[3] = cg[i].data_ptr(), cc[i].data_ptr(), cv[i].data_ptr(), cs[i].data_ptr()
             fr[8], fr[9], fr[10] = nrow, ncand, npad
             fr[11] = _f2w(er.jump_thresh)
+            fr[12] = er.scan_window
             frecs.append(fr)
         out["recs"] = np.stack(recs).astype(np.int64)
         out["fues"] = np.stack(frecs).astype(np.int64)
@@ -875,7 +876,7 @@ class SolvePlan:
             rec.add("fues", None, "lcmx_fues_step", g["fues"][k], g["tiles_f"], 0, ncand, period)
         else:
             rec.append(
-                Launch("fues", ("fues", name, period % 2, er.jump_thresh), "lcmx_fues_scan", 0, 0,
+                Launch("fues", ("fues", name, period % 2, er.jump_thresh, er.scan_window), "lcmx_fues_scan", 0, 0,
                        self.n * b["nrow"], 0, 0, 0, period)
             )
         rec.add("egm", ek, uname, rows, g["tiles_u"], 256, 0, period)
@@ -892,7 +893,7 @@ class SolvePlan:
 
         return launch
 
-    def _fues_launch(self, spec_name, slot, thr, instances=None):
+    def _fues_launch(self, spec_name, slot, thr, window=0, instances=None):
         from pylcm_b200.runtime import get_context
 
         ctx = get_context(self.eng.device)
@@ -914,7 +915,7 @@ class SolvePlan:
 
         def launch(stream):
             for ptrs, outs, nk, ws, wb in calls:
-                ctx.fues_scan(*ptrs, nrow, ncand, thr, *outs, npad, nk, ws, wb, stream)
+                ctx.fues_scan(*ptrs, nrow, ncand, thr, *outs, npad, nk, ws, wb, stream, n_points_to_scan=window)
 
         return launch
 
@@ -927,7 +928,7 @@ class SolvePlan:
         out = []
         for l in launches:
             if l.kind == "fues":
-                out.append(self._fues_item_launch(l, ib, pb) if l.module is None else self._fues_launch(*l.module[1:4]))
+                out.append(self._fues_item_launch(l, ib, pb) if l.module is None else self._fues_launch(*l.module[1:5]))
                 continue
             out.append(
                 l.module.module.prepared(
@@ -1107,7 +1108,7 @@ class BatchPlan:
                         continue
                     pl, l, h, gk = lst[j]
                     if gk is None:
-                        b.append(Launch("fues", (pl,) + tuple(l.module[1:4]) + (tuple(sl),), l.kernel, 0, 0,
+                        b.append(Launch("fues", (pl,) + tuple(l.module[1:5]) + (tuple(sl),), l.kernel, 0, 0,
                                         l.n_items, 0, 0, 0, k))
                         continue
                     arr, tiles = h
@@ -1137,8 +1138,8 @@ class BatchPlan:
                 if l.module is None:
                     out.append(SolvePlan._fues_item_launch(self, l, ib, pb))
                 else:
-                    pl, name, slot, thr, sl = l.module
-                    out.append(pl._fues_launch(name, slot, thr, sl))
+                    pl, name, slot, thr, window, sl = l.module
+                    out.append(pl._fues_launch(name, slot, thr, window, sl))
                 continue
             out.append(
                 l.module.module.prepared(

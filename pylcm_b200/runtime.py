@@ -84,7 +84,7 @@ def load_library() -> ctypes.CDLL:
                                    ip),
             "lcmx_fues_workspace_bytes": ([ip, ip], ctypes.c_size_t),
             "lcmx_fues_scan": (
-                [vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp, ctypes.c_size_t, vp],
+                [vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, ip, vp, vp, vp, ip, vp, vp, ctypes.c_size_t, vp],
                 ip,
             ),
             "lcmx_fues_scan_static": ([vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
@@ -151,12 +151,13 @@ class Context:
         return int(self.lib.lcmx_fues_workspace_bytes(n_rows, n_in))
 
     def fues_scan(self, grid, policy, value, savings, n_rows, n_in, jump_thresh, grid_out, policy_out,
-                  value_out, n_out, n_kept, workspace, workspace_bytes, stream) -> None:
-        """FUES envelope of candidate rows (all arguments are device pointers)."""
+                  value_out, n_out, n_kept, workspace, workspace_bytes, stream, n_points_to_scan: int = 0) -> None:
+        """FUES envelope of candidate rows (all arguments are device pointers;
+        `n_points_to_scan` <= 0: exhaustive look-ahead)."""
         self.check(
             self.lib.lcmx_fues_scan(self.h, grid, policy, value, savings, n_rows, n_in, float(jump_thresh),
-                                    grid_out, policy_out, value_out, n_out, n_kept, workspace,
-                                    workspace_bytes, stream)
+                                    int(n_points_to_scan), grid_out, policy_out, value_out, n_out, n_kept,
+                                    workspace, workspace_bytes, stream)
         )
 
 

@@ -17,11 +17,16 @@ class FUESEnvelope:
 
     jump_thresh: float = 2.0
     n_points_to_scan: int | None = None
-    scan_unroll: int = 1
+    scan_unroll: int = 1  # a loop-unrolling knob of the reference's scan; results do not depend on it
 
     def __post_init__(self) -> None:
         if self.jump_thresh <= 0:
             raise ValueError("jump_thresh must be positive")
+        if self.n_points_to_scan is not None:
+            if int(self.n_points_to_scan) < 1:
+                raise ValueError("n_points_to_scan must be a positive integer or None")
+        if self.scan_unroll < 1:
+            raise ValueError("scan_unroll must be >= 1")
 
 
 @dataclasses.dataclass(frozen=True, kw_only=True)

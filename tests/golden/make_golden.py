@@ -1,7 +1,8 @@
 """Extract the reference's stored float64 solutions into small .npz fixtures.
 
-Run once in a checkout that has the reference project at REFERENCE (default
-/root/reference); the outputs are committed, so tests never read the reference.
+Run once with the environment variable REFERENCE set to a checkout of the
+reference project; the outputs are committed, so tests never read the
+reference.
 
 The reference's .pkl files hold cloudpickled JAX arrays; they unpickle without
 JAX through a stub of ``jax._src.array._reconstruct_array`` that rebuilds the
@@ -17,7 +18,12 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE = Path(os.environ.get("REFERENCE", "/root/reference"))
+def _reference() -> Path:
+    ref = os.environ.get("REFERENCE")
+    if not ref:
+        raise SystemExit("set REFERENCE to the directory of a checkout of the reference project")
+    return Path(ref)
+
 OUT = Path(__file__).resolve().parent
 
 
@@ -50,7 +56,7 @@ def main() -> None:
     _install_jax_stub()
     import pandas as pd
 
-    data = REFERENCE / "tests" / "data"
+    data = _reference() / "tests" / "data"
     np.savez(OUT / "regression_solution.npz", **_flatten(pd.read_pickle(data / "regression_tests" / "solution.pkl")))
     for kind in ("uniform", "normal", "lognormal", "tauchen", "rouwenhorst"):
         sol = pd.read_pickle(data / "processes" / f"solution_{kind}.pkl")

@@ -42,6 +42,18 @@ def test_dcegm_income_shock_model_matches_oracle(taste):
             assert rel_err(V[p][r], Vo[p][r]) < 1e-10, (taste, p, r)
 
 
+@pytest.mark.parametrize("window", [3, 25])
+def test_dcegm_bounded_look_ahead_matches_oracle(window):
+    """FUESEnvelope(n_points_to_scan=k) on the GPU and in the oracle."""
+    model = M.dcegm_model(n_periods=5, n_savings=200, n_wealth=100, n_points_to_scan=window)
+    params = M.dcegm_params(4)
+    V = model.solve(params=params, log_level="off")
+    Vo, _ = oracle_solve(model, params)
+    for p in Vo:
+        for r in Vo[p]:
+            assert rel_err(V[p][r], Vo[p][r]) < 1e-10, (window, p, r)
+
+
 def test_dcegm_batch_equals_single():
     model = M.dcegm_model(n_periods=4, n_savings=120, n_wealth=60)
     ps = [M.dcegm_params(s) for s in range(3)]

@@ -9,7 +9,7 @@ from tests.test_fues_oracle import _crossing
 pytestmark = pytest.mark.gpu
 
 
-def _gpu_fues(rows_g, rows_c, rows_v, rows_s, n_out, thr=2.0):
+def _gpu_fues(rows_g, rows_c, rows_v, rows_s, n_out, thr=2.0, window=0):
     import torch
 
     from pylcm_b200.runtime import get_context
@@ -26,7 +26,8 @@ def _gpu_fues(rows_g, rows_c, rows_v, rows_s, n_out, thr=2.0):
     ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream().cuda_stream
     ctx.fues_scan(g.data_ptr(), c.data_ptr(), v.data_ptr(), s.data_ptr(), n_rows, n_in, thr,
-                  go.data_ptr(), co.data_ptr(), vo.data_ptr(), n_out, nk.data_ptr(), ws.data_ptr(), wb, stream)
+                  go.data_ptr(), co.data_ptr(), vo.data_ptr(), n_out, nk.data_ptr(), ws.data_ptr(), wb, stream,
+                  n_points_to_scan=window)
     torch.cuda.synchronize()
     return go.cpu().numpy(), co.cpu().numpy(), vo.cpu().numpy(), nk.cpu().numpy()
 
@@ -120,7 +121,8 @@ def test_item_form_matches_the_contiguous_form():
         ins = [d(G), d(C), d(V), d(S)]
         outs = [torch.full((n_rows, n_out), 7.0, dtype=torch.float64, device="cuda") for _ in range(3)]
         nk = torch.zeros(n_rows, dtype=torch.int32, device="cuda")
-        w = [t.data_ptr() for t in ins] + [t.data_ptr() for t in outs] + [nk.data_ptr(), n_rows, n_in, n_out, _f2w(thr)]
+        w = [t.data_ptr() for t in ins] + [t.data_ptr() for t in outs] + [nk.data_ptr(), n_rows, n_in, n_out, _f2w(thr),
+                                                                            0]
         words.append(np.array(w, dtype=np.int64))
         tiles.append(n_rows)
         keep.append((G, C, V, S, n_out, thr, ins, outs, nk))
@@ -135,3 +137,46 @@ def test_item_form_matches_the_contiguous_form():
         np.testing.assert_array_equal(outs[1].cpu().numpy(), co)
         np.testing.assert_array_equal(outs[2].cpu().numpy(), vo)
         np.testing.assert_array_equal(nk.cpu().numpy(), k)
+
+
+@pytest.mark.parametrize("n", [300, 5000])
+@pytest.mark.parametrize("window", [2, 7, 40])
+def test_bounded_look_ahead_matches_the_oracle(n, window):
+    """FUESEnvelope(n_points_to_scan=k): the same-segment look-ahead inspects
+    k positions on either side (fues.py:1016-1079), on the shared-memory
+    (300) and the global-workspace (5000 candidates) kernels."""
+    G, C, V, S = _rows_nonconcave(4, n, seed=n + window)
+    n_out = 2 * n + 2
+    go, co, vo, nk = _gpu_fues(G, C, V, S, n_out, window=window)
+    for r in range(G.shape[0]):
+        rg, rc, rv, k = refine(G[r], C[r], V[r], S[r], n_out, n_points_to_scan=window)
+        assert nk[r] == k
+        _same(go[r], rg)
+        _same(co[r], rc)
+        _same(vo[r], rv)
+
+
+def test_item_form_honours_the_window_word():
+    import torch
+
+    from pylcm_b200.engine import _f2w
+    from pylcm_b200.runtime import get_context
+
+    ctx = get_context(0)
+    n_rows, n_in, window = 3, 500, 3
+    G, C, V, S = _rows_nonconcave(n_rows, n_in, seed=21)
+    n_out = 2 * n_in + 2
+    d = lambda a: torch.as_tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")  # noqa: E731
+    ins = [d(G), d(C), d(V), d(S)]
+    outs = [torch.full((n_rows, n_out), 7.0, dtype=torch.float64, device="cuda") for _ in range(3)]
+    nk = torch.zeros(n_rows, dtype=torch.int32, device="cuda")
+    w = [t.data_ptr() for t in ins] + [t.data_ptr() for t in outs] + [nk.data_ptr(), n_rows, n_in, n_out, _f2w(2.0),
+                                                                        window]
+    items = torch.as_tensor(np.array(w, dtype=np.int64), device="cuda")
+    prefix = torch.as_tensor(np.array([0, n_rows], dtype=np.int32), device="cuda")
+    ctx.fues_step(items.data_ptr(), prefix.data_ptr(), 1, n_rows, n_in, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    go, co, vo, k = _gpu_fues(G, C, V, S, n_out, window=window)
+    np.testing.assert_array_equal(outs[0].cpu().numpy(), go)
+    np.testing.assert_array_equal(outs[2].cpu().numpy(), vo)
+    np.testing.assert_array_equal(nk.cpu().numpy(), k)

@@ -59,3 +59,39 @@ def test_node_aligned_crossing_keeps_both_branches():
     at = rg[m] == 10.0
     assert at.sum() == 2  # both branch policies at the node
     np.testing.assert_allclose(np.sort(rc[m][at]), [4.0, 9.0])
+
+
+def _interlopers(n_between: int):
+    """One concave segment A (savings slope 0.5) with runs of `n_between`
+    points of a lower segment B (savings slope 0.05, a policy jump) between
+    consecutive A points."""
+    ra = np.arange(1.0, 11.0)
+    g, c, v = [], [], []
+    for k, r in enumerate(ra):
+        g.append(r)
+        c.append(0.5 * r)
+        v.append(np.log(0.5 * r) + 2.0)
+        if k + 1 < len(ra):
+            for q in range(n_between):
+                rb = r + (q + 1) / (n_between + 1)
+                g.append(rb)
+                c.append(0.95 * rb)
+                v.append(np.log(0.95 * rb) + 1.0 + 0.2 * np.sin(7 * rb))
+    g, c, v = map(np.asarray, (g, c, v))
+    return g, c, v, g - c
+
+
+def test_a_window_shorter_than_the_interloper_runs_changes_the_envelope():
+    """The reference's caveat (fues.py:114-128): a bounded look-ahead that
+    cannot reach past a run of off-segment candidates treats a segment point
+    as without continuation; an exhaustive scan (None, or a window covering
+    the row) reaches it."""
+    g, c, v, s = _interlopers(4)
+    n_out = 4 * len(g)
+    full = refine(g, c, v, s, n_out)
+    wide = refine(g, c, v, s, n_out, n_points_to_scan=len(g))
+    narrow = refine(g, c, v, s, n_out, n_points_to_scan=2)
+    for a, b in zip(full[:3], wide[:3]):
+        np.testing.assert_array_equal(a, b)
+    assert full[3] == wide[3]
+    assert not all(np.array_equal(a, b, equal_nan=True) for a, b in zip(full[:3], narrow[:3]))

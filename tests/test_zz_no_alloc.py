@@ -64,7 +64,7 @@ def _run(ctx, kind, dev_rows, n_rows, n, n_out, stream):
     if kind == "workspace":
         wb = lib.lcmx_fues_workspace_bytes(n_rows, n)
         ws = torch.empty(wb, dtype=torch.uint8, device="cuda")
-        rc = lib.lcmx_fues_scan(ctx.h, g.data_ptr(), c.data_ptr(), v.data_ptr(), s.data_ptr(), n_rows, n, 2.0,
+        rc = lib.lcmx_fues_scan(ctx.h, g.data_ptr(), c.data_ptr(), v.data_ptr(), s.data_ptr(), n_rows, n, 2.0, 0,
                                 go.data_ptr(), co.data_ptr(), vo.data_ptr(), n_out, nk.data_ptr(),
                                 ws.data_ptr(), wb, stream)
     else:
