@@ -9,8 +9,15 @@ batch-size bucket, so tuning runs once per (model structure, batch bucket).
 
 The candidate set is built around the occupancy heuristic of
 ``engine.default_config``: lanes in {L/2, L, 2L} (L the heuristic), states per
-thread in {1, 2}, block in {128, 256}, and either the compiler's register
-choice or a bound that keeps 1024 resident threads per SM.
+thread in {1, 2} (and 4 in the single-precision search), block in {128, 256},
+action chunk in {256, 512}.
+
+A candidate that NVRTC cannot compile, or whose launch the driver refuses
+(resources), is skipped.  Any other failure -- in particular an error left
+on the context by a launch that ran -- is raised: the context would be
+unusable for the remaining candidates and for the caller.
+
+Used by ``BatchSolver(..., autotune=True)`` and ``Server(..., autotune=True)``.
 """
 
 from __future__ import annotations
@@ -43,15 +50,27 @@ def _structure_key(eng: SolveEngine, spec, params) -> str:
 
 
 def candidates(spec, precision: str, n_items: int) -> list[LaunchConfig]:
+    """Launch shapes around the heuristic's; the heuristic's own shape first."""
     base = default_config(spec, precision, n_items)
     lanes_set = sorted({max(1, base.lanes // 2), base.lanes, min(32, base.lanes * 2)})
-    out = []
-    for lanes, sb, block, mb in itertools.product(lanes_set, (1, 2), (128, 256), (0, 4)):
-        if lanes * 8 > max(8, spec.n_actions):
+    sbs = (1, 2, 4) if precision == "fp32" else (1, 2)
+    out = [base]
+    for lanes, sb, block, chunk in itertools.product(lanes_set, sbs, (128, 256), (256, 512)):
+        if lanes * 8 > max(8, spec.n_actions) or block // lanes < 8:
             continue
-        mbk = mb * (256 // block) if mb else 0
-        out.append(LaunchConfig(block=block, lanes=lanes, chunk=256, sb=sb, min_blocks=mbk))
+        cfg = LaunchConfig(block=block, lanes=lanes, chunk=chunk, sb=sb)
+        if cfg not in out:
+            out.append(cfg)
     return out
+
+
+def _skippable(e: Exception) -> bool:
+    """A candidate failure that leaves the context usable: NVRTC rejected
+    the source (LCMX_ERR_COMPILE) or the driver refused the launch
+    configuration (LCMX_ERR_LAUNCH before anything ran)."""
+    from pylcm_b200.exceptions import KernelError
+
+    return isinstance(e, KernelError) and e.status in (2, 4)
 
 
 def _time_regime(model, precision: str, params_list, spec, cfg: LaunchConfig, reps: int = 2) -> float:
@@ -105,7 +124,11 @@ def tune(model, precision: str, params_list, regimes: list[str] | None = None, v
         for cfg in candidates(spec, precision, n):
             try:
                 t = _time_regime(model, precision, params_list, spec, cfg)
-            except Exception as e:  # noqa: BLE001  (a candidate that fails to launch is skipped)
+            except Exception as e:
+                if not _skippable(e):
+                    raise
+                # the refused candidate must not have left an error behind
+                torch.cuda.synchronize()
                 if verbose:
                     print("autotune: skip", cfg, repr(e)[:120])
                 continue

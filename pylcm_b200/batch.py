@@ -22,16 +22,28 @@ from pylcm_b200.engine import SolveEngine, SolvePlan
 
 class BatchSolver:
     def __init__(self, model, batch_size: int, precision: str = "fp32", template_params=None,
-                 use_graph: bool = True, configs: dict | None = None, device: int = 0) -> None:
+                 use_graph: bool = True, configs: dict | None = None, device: int = 0,
+                 autotune: bool = False) -> None:
+        """`autotune=True` times candidate launch shapes of kernel (a) for
+        this model and batch size once (cached on disk per GPU, generated
+        code and batch bucket, see ``pylcm_b200.autotune``) and uses the
+        fastest; explicit `configs` win over tuned ones."""
         import torch
 
         self.torch = torch
         self.model = model
         self.n = int(batch_size)
         self.precision = precision
-        self.engine = SolveEngine(model, precision, configs=configs, device=device)
         if template_params is None:
             raise ValueError("template_params (one valid params dict) is required to trace the model")
+        cfgs = {}
+        if autotune:
+            from pylcm_b200 import autotune as _at
+
+            cfgs.update(_at.tune(model, precision, [template_params] * self.n))
+        cfgs.update(configs or {})
+        self.configs = cfgs
+        self.engine = SolveEngine(model, precision, configs=cfgs, device=device)
         self.plan: SolvePlan = self.engine.plan([template_params] * self.n)
         self.use_graph = use_graph
         # pinned host staging for parameters and results

@@ -180,7 +180,12 @@ class Server:
     """
 
     def __init__(self, device: int = 0, precision: str = "fp32", max_batch: int = 32, n_streams: int = 4,
-                 hbm_budget_bytes: int | None = None, configs: Mapping | None = None, pool_slots: int = 4) -> None:
+                 hbm_budget_bytes: int | None = None, configs: Mapping | None = None, pool_slots: int = 4,
+                 autotune: bool = False) -> None:
+        """`autotune=True`: the launch shape of each family's regimes is tuned
+        once, on the family's first model at the job size `max_batch`
+        (``pylcm_b200.autotune``, cached on disk); it then stays pinned for
+        the family, so results still do not depend on the batch."""
         import torch
 
         self.torch = torch
@@ -195,6 +200,7 @@ class Server:
             hbm_budget_bytes = free // 2
         self.budget = int(hbm_budget_bytes)
         self.configs = dict(configs or {})
+        self.autotune = bool(autotune)
         self._engines: dict[Hashable, SolveEngine] = {}
         self._family_cfg: dict[Hashable, dict] = {}
         self._pools: dict[Hashable, list[_Pool]] = {}
@@ -219,7 +225,12 @@ class Server:
         if eng is None:
             cfgs = self._family_cfg.get(req.family)
             if cfgs is None:
-                cfgs = dict(self.configs.get(req.family, {}))
+                cfgs = {}
+                if self.autotune:
+                    from pylcm_b200 import autotune as _at
+
+                    cfgs.update(_at.tune(req.model, self.precision, [req.params] * self.max_batch))
+                cfgs.update(self.configs.get(req.family, {}))
                 for s in req.model.regime_specs:
                     if s.name not in cfgs:
                         # jobs of tens of requests: 2 lanes x 2 states per thread
