@@ -462,7 +462,7 @@ class RegimeKernels:
         return "\n".join(parts)
 
     def e_words_for(self, t: TargetPlan) -> int:
-        return 8 + len(t.spec.states)
+        return 9 + len(t.spec.states)
 
     def bellman_name(self) -> str:
         return f"lcm_bellman_{self.tag}"
@@ -1654,8 +1654,8 @@ class RegimeKernels:
         L += ["  }", "};",
               f'extern "C" __global__ void __launch_bounds__(128) {name}('
               "const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles) {",
-              f"  lcm_tc_expect<{K}, {J}>(items, tile_prefix, n_items, n_tiles, {8 + len(t.spec.states)}, "
-              f"WFill_{name}{{}});",
+              f"  lcm_tc_expect<{K}, {J}>(items, tile_prefix, n_items, n_tiles, {9 + len(t.spec.states)}, "
+              f"{8 + len(t.spec.states)}, WFill_{name}{{}});",
               "}"]
         return "\n".join(L)
 
@@ -1674,8 +1674,9 @@ class RegimeKernels:
         # item layout for (b)
         # 0 Vt (double*), 1 EV64 out, 2 EV32 out (0 if none), 3 PV (params of source)
         # 4 period, 5 age, 6 cblk, 7 n_cols, 8.. sizes of target axes
-        self.EW = {"V": 0, "EV64": 1, "EV32": 2, "P": 3, "PERIOD": 4, "AGE": 5, "CBLK": 6, "NCOLS": 7, "SIZES": 8}
-        self.e_words = 8 + len(tg.states)
+        self.EW = {"V": 0, "EV64": 1, "EV32": 2, "P": 3, "PERIOD": 4, "AGE": 5, "CBLK": 6, "NCOLS": 7, "SIZES": 8,
+                   "BSTATS": 8 + len(tg.states)}
+        self.e_words = 9 + len(tg.states)
         ap(f"// ---- expectation {spec.name} -> {tg.name}: K={K} J={J}")
         ap(
             f'extern "C" __global__ void __launch_bounds__({B}) {name}('
@@ -1704,8 +1705,14 @@ class RegimeKernels:
         ap("      Winv[k] = sw > 0.0 ? sw : 1.0;")
         ap("    }")
         ap("    __syncthreads();")
-        ap(f"    const int col = (tile - tile_prefix[item]) * {B} + (int)threadIdx.x;")
-        ap("    if (col < n_cols) {")
+        # block statistics of the float table (word BSTATS, 0: none): per row k
+        # and 16 columns, (max, finite |max|), for the search's group skipping
+        ap(f"    float2* BST = EV32 ? lcm_wp<float2>(it, {8 + len(tg.states)}) : nullptr;")
+        ap("    const int nb16 = (n_cols + 15) >> 4;")
+        ap(f"    const int col_t = (tile - tile_prefix[item]) * {B} + (int)threadIdx.x;")
+        ap("    const bool live = col_t < n_cols;")
+        ap("    const int col = live ? col_t : 0;")
+        ap("    {")
         # decode col -> det indices + cflat ; compute base offset per j
         ap("      const int cflat = col % cblk; int dr = col / cblk;")
         det_names = []
@@ -1717,7 +1724,7 @@ class RegimeKernels:
         ap(f"      for (int k0 = 0; k0 < {K}; k0 += {KC}) {{")
         ap(f"        double acc[{KC}];")
         ap(f"        #pragma unroll\n        for (int kk = 0; kk < {KC}; ++kk) acc[kk] = 0.0;")
-        ap(f"        for (int j = 0; j < {J}; ++j) {{")
+        ap(f"        for (int j = 0; j < (live ? {J} : 0); ++j) {{")
         ap("          int jr = j;")
         for pos in reversed(stoch):
             ax = tg.states[pos]
@@ -1735,8 +1742,14 @@ class RegimeKernels:
         ap(f"        #pragma unroll\n        for (int kk = 0; kk < {KC}; ++kk) {{")
         ap(f"          const int k = k0 + kk; if (k < {K}) {{")
         ap("            const double r = acc[kk] / Winv[k];")
-        ap("            EV64[(i64)k * n_cols + col] = r;")
-        ap("            if (EV32) EV32[(i64)k * n_cols + col] = (float)r;")
+        ap("            if (live) {")
+        ap("              EV64[(i64)k * n_cols + col] = r;")
+        ap("              if (EV32) EV32[(i64)k * n_cols + col] = (float)r;")
+        ap("            }")
+        ap("            if (BST) {  // uniform over the CTA (one item per tile)")
+        ap("              const float2 st = lcm_block16_stats(live ? (float)r : -lcm_lim<float>::inf());")
+        ap("              if (live && (threadIdx.x & 15) == 0) BST[(i64)k * nb16 + (col >> 4)] = st;")
+        ap("            }")
         ap("          }")
         ap("        }")
         ap("      }")

@@ -160,6 +160,26 @@ __device__ __forceinline__ T lcm_interp2(const S* __restrict__ blk, int n0, int 
   return acc;
 }
 
+// Block statistics of a float expectation row, for the exact skipping of
+// action groups in the single-precision search: over 16 consecutive columns
+// (16 consecutive threads of a warp), the maximum -- NaN when any value is NaN
+// -- and the largest |value| among the finite values.  Lanes without a column
+// pass -inf.  Every lane of the warp must call it.
+__device__ __forceinline__ float lcm_nanmax(float a, float b) {
+  return (a != a) ? a : ((b != b || b > a) ? b : a);
+}
+__device__ __forceinline__ float2 lcm_block16_stats(float x) {
+  float mx = x, ab = lcm_isfinite(x) ? fabsf(x) : 0.0f;
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    const float omx = __shfl_xor_sync(0xffffffffu, mx, o);
+    const float oab = __shfl_xor_sync(0xffffffffu, ab, o);
+    mx = lcm_nanmax(mx, omx);
+    ab = fmaxf(ab, oab);
+  }
+  return make_float2(mx, ab);
+}
+
 // Running (max, first argmax, nan) over feasible actions.
 template <typename T> struct LcmBest {
   T v;

@@ -162,10 +162,12 @@ __device__ __forceinline__ u32 lcm_kmajor_off(int r, int j, int rows) {
 // The expectation of one kernel launch.  `wfill(it, W)` writes the item's
 // FP64 weights W[k * J + j]; V' rows are `Vt + j * cblk + col` (targets whose
 // discrete axes are all stochastic).  Item words: 0 V' (double*), 2 EV32
-// (float*), 6 cblk, 7 n_cols.
+// (float*), 6 cblk, 7 n_cols, `bst_word` the block statistics of EV32 (per
+// row k and 16 columns, see lcm_block16_stats; 0: none).
 template <int K, int J, typename WFill>
 __device__ __forceinline__ void lcm_tc_expect(const i64* __restrict__ items, const int* __restrict__ tile_prefix,
-                                              int n_items, int n_tiles, int e_words, const WFill& wfill) {
+                                              int n_items, int n_tiles, int e_words, int bst_word,
+                                              const WFill& wfill) {
   using S = LcmTcShape<K, J>;
   constexpr int JP = S::JP, NP = S::NP, KC = S::KC;
   extern __shared__ unsigned char lcm_dsmem[];
@@ -282,28 +284,32 @@ __device__ __forceinline__ void lcm_tc_expect(const i64* __restrict__ items, con
       failed = true;
     } else {
       // ---- epilogue: row tid of D (TMEM lane tid) holds EV of column col
+      float2* BST = bst_word >= 0 ? lcm_wp<float2>(it, bst_word) : nullptr;
+      const int nb16 = (n_cols + 15) >> 4;
       const u32 lane_base = tmem + ((u32)(warp * 32) << 16);
 #pragma unroll
       for (int n0 = 0; n0 < NP; n0 += 16) {
         float d[16];
         lcm_tmem_ld16(lane_base + (u32)n0, d);
-        if (live && !nonfinite) {
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const int k = n0 + q;
-            if (k < K) EV32[(i64)k * n_cols + col] = d[q] * Wscale[k];
+        for (int q = 0; q < 16; ++q) {
+          const int k = n0 + q;
+          if (k >= K) continue;
+          float e = d[q] * Wscale[k];
+          if (live && nonfinite) {  // FP64, zero-safe, node by node
+            double num = 0.0, sw = 0.0;
+            for (int j = 0; j < J; ++j) {
+              const double w = Wd[k * J + j];
+              sw += w;
+              num += lcm_zs(w, Vt[(i64)j * cblk + col]);
+            }
+            e = (float)(num / (sw > 0.0 ? sw : 1.0));
           }
-        }
-      }
-      if (live && nonfinite) {  // FP64, zero-safe, node by node
-        for (int k = 0; k < K; ++k) {
-          double num = 0.0, sw = 0.0;
-          for (int j = 0; j < J; ++j) {
-            const double w = Wd[k * J + j];
-            sw += w;
-            num += lcm_zs(w, Vt[(i64)j * cblk + col]);
+          if (live) EV32[(i64)k * n_cols + col] = e;
+          if (BST) {  // uniform over the CTA (one item per tile)
+            const float2 st = lcm_block16_stats(live ? e : -lcm_lim<float>::inf());
+            if (live && (tid & 15) == 0) BST[(i64)k * nb16 + (col >> 4)] = st;
           }
-          EV32[(i64)k * n_cols + col] = (float)(num / (sw > 0.0 ? sw : 1.0));
         }
       }
     }
