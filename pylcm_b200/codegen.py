@@ -312,6 +312,7 @@ class TargetPlan:
     w_coord: int = -1
     w_scalar: int = -1
     w_vraw: int = -1
+    w_bst: int = -1
     unreachable: bool = False  # no law for one of the target's states
 
     @property
@@ -377,6 +378,7 @@ class LaunchConfig:
     chunk: int = 512  # actions per shared-memory table chunk
     sb: int = 1  # states per thread (register blocking)
     min_blocks: int = 0  # __launch_bounds__ min CTAs per SM (0 = compiler's choice)
+    prune: bool = True  # single-precision search: exact skipping of action groups where eligible
 
     @property
     def states_per_tile(self) -> int:
@@ -446,6 +448,8 @@ class RegimeKernels:
                 # the target's value array itself (node-by-node reads in the
                 # simulation, for process values outside the process grid)
                 t.w_vraw = take()
+                # block statistics of the float table (group skipping; 0: none)
+                t.w_bst = take()
         self.n_words = max(w, 1)
 
     # -------------------------------------------------------------- source
@@ -736,6 +740,8 @@ class RegimeKernels:
             loads.append(f"ev{ti} = lcm_evsel<E>::get(it, {t.w_ev64}, {t.w_ev32});")
             ap(f"  const double* vr{ti};")
             loads.append(f"vr{ti} = lcm_wp<const double>(it, {t.w_vraw});")
+            ap(f"  const float2* bst{ti};")
+            loads.append(f"bst{ti} = lcm_wp<const float2>(it, {t.w_bst});")
             for pos in t.det_pos + t.cont_pos:
                 ap(f"  int n{ti}_{pos};")
                 loads.append(f"n{ti}_{pos} = lcm_wi(it, {t.w_sizes + pos});")
@@ -1007,6 +1013,7 @@ class RegimeKernels:
             f"{self.bellman_name()}(const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, int n_tiles) {{"
         )
         ap("  extern __shared__ __align__(16) unsigned char lcm_smem[];")
+        gumax_at = len(L)  # a per-group utility maximum is declared here when groups are skipped
         ap(f"  {TT}* tabf = reinterpret_cast<{TT}*>(lcm_smem);")
         ap(f"  int* tabi = reinterpret_cast<int*>(lcm_smem + {NF * CH * (4 if fp32 else 8)});")
         ap("  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {")
@@ -1120,6 +1127,157 @@ class RegimeKernels:
             o.append("}")
             return o
 
+        # ---- exact skipping of action groups (single-precision search)
+        G = max(16, LANES)
+
+        def provider(n, kb: str) -> str | None:
+            """Kernel-scope expression of a hoisted boundary node (double)."""
+            if isinstance(n, ir.Expr) and n.op == "const":
+                return f"((double){_c_float(float(n.args[0]), 'double')})"
+            for lst, fmt in ((bP, "PVd[{i}]"), (bD, "DV[{i}]"), (bS, "SV[" + kb + "][{i}]"),
+                             (bSD, "SDV[" + kb + "][{i}]")):
+                for i, m in enumerate(lst):
+                    if m is n:
+                        return fmt.format(i=i)
+            return None
+
+        def prune_info(ti: int):
+            if not fp32 or taste or spec.terminal or not self.cfg.prune:
+                return None
+            t = self.targets[ti]
+            if t.scalar or t.unreachable or t.det_pos or len(t.cont_pos) != 1:
+                return None
+            pos = t.cont_pos[0]
+            if (ti, pos) not in self._affine:
+                return None
+            x0, gr, cv = self._affine[(ti, pos)]
+            U = ir.const(self.tr.U)
+            ia = {id(n): i for i, n in enumerate(bA)}
+            if not isinstance(U, ir.Expr) or id(U) not in ia or slot[ia[id(U)]][0] != "F":
+                return None
+            if id(cv) not in ia or slot[ia[id(cv)]][0] != "F":
+                return None
+            beta = ir.const(self.tr.beta)
+            pb = provider(beta, "kb")
+            if pb is None or not pb.startswith("PVd"):
+                return None
+            px0, pg = provider(ir.const(x0), "kb"), provider(ir.const(gr), "kb")
+            if px0 is None or pg is None:
+                return None
+            key = "0"
+            for kind, name, size in t.key_vars:
+                iv = f"SI[kb][{[a.name for a in dstates].index(name)}]" if kind == "state" else f"DI_{name}"
+                key = f"({key}) * {size} + {iv}"
+            return {"uf": slot[ia[id(U)]][1], "cvf": slot[ia[id(cv)]][1], "beta": pb, "x0": px0, "g": pg,
+                    "key": key, "n": f"C.n{ti}_{pos}", "a": f"C.a{ti}_0", "b": f"C.b{ti}_0", "bst": f"C.bst{ti}"}
+
+        def inner_loop_pruned(sa_fn: str, pi: dict) -> list[str]:
+            """inner_loop with exact skipping of groups of G consecutive
+            continuous actions.  Per state, an upper bound of Q over a group
+            -- the group's largest utility (from the action table) plus beta
+            times the largest expectation-table value among the cells the
+            group's coordinates can read (from the table's block statistics),
+            plus a rounding margin -- is compared with the state's current
+            second-best value (or the second best of a pilot pass over the
+            group midpoints, which is never above the final second best).  A
+            group whose bound is below it cannot enter the top two: skipping
+            it leaves the search's two candidates, and so V and the policy,
+            exactly as without skipping.  Every lane still visits its own
+            actions in increasing order.  Groups whose coordinates leave
+            [0.5, n - 1.5] (extrapolation), NaN bounds and negative beta are
+            never skipped."""
+            o = []
+            di_args = "".join(f"DI_{a.name}, " for a in dacts)
+            call = f"{sa_fn}<float, float>(C, PV, PVd, DV, SV[kb], SDV[kb], af, SI[kb], {di_args}period, age, q)"
+            o.append(f"const float beta_f = (float)({pi['beta'].replace('kb', '0')});")
+            o.append(f"const bool pr_on = {pi['bst']} != nullptr && beta_f >= 0.0f;")
+            o.append(f"const int n_c = {pi['n']};")
+            o.append("const int nb16 = (n_c + 15) >> 4;")
+            o.append("const float c_hi_lim = (float)(n_c - 1) - 0.5f;")
+            o.append(f"float Kc[{SB}], Mc[{SB}]; int keyr[{SB}];")
+            o.append(f"#pragma unroll\nfor (int kb = 0; kb < {SB}; ++kb) {{")
+            o.append(f"  Kc[kb] = ((float)({pi['x0']}) - {pi['a']}) * {pi['b']};")
+            o.append(f"  Mc[kb] = (float)({pi['g']}) * {pi['b']};")
+            o.append(f"  keyr[kb] = {pi['key']};")
+            o.append("}")
+            o.append(f"for (int c0 = 0; c0 < n_ac; c0 += {CH}) {{")
+            o.append(f"  const int cn = min({CH}, n_ac - c0);")
+            o.append("  __syncthreads();")
+            o.append(f"  for (int j = threadIdx.x; j < cn; j += {B}) {{")
+            o.append("    const i64 a = (i64)ad * n_ac + c0 + j;")
+            for k in range(nf):
+                o.append(f"    tabf[{k} * {CH} + j] = ({TT})atf[(i64){k} * n_actions + a];")
+            for k in range(ni):
+                o.append(f"    tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
+            o.append("  }")
+            o.append("  __syncthreads();")
+            o.append(f"  const int ng = (cn + {G - 1}) / {G};")
+            o.append(f"  for (int g = threadIdx.x; g < ng; g += {B}) {{")
+            o.append("    float m = -lcm_lim<float>::inf();")
+            o.append(f"    const int j1 = min(cn, g * {G} + {G});")
+            o.append(f"    for (int j = g * {G}; j < j1; ++j) m = lcm_nanmax(m, tabf[{pi['uf']} * {CH} + j]);")
+            o.append("    gumax[g] = m;")
+            o.append("  }")
+            o.append("  __syncthreads();")
+            o.append(f"  float thr[{SB}];")
+            o.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) "
+                     "thr[kb] = best[kb].idx2 >= 0 ? best[kb].v2 : -lcm_lim<float>::inf();")
+            o.append("  if (pr_on) {")
+            o.append(f"    float p1[{SB}], p2[{SB}];")
+            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) p1[kb] = p2[kb] = -lcm_lim<float>::inf();")
+            o.append(f"    for (int g = lane; g < ng; g += {LANES}) {{")
+            o.append(f"      const int j = min(g * {G} + {G // 2}, cn - 1);")
+            o.append(f"      AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
+            o.append(f"      #pragma unroll\n      for (int kb = 0; kb < {SB}; ++kb) {{")
+            o.append("        float q;")
+            o.append(f"        if (act[kb] && {call} && q > p2[kb]) {{")
+            o.append("          if (q > p1[kb]) { p2[kb] = p1[kb]; p1[kb] = q; } else { p2[kb] = q; }")
+            o.append("        }")
+            o.append("      }")
+            o.append("    }")
+            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) thr[kb] = fmaxf(thr[kb], p2[kb]);")
+            o.append("  }")
+            o.append("  for (int g = 0; g < ng; ++g) {")
+            o.append(f"    const int j0 = g * {G}, j1 = min(cn, j0 + {G});")
+            o.append(f"    bool run[{SB}]; bool any = false;")
+            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
+            o.append("      bool skip = false;")
+            o.append("      if (pr_on && act[kb]) {")
+            o.append("        const float um = gumax[g];")
+            o.append(f"        const float cva = tabf[{pi['cvf']} * {CH} + j0], cvb = tabf[{pi['cvf']} * {CH} + j1 - 1];")
+            o.append("        const float ca = Kc[kb] + Mc[kb] * cva, cb = Kc[kb] + Mc[kb] * cvb;")
+            o.append("        const float lo = fminf(ca, cb), hi = fmaxf(ca, cb);")
+            o.append("        if (ca == ca && cb == cb && lo >= 0.5f && hi <= c_hi_lim) {")
+            o.append("          const int L0 = max((int)lo - 1, 0), H1 = min((int)hi + 2, n_c - 1);")
+            o.append(f"          const float2* row = {pi['bst']} + (i64)keyr[kb] * nb16;")
+            o.append("          float mx = -lcm_lim<float>::inf(), ab = 0.0f;")
+            o.append("          for (int b = L0 >> 4; b <= (H1 >> 4); ++b) {")
+            o.append("            const float2 st = __ldg(row + b);")
+            o.append("            mx = lcm_nanmax(mx, st.x);")
+            o.append("            ab = fmaxf(ab, st.y);")
+            o.append("          }")
+            o.append("          const float ub = um + beta_f * mx;")
+            o.append("          const float marg = 3.8e-6f * (fabsf(um) + beta_f * ab);")
+            o.append("          skip = ub + marg < thr[kb];")
+            o.append("        }")
+            o.append("      }")
+            o.append("      run[kb] = act[kb] && !skip;")
+            o.append("      any = any || run[kb];")
+            o.append("    }")
+            o.append("    if (!any) continue;")
+            o.append(f"    for (int j = j0 + lane; j < j1; j += {LANES}) {{")
+            o.append(f"      AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
+            o.append("      const int aidx = ad * n_ac + c0 + j;")
+            o.append(f"      #pragma unroll\n      for (int kb = 0; kb < {SB}; ++kb) {{")
+            o.append("        float q;")
+            o.append(f"        if (run[kb] && {call}) best[kb].push(q, aidx);")
+            o.append("      }")
+            o.append("    }")
+            o.append("  }")
+            o.append("}")
+            return o
+
+        any_pruned = False
         if unswitch:
             rid_expr = f"(int)PVd[{[id(x) for x in bP].index(id(self.tr.regime_id))}]" if rid_phase == "P" else None
             if rid_phase == "D":
@@ -1129,7 +1287,11 @@ class RegimeKernels:
             for ti, t in enumerate(self.targets):
                 ap(f"      {'if' if first else 'else if'} (rid == {t.spec.rid}) {{")
                 first = False
-                for s_ in inner_loop(SA.format(ti + 1)):
+                pi = prune_info(ti)
+                if pi is not None:
+                    any_pruned = True
+                body = inner_loop(SA.format(ti + 1)) if pi is None else inner_loop_pruned(SA.format(ti + 1), pi)
+                for s_ in body:
                     ap("        " + s_)
                 ap("      }")
             ap("      else {")
@@ -1140,6 +1302,9 @@ class RegimeKernels:
             for s_ in inner_loop(SA.format(0)):
                 ap("      " + s_)
         ap("    }")
+        if any_pruned:
+            L.insert(gumax_at, f"  __shared__ float gumax[{(CH + G - 1) // G}];")
+        self.prunes_groups = any_pruned
 
         # ---- reduction and epilogue
         def final_eval(a_var: str, out_var: str, loc: str) -> list[str]:

@@ -376,6 +376,7 @@ class SolvePlan:
                     self._vck[t.spec.name] = eng.value_carry_kernel(t.spec, t.value_euler, params_list[0])
 
         # EV buffers per (source, target set, target)
+        self.bst: dict[tuple, Any] = {}
         for period, s, targets, rk in step_list:
             if not isinstance(rk, RegimeKernels):
                 continue
@@ -392,6 +393,10 @@ class SolvePlan:
                 e64 = torch.empty((n, t.K, ncols), dtype=torch.float64, device=dev)
                 e32 = torch.empty((n, t.K, ncols), dtype=torch.float32, device=dev) if fp32 else None
                 self.ev[k] = (e64, e32, ncols, cblk)
+                # block statistics of the float table rows (max, finite |max|
+                # per 16 columns) for the search's exact group skipping
+                if fp32 and not t.det_pos:
+                    self.bst[k] = torch.empty((n, t.K, (ncols + 15) // 16, 2), dtype=torch.float32, device=dev)
 
         # action tables (kernel a0 output) per (regime, target set), reused across periods
         self.atab: dict[tuple, Any] = {}
@@ -451,11 +456,13 @@ class SolvePlan:
             if not (t.needs_contraction or fp32):
                 continue
             e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
+            bst = self.bst.get((s.name, targets, t.spec.name))
             Vt = self.V[t.spec.name]
             tslot = self.slot[t.spec.name][period + 1]
             recs = []
             for i in range(n):
                 r = np.zeros(rk.e_words_for(t), dtype=np.int64)
+                r[8 + len(t.spec.states)] = bst[i].data_ptr() if bst is not None else 0
                 r[0] = Vt[i, tslot].data_ptr()
                 r[1] = e64[i].data_ptr()
                 r[2] = e32[i].data_ptr() if e32 is not None else 0
@@ -506,6 +513,8 @@ class SolvePlan:
                     e64, e32, ncols, cblk = self.ev[(s.name, targets, t.spec.name)]
                     r[t.w_ev64] = e64[i].data_ptr()
                     r[t.w_ev32] = e32[i].data_ptr() if e32 is not None else 0
+                    bst = self.bst.get((s.name, targets, t.spec.name))
+                    r[t.w_bst] = bst[i].data_ptr() if bst is not None else 0
                 else:
                     r[t.w_ev64] = tV[i, tslot].data_ptr()
                     r[t.w_ev32] = 0

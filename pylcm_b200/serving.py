@@ -84,8 +84,8 @@ class Result:
 def solve_bytes(eng: SolveEngine) -> int:
     """HBM bytes one solve instance (a pool slot) of `eng`'s model holds:
     T x states value (float64) and policy (int32) arrays per regime, the
-    expectation tables (float64, plus float32 copies in the single-precision
-    search), the action tables, the DC-EGM carry rows (two-period ring) and
+    expectation tables (float64, plus float32 copies and their block
+    statistics in the single-precision search), the action tables, the DC-EGM carry rows (two-period ring) and
     candidates, and the marginal-value rows of regimes DC-EGM reads as value
     arrays."""
     from pylcm_b200.egm import is_egm
@@ -112,7 +112,9 @@ def solve_bytes(eng: SolveEngine) -> int:
         # expectation tables of the targets (at most one per target and target set)
         for t in specs:
             if t.states and not s.terminal:
-                b += t.n_states * (8 + (4 if fp32 else 0))
+                # double table, float copy and its block statistics (8 B per
+                # 16 columns) in the single-precision search
+                b += t.n_states * 8 + (t.n_states * 4 + -(-t.n_states // 16) * 8 if fp32 else 0)
         b += 4 * s.n_actions * 4  # action table
     return int(b)
 
