@@ -1142,7 +1142,10 @@ class RegimeKernels:
             return None
 
         def prune_info(ti: int):
-            if not fp32 or taste or spec.terminal or not self.cfg.prune:
+            # one continuous action: within a group of consecutive inner
+            # actions its value is monotone, so the group's coordinates lie
+            # between those of its first and last action
+            if not fp32 or taste or spec.terminal or not self.cfg.prune or len(cacts) != 1:
                 return None
             t = self.targets[ti]
             if t.scalar or t.unreachable or t.det_pos or len(t.cont_pos) != 1:
