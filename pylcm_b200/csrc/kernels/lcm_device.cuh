@@ -395,12 +395,47 @@ __device__ __forceinline__ void lcm_bracket_read(double x0, double x1, double f0
   slope_val = s;
 }
 
+// lcm_row_bracket for the 32 converged lanes of a warp reading the same
+// sorted row (same xp and L on every lane; `xq` per lane): the brackets of
+// the warp's smallest and largest query bound every lane's bracket, so when
+// at most 32 nodes lie between them each lane counts the nodes at or below
+// its query among those (held one per lane, searched through shuffles)
+// instead of searching the row in memory.  The result equals
+// lcm_row_bracket's on every lane (a NaN query gets L - 1, as there); with a
+// wider window every lane falls back to its own search.
+__device__ __forceinline__ int lcm_row_bracket_warp(const double* __restrict__ xp, int L, double xq) {
+  const unsigned full = 0xffffffffu;
+  double qmin = xq, qmax = xq;  // fmin / fmax skip NaN queries
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    qmin = fmin(qmin, __shfl_xor_sync(full, qmin, o));
+    qmax = fmax(qmax, __shfl_xor_sync(full, qmax, o));
+  }
+  if (qmin != qmin) return L - 1;  // every query is NaN
+  const int i_lo = lcm_row_bracket(xp, L, qmin);
+  const int i_hi = lcm_row_bracket(xp, L, qmax);
+  const int W = i_hi - i_lo;  // nodes in (i_lo, i_hi]
+  if (W > 32) return xq != xq ? L - 1 : lcm_row_bracket(xp, L, xq);
+  const int lane = threadIdx.x & 31;
+  const double node = lane < W ? xp[i_lo + 1 + lane] : LCM_INF;
+  int lo = 0, hi = W;
+#pragma unroll
+  for (int s = 0; s < 6; ++s) {
+    const int mid = (lo + hi) >> 1;
+    const double x = __shfl_sync(full, node, mid & 31);
+    if (lo < hi) {
+      if (x > xq) hi = mid; else lo = mid + 1;
+    }
+  }
+  return xq != xq ? L - 1 : i_lo + lo;
+}
+
 __device__ __forceinline__ void lcm_row_read(const double* __restrict__ xp, const double* __restrict__ fp,
                                              const double* __restrict__ dp, int L, double xq,
-                                             double& val, double& slope_val) {
+                                             double& val, double& slope_val, bool warp_uniform = false) {
   if (L <= 0) { val = slope_val = LCM_NAN; return; }
   if (L == 1) { val = fp[0]; slope_val = dp ? dp[0] : LCM_NAN; return; }
-  const int idx = lcm_row_bracket(xp, L, xq);
+  const int idx = warp_uniform ? lcm_row_bracket_warp(xp, L, xq) : lcm_row_bracket(xp, L, xq);
   if (idx >= L - 1) { val = fp[L - 1]; slope_val = dp ? dp[L - 1] : LCM_NAN; return; }
   const int b = idx < 0 ? 0 : idx;
   lcm_bracket_read(xp[b], xp[b + 1], fp[b], fp[b + 1], dp ? dp[b] : 0.0, dp ? dp[b + 1] : 0.0, dp != nullptr, idx, xq,

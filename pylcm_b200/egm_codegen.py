@@ -94,6 +94,20 @@ class EgmKernels:
             prov[id(ir.var(kind, a.name, "i"))] = f"dc_{a.name}"
         return prov
 
+    @staticmethod
+    def _row_exprs(t) -> list:
+        """Expressions that decide which carry rows a continuation read
+        touches and with what weight: the regime probability and the laws of
+        the target's discrete states."""
+        out = [t.prob]
+        for ax in [a for a in t.spec.states if a.kind != "continuous"]:
+            law = t.disc_laws[ax.name]
+            if law.kind == "markov":
+                out += list(law.expr.items)
+            elif law.kind == "det":
+                out.append(law.expr)
+        return [x for x in out if isinstance(ir.const(x), ir.Expr)]
+
     def _weights(self, body: list, ti: int, t, names: dict) -> list:
         """Emit the weight vector of every discrete state of target `t`
         (process row, Markov row or one-hot deterministic law)."""
@@ -190,9 +204,15 @@ class EgmKernels:
         ap(f"    const int n_sav = lcm_wi(it, {self.W_NSAV});")
         ap(f"    const int nc = {er.n_constrained};")
         ap("    const int n_cand = nc + n_sav;")
-        ap("    const int e = (tile - tile_prefix[item]) * 256 + (int)threadIdx.x;")
-        ap(f"    if (e >= {nrow} * n_sav) continue;")
+        ap("    const int e_t = (tile - tile_prefix[item]) * 256 + (int)threadIdx.x;")
+        # lanes past the end repeat the last element (their results are not
+        # written) so that every warp stays converged for the shared reads
+        ap(f"    const bool live = e_t < {nrow} * n_sav;")
+        ap(f"    const int e = live ? e_t : {nrow} * n_sav - 1;")
         ap("    const int row = e / n_sav, j = e % n_sav;")
+        # one candidate row for the whole warp: its carry-row reads share
+        # their bracket search (lcm_row_bracket_warp)
+        ap("    const bool warp_row = __all_sync(0xffffffffu, live && row == __shfl_sync(0xffffffffu, row, 0));")
         body: list[str] = []
         prov = dict(base_prov)
         prov.update(self._row_decode(body, "row"))
@@ -261,7 +281,13 @@ class EgmKernels:
                 body.append(f"      for (int d = 0; d < {nd_t}; ++d) {{")
                 body.append(f"        const i64 crow = (i64)jc * {nd_t} + d;")
                 body.append("        const int Lk = min(NK[crow], npad);")
-                body.append("        lcm_row_read(RG + crow * npad, RV + crow * npad, RM + crow * npad, NK[crow] > npad ? 0 : Lk, Rn, vals[d], mus[d]);")
+                # the shared search needs the row's control flow to be the
+                # same on every lane: the regime probability and the node
+                # weights must not depend on the savings node
+                uniform = not any(n is A_VAR for n in ir.topo_order([ir.const(x) for x in self._row_exprs(t)]))
+                flag = "warp_row" if uniform else "false"
+                body.append("        lcm_row_read(RG + crow * npad, RV + crow * npad, RM + crow * npad, NK[crow] > npad ? 0 : Lk, "
+                            f"Rn, vals[d], mus[d], {flag});")
                 body.append("      }")
                 if tg.taste_shocks:
                     body.append("      double vmax = -LCM_INF;")
@@ -311,10 +337,10 @@ class EgmKernels:
         body.append(f"double* CC = lcm_wp<double>(it, {self.W_CC}) + (i64)row * n_cand;")
         body.append(f"double* CV = lcm_wp<double>(it, {self.W_CV}) + (i64)row * n_cand;")
         body.append(f"double* CS = lcm_wp<double>(it, {self.W_CS}) + (i64)row * n_cand;")
-        body.append("{ const bool dead = vj == -LCM_INF;")
+        body.append("if (live) { const bool dead = vj == -LCM_INF;")
         body.append("  CG[nc + j] = dead ? LCM_NAN : mj; CC[nc + j] = dead ? LCM_NAN : cj;")
         body.append("  CV[nc + j] = dead ? LCM_NAN : vj; CS[nc + j] = dead ? LCM_NAN : A; }")
-        body.append("if (j == 0) {")
+        body.append("if (live && j == 0) {")
         body.append(f"  lcm_wp<double>(it, {self.W_EV0})[row] = EV;")
         body.append(f"  const int ng = lcm_wi(it, {self.W_NGRID});")
         body.append(f"  const double Rmax = lcm_wp<const double>(it, {self.W_GRID})[ng - 1];")
