@@ -8,7 +8,10 @@ own units on its own GPU.  What crosses ranks is bookkeeping only:
   (largest first onto the least-loaded rank);
 - `max_over_ranks`: the job's time is the slowest rank's (one all-reduce of
   a scalar);
-- `gather_to_root`: per-unit results (moments, summaries) collected on rank 0.
+- `gather_to_root`: per-unit results (moments, summaries) collected on rank 0;
+- `serve_partitioned`: the multi-GPU front end of the serving loop -- every
+  rank holds the same request stream, serves the requests the footprint
+  partition gives it on its own GPU, and rank 0 receives every result.
 
 The process group is `torch.distributed` with NCCL on GPUs (gloo on CPUs).
 """
@@ -62,3 +65,31 @@ def gather_to_root(items: dict[int, Any]) -> dict[int, Any] | None:
             raise ValueError(f"units {sorted(overlap)} reported by two ranks")
         merged.update(part)
     return merged
+
+
+def serve_partitioned(requests: Sequence, server, realtime: bool = False) -> tuple[dict | None, float]:
+    """One rank's part of a serving job spread over the ranks of the default
+    process group (one process per GPU).
+
+    Every rank passes the same `requests`; `partition` assigns them by
+    `server.footprint(request)` (HBM bytes of a solve + simulate), each rank
+    serves its share with `server.run` on its own GPU -- no exchange on the
+    data path -- and the results are gathered on rank 0.  Returns
+    ({request index: result} on rank 0, None elsewhere; the job's wall time,
+    the slowest rank's)."""
+    import time
+
+    import torch.distributed as dist
+
+    ready = dist.is_available() and dist.is_initialized()
+    world = dist.get_world_size() if ready else 1
+    rank = dist.get_rank() if ready else 0
+    fps = [int(server.footprint(r)) for r in requests]
+    mine = partition(fps, world)[rank]
+    t0 = time.perf_counter()
+    results = server.run([requests[i] for i in mine], realtime=realtime) if mine else []
+    wall = time.perf_counter() - t0
+    device = "cuda" if ready and dist.get_backend() == "nccl" else None
+    wall = max_over_ranks(wall, device=device)
+    merged = gather_to_root({i: res for i, res in zip(mine, results)})
+    return merged, wall
