@@ -8,9 +8,21 @@ regime and next states (deterministic laws, Markov draws,
 ``next_state.py:301-341``, and process draws, ``processes/ar1.py:122-132``,
 ``processes/iid.py``).
 
-Random numbers: the same counter-based Philox-4x32-10 stream as the GPU
-kernel (counter = (subject, period, stream id, 0), key = the seed), restated
-here in NumPy, so GPU and oracle paths can be compared draw for draw.
+Random numbers, two streams:
+
+- ``rng="philox"``: the counter-based Philox-4x32-10 stream of the GPU
+  kernel's serving form (counter = (subject, period, stream id, 0), key = the seed),
+  restated in NumPy, so GPU and oracle paths can be compared draw for draw;
+- ``rng="jax"`` (default): the reference's own stream (``pylcm_b200.jaxrng``, JAX's
+  Threefry-2x32 with its key threading): ``key(seed)``; per period, per active
+  regime in declaration order, the taste-shock keys (``simulate.py:562-572``)
+  and then ``split(key, 3)`` into the next-state key, the regime key and the
+  running key (``simulate.py:630``); per subject, one key per stochastic
+  next-state function (sorted qualified names, ``transitions.py:111-125``)
+  and one for the regime draw (``transitions.py:260-275``); the samplers of
+  ``jax.random`` (``choice`` with weights, ``normal``, ``uniform``,
+  ``bernoulli``, ``gumbel``).  This stream reproduces the reference's stored
+  stochastic simulations.
 """
 
 from __future__ import annotations
@@ -86,8 +98,51 @@ def categorical(p: np.ndarray, u: np.ndarray) -> np.ndarray:
     return np.where(none, p.shape[1] - 1, idx)
 
 
-def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
-    """Per period: regime_id, value, states, actions (NaN where not defined)."""
+class _JaxStream:
+    """The reference's key threading over one simulation (``rng="jax"``)."""
+
+    def __init__(self, seed: int, n: int) -> None:
+        from pylcm_b200 import jaxrng
+
+        self.J = jaxrng
+        self.key = jaxrng.key(seed)
+        self.n = n
+
+    def taste_keys(self):
+        self.key, d = self.J.simulation_keys(self.key, ["taste_shock"], self.n)
+        return d["taste_shock"]
+
+    def split3(self):
+        ks = self.J.split(self.key, 3)
+        self.key = ks[2]
+        return ks[0], ks[1]
+
+
+def _reachable_targets(spec, specs, res, model) -> list:
+    """Targets the regime's transition reaches with positive probability in
+    some period (the reference's simulation reachability)."""
+    from pylcm_b200.validation import _regime_probs
+
+    out = set()
+    for period in spec.active_periods:
+        if period + 1 >= model.n_periods:
+            continue
+        P, _ = _regime_probs(spec, specs, res, period, float(model.ages.values[period]))
+        for s in specs:
+            if np.any(np.nan_to_num(P[:, s.rid]) > 0):
+                out.add(s.name)
+    return [s for s in specs if s.name in out]
+
+
+def _erfinv(u):
+    from scipy.special import erfinv
+
+    return erfinv(u)
+
+
+def simulate(model, params, initial_conditions, seed: int = 0, V=None, rng: str = "jax") -> dict:
+    """Per period: regime_id, value, states, actions (NaN where not defined).
+    `rng` selects the random stream (see the module docstring)."""
     specs = model.regime_specs
     res = ParamResolver(params, model.fixed_params, tuple(s.name for s in specs))
     if V is None:
@@ -111,6 +166,11 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
         S[k] = np.asarray(v, dtype=np.float64).copy()
     out = {}
     by_id = {s.rid: s for s in specs}
+    jax_rng = rng == "jax"
+    stream = _JaxStream(seed, N) if jax_rng else None
+    # the reference walks the active regimes in declaration order
+    order = [next(s for s in specs if s.name == nm) for nm in model.user_regimes] if jax_rng else specs
+    reach = {s.name: _reachable_targets(s, specs, res, model) for s in specs if not s.terminal} if jax_rng else {}
     for period in range(T):
         age = float(model.ages.values[period])
         val = np.full(N, np.nan)
@@ -118,10 +178,16 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
         newR = np.full(N, -1, dtype=np.int64)
         newS = {n: np.full(N, np.nan) for n in snames}
         nxt = V.get(period + 1, {})
-        for spec in specs:
+        for spec in order:
             if period not in spec.active_periods:
                 continue
             sel = np.nonzero(rid == spec.rid)[0]
+            jk = None
+            if jax_rng:
+                # every active regime advances the running key, members or not
+                jk = {"taste": stream.taste_keys() if spec.taste_shocks else None}
+                if not spec.terminal:
+                    jk["states"], jk["regime"] = stream.split3()
             if sel.size == 0:
                 continue
             rng = Rng(seed, period, sel)
@@ -135,7 +201,14 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
                 Qd = Qm.reshape(len(sel), nd, nc)
                 cont_arg = Qd.argmax(axis=2)
                 Qc = Qd.max(axis=2)
-                noise = np.stack([scale * (rng.gumbel(64 + d) - EULER_GAMMA) for d in range(nd)], axis=1)
+                if jax_rng:
+                    # jax.random.gumbel(key, (nd,)): one uniform per discrete
+                    # cell from the counters (0, d) of the subject's key
+                    from pylcm_b200 import jaxrng
+
+                    noise = scale * (jaxrng.gumbel_shaped(jk["taste"][sel], nd) - EULER_GAMMA)
+                else:
+                    noise = np.stack([scale * (rng.gumbel(64 + d) - EULER_GAMMA) for d in range(nd)], axis=1)
                 noisy = Qc + noise  # -inf stays -inf, a NaN cell is NaN (argmax: first NaN)
                 dstar = noisy.argmax(axis=1)
                 aa = dstar * nc + cont_arg[np.arange(len(sel)), dstar]
@@ -161,11 +234,29 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
             targets = tuple(s.name for s in specs if (period + 1) in s.active_periods)
             tr = trace_regime(spec, specs, res, targets)
             env = _eval_env(spec, sv, chosen, period, age, res)
+            skeys = None
+            if jax_rng:
+                from pylcm_b200 import jaxrng
+
+                tr_all = trace_regime(spec, specs, res, tuple(t.name for t in reach[spec.name]))
+                qnames = sorted(
+                    f"{t}__next_{nm}"
+                    for t, laws in tr_all.next_states.items() if laws is not None
+                    for nm, law in laws.items() if law.kind in ("markov", "process")
+                )
+                _, skeys = jaxrng.simulation_keys(jk["states"], qnames, N)
+                _, rkeys = jaxrng.simulation_keys(jk["regime"], ["regime_transition"], N)
             if tr.regime_id is not None:
                 r_new = np.broadcast_to(_ev(tr.regime_id, env, tr), (len(sel),)).astype(np.int64)
             else:
                 probs = np.stack([np.broadcast_to(_ev(p, env, tr), (len(sel),)) for p in tr.regime_probs], axis=1)
-                r_new = categorical(probs, rng.uniform(0))
+                if jax_rng:
+                    # choice over the regimes active next period, by regime id
+                    cand = [s.rid for s in specs if s.name in targets]
+                    k = jaxrng.choice_index(rkeys["regime_transition"][sel], probs[:, cand])
+                    r_new = np.asarray(cand, dtype=np.int64)[k]
+                else:
+                    r_new = categorical(probs, rng.uniform(0))
             newR[sel] = r_new
             for tname in targets:
                 tgt = next(s for s in specs if s.name == tname)
@@ -178,7 +269,12 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
                         x = np.broadcast_to(_ev(law.expr, env, tr), (len(sel),)).astype(np.float64)
                     elif law.kind == "markov":
                         p = np.stack([np.broadcast_to(_ev(it, env, tr), (len(sel),)) for it in law.expr.items], axis=1)
-                        x = categorical(p, rng.uniform(1 + k)).astype(np.float64)
+                        if jax_rng:
+                            x = jaxrng.choice_index(skeys[f"{tname}__next_{ax.name}"][sel], p).astype(np.float64)
+                        else:
+                            x = categorical(p, rng.uniform(1 + k)).astype(np.float64)
+                    elif jax_rng:
+                        x = _jax_process_draw(spec, law, res, sv, skeys[f"{tname}__next_{ax.name}"][sel])
                     else:
                         grid = spec.state(law.source_process).grid
                         pp = res.process_params(spec.name, law.source_process, grid)
@@ -205,6 +301,33 @@ def simulate(model, params, initial_conditions, seed: int = 0, V=None) -> dict:
         rid = newR
         S = newS
     return out
+
+
+def _jax_process_draw(spec, law, res, sv, keys):
+    """The reference's process draws (``processes/ar1.py:122-132, 191-201,
+    305-319``, ``processes/iid.py:58-65, 135-140, 201-206, 286-298``) from
+    the subjects' keys."""
+    from pylcm_b200 import jaxrng
+
+    grid = spec.state(law.source_process).grid
+    pp = {k: float(v) for k, v in res.process_params(spec.name, law.source_process, grid).items()}
+    cls = type(grid).__name__
+    y = sv[law.source_process]
+    if cls in ("TauchenAR1Process", "RouwenhorstAR1Process"):
+        return pp["mu"] + pp["rho"] * y + pp["sigma"] * jaxrng.normal(keys, _erfinv)
+    if cls == "NormalIIDProcess":
+        return pp["mu"] + pp["sigma"] * jaxrng.normal(keys, _erfinv)
+    if cls == "LogNormalIIDProcess":
+        return np.exp(pp["mu"] + pp["sigma"] * jaxrng.normal(keys, _erfinv))
+    if cls == "UniformIIDProcess":
+        return jaxrng.uniform(keys, pp["start"], pp["stop"])
+    if cls in ("TauchenNormalMixtureAR1Process", "NormalMixtureIIDProcess"):
+        k2 = jaxrng.split(keys, 2)
+        comp = jaxrng.bernoulli(k2[..., 0, :], pp["p1"])
+        z = jaxrng.normal(k2[..., 1, :], _erfinv)
+        eps = np.where(comp, pp["mu1"] + pp["sigma1"] * z, pp["mu2"] + pp["sigma2"] * z)
+        return eps if cls == "NormalMixtureIIDProcess" else pp["mu"] + pp["rho"] * y + eps
+    raise NotImplementedError(cls)
 
 
 def _eval_env(spec, sv, chosen, period, age, res):

@@ -1452,7 +1452,11 @@ class RegimeKernels:
         w = self.n_words
         self.SW_N, self.SW_RID_IN, self.SW_RID_OUT, self.SW_VAL, self.SW_AIDX = w, w + 1, w + 2, w + 3, w + 4
         self.SW_SEED = w + 5  # XOR-ed into the launch seed: one Philox key per item
-        w += 6
+        # JAX-stream key table of the item (0: the Philox stream): 2 words per
+        # slot -- 0 the regime draw, 1 the taste shocks, then one per state
+        # of each target (sim_slot)
+        self.SW_JKEYS = w + 6
+        w += 7
         self.SW_ACT = w
         w += len(spec.actions)
         self.SW_SIN = w
@@ -1469,6 +1473,13 @@ class RegimeKernels:
         self.SW_SOUT = w
         w += len(names)
         self.sim_words = w
+        self.sim_slot: dict[tuple, int] = {}
+        q = 2
+        for ti, t in enumerate(self.targets):
+            for k, ax in enumerate(t.spec.states):
+                self.sim_slot[(t.spec.name, ax.name)] = q
+                q += 1
+        self.sim_n_slots = q
 
     def sim_name(self) -> str:
         return f"lcm_sim_{self.tag}"
@@ -1553,6 +1564,8 @@ class RegimeKernels:
         ap("    (void)period; (void)age; (void)ati; (void)PV;")
         ap(f"    const u64 key = seed ^ (u64)it[{self.SW_SEED}];")
         ap("    LcmRng rng; rng.k0 = (u32)key; rng.k1 = (u32)(key >> 32); rng.subject = (u32)s; rng.period = (u32)period;")
+        ap(f"    const u32* JK = lcm_wp<const u32>(it, {self.SW_JKEYS});")
+        ap("    const LcmJaxRng jr{JK, (u32)s};")
         for s_ in eP.lines:
             ap("    " + s_)
         ap(f"    double PVd[{nP}]; PVd[0] = 0.0;")
@@ -1620,7 +1633,8 @@ class RegimeKernels:
             ap("    int dstar = -1, dnan = -1; double bn = -lcm_lim<double>::inf(); double vstar = -lcm_lim<double>::inf();")
             ap(f"    for (int d = 0; d < {ND}; ++d) {{")
             ap("      const double qc = bd[d].nan ? lcm_lim<double>::nan() : (bd[d].idx < 0 ? -lcm_lim<double>::inf() : bd[d].v);")
-            ap("      const double noisy = qc + scale * (rng.gumbel(64u + (u32)d) - 0.5772156649015329);")
+            ap("      const double g = JK ? jr.gumbel(1, d) : rng.gumbel(64u + (u32)d);")
+            ap("      const double noisy = qc + scale * (g - 0.5772156649015329);")
             ap("      if (dnan < 0 && noisy != noisy) dnan = d;")
             ap("      if (dstar < 0 || noisy > bn) { bn = noisy; dstar = d; vstar = qc; }")
             ap("    }")
@@ -1672,7 +1686,8 @@ class RegimeKernels:
                 ap(f"    double rp[{len(probs)}];")
                 for i, p_ in enumerate(probs):
                     ap(f"    rp[{i}] = (double)({p_});")
-                ap(f"    const int rid = lcm_categorical<{len(probs)}>(rp, rng.uniform(0u));")
+                ap(f"    const int rid = JK ? lcm_jax_choice<{len(probs)}>(rp, jr.uniform(0)) "
+                   f": lcm_categorical<{len(probs)}>(rp, rng.uniform(0u));")
             ap(f"    {rid_out} = rid;")
             for t in self.targets:
                 if t.unreachable:
@@ -1684,6 +1699,7 @@ class RegimeKernels:
                     law = t.laws[ax.name]
                     dst = f"lcm_wp<double>(it, {out_idx[ax.name]})[s]"
                     stream = f"{1 + k}u"
+                    q = self.sim_slot[(t.spec.name, ax.name)]
                     if law.kind in ("cont", "det"):
                         v = et.emit(law.expr)
                         for s_ in et.lines:
@@ -1698,25 +1714,29 @@ class RegimeKernels:
                         ap(f"      {{ double mp[{len(vs)}];")
                         for i, v in enumerate(vs):
                             ap(f"        mp[{i}] = (double)({v});")
-                        ap(f"        {dst} = (double)lcm_categorical<{len(vs)}>(mp, rng.uniform({stream})); }}")
+                        ap(f"        {dst} = (double)(JK ? lcm_jax_choice<{len(vs)}>(mp, jr.uniform({q})) "
+                           f": lcm_categorical<{len(vs)}>(mp, rng.uniform({stream}))); }}")
                     else:  # process: draw from the source process's law
                         src = law.source_process
                         grid = spec.state(src).grid
                         fld = lambda f, src=src: f"PV[{self.param_off[proc_field_name(src, f)][0]}]"  # noqa: E731
                         cls = type(grid).__name__
+                        nz = f"(JK ? jr.normal({q}) : rng.normal({stream}))"
                         if cls in ("TauchenAR1Process", "RouwenhorstAR1Process"):
-                            ap(f"      {dst} = {fld('mu')} + {fld('rho')} * pv_{src} + {fld('sigma')} * rng.normal({stream});")
+                            ap(f"      {dst} = {fld('mu')} + {fld('rho')} * pv_{src} + {fld('sigma')} * {nz};")
                         elif cls == "NormalIIDProcess":
-                            ap(f"      {dst} = {fld('mu')} + {fld('sigma')} * rng.normal({stream});")
+                            ap(f"      {dst} = {fld('mu')} + {fld('sigma')} * {nz};")
                         elif cls == "LogNormalIIDProcess":
-                            ap(f"      {dst} = exp({fld('mu')} + {fld('sigma')} * rng.normal({stream}));")
+                            ap(f"      {dst} = exp({fld('mu')} + {fld('sigma')} * {nz});")
                         elif cls == "UniformIIDProcess":
-                            ap(f"      {dst} = {fld('start')} + ({fld('stop')} - {fld('start')}) * rng.uniform({stream});")
+                            ap(f"      {dst} = JK ? jr.uniform({q}, {fld('start')}, {fld('stop')}) "
+                               f": {fld('start')} + ({fld('stop')} - {fld('start')}) * rng.uniform({stream});")
                         elif cls in ("TauchenNormalMixtureAR1Process", "NormalMixtureIIDProcess"):
                             # component 1 with probability p1 (its own stream), then its normal
                             ar = f"{fld('mu')} + {fld('rho')} * pv_{src} + " if cls.startswith("Tauchen") else ""
-                            ap(f"      {{ const bool c1 = rng.uniform({128 + k}u) < {fld('p1')};")
-                            ap(f"        const double z = rng.normal({stream});")
+                            ap("      { double z; bool c1;")
+                            ap(f"        if (JK) {{ c1 = jr.mixture({q}, {fld('p1')}, z); }}")
+                            ap(f"        else {{ c1 = rng.uniform({128 + k}u) < {fld('p1')}; z = rng.normal({stream}); }}")
                             ap(f"        {dst} = {ar}(c1 ? {fld('mu1')} + {fld('sigma1')} * z : {fld('mu2')} + {fld('sigma2')} * z); }}")
                         else:
                             raise TracingError(f"no simulation draw for process {cls}")

@@ -332,6 +332,102 @@ struct LcmRng {
   __device__ __forceinline__ double gumbel(u32 stream) const { return -log(-log(uniform(stream))); }
 };
 
+// JAX's default stream (the reference's jax.random in 64-bit mode):
+// Threefry-2x32 with 20 rounds (Salmon, Moraes, Dror and Shaw 2011) of the
+// counter pair (x0, x1) under the key (k0, k1).
+__device__ __forceinline__ u32 lcm_rotl32(u32 x, int r) { return (x << r) | (x >> (32 - r)); }
+__device__ __forceinline__ void lcm_threefry2x32(u32 k0, u32 k1, u32& x0, u32& x1) {
+  const u32 ks[3] = {k0, k1, k0 ^ k1 ^ 0x1BD11BDAu};
+  const int rot[2][4] = {{13, 15, 26, 6}, {17, 29, 16, 24}};
+  x0 += ks[0];
+  x1 += ks[1];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      x0 += x1;
+      x1 = lcm_rotl32(x1, rot[i & 1][j]);
+      x1 ^= x0;
+    }
+    x0 += ks[(i + 1) % 3];
+    x1 += ks[(i + 2) % 3] + (u32)(i + 1);
+  }
+}
+
+// Draws of one subject from JAX's stream.  `keys` holds, per stream slot q,
+// the key the reference splits into one key per subject (subject s gets the
+// hash of the counters (0, s + 1)); a draw of shape () uses the 64 bits of
+// the subject key's counters (0, 0), element d of a vector draw those of
+// (0, d); uniform: those bits' high 52 as a mantissa in [1, 2) minus one.
+struct LcmJaxRng {
+  const u32* keys;
+  u32 subject;
+  __device__ __forceinline__ void subject_key(int q, u32& a, u32& b) const {
+    a = 0u;
+    b = subject + 1u;
+    lcm_threefry2x32(keys[2 * q], keys[2 * q + 1], a, b);
+  }
+  static __device__ __forceinline__ double u01(u32 k0, u32 k1, u32 c) {
+    u32 a = 0u, b = c;
+    lcm_threefry2x32(k0, k1, a, b);
+    const u64 bits = ((u64)a << 32) | (u64)b;
+    return __longlong_as_double((long long)((bits >> 12) | 0x3FF0000000000000ULL)) - 1.0;
+  }
+  // jax.random.uniform(key, minval=lo, maxval=hi)
+  static __device__ __forceinline__ double scaled(double f, double lo, double hi) {
+    const double x = f * (hi - lo) + lo;
+    return x > lo ? x : lo;
+  }
+  __device__ __forceinline__ double uniform(int q, double lo = 0.0, double hi = 1.0) const {
+    u32 a, b;
+    subject_key(q, a, b);
+    return scaled(u01(a, b, 0u), lo, hi);
+  }
+  // sqrt(2) erfinv(u), u uniform on (nextafter(-1, 0), 1)
+  static __device__ __forceinline__ double normal_of(u32 a, u32 b) {
+    const double lo = -0.99999999999999989;  // nextafter(-1, 0)
+    return 1.4142135623730951 * erfinv(scaled(u01(a, b, 0u), lo, 1.0));
+  }
+  __device__ __forceinline__ double normal(int q) const {
+    u32 a, b;
+    subject_key(q, a, b);
+    return normal_of(a, b);
+  }
+  // element d of jax.random.gumbel(key, (n,)): -log(-log(u)), u on [tiny, 1)
+  __device__ __forceinline__ double gumbel(int q, int d) const {
+    u32 a, b;
+    subject_key(q, a, b);
+    const double u = scaled(u01(a, b, (u32)d), 2.2250738585072014e-308, 1.0);
+    return -log(-log(u));
+  }
+  // normal-mixture innovation: key1, key2 = split(key); component 1 when
+  // uniform(key1) < p1; the normal from key2
+  __device__ __forceinline__ bool mixture(int q, double p1, double& z) const {
+    u32 a, b;
+    subject_key(q, a, b);
+    u32 a1 = 0u, b1 = 0u, a2 = 0u, b2 = 1u;
+    lcm_threefry2x32(a, b, a1, b1);
+    lcm_threefry2x32(a, b, a2, b2);
+    z = normal_of(a2, b2);
+    return u01(a1, b1, 0u) < p1;
+  }
+};
+
+// jax.random.choice(key, n, p=p): the first index whose cumulative weight
+// reaches total * (1 - u)
+template <int N>
+__device__ __forceinline__ int lcm_jax_choice(const double* p, double u) {
+  double cum[N];
+  double acc = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) { acc += p[i]; cum[i] = acc; }
+  const double r = acc * (1.0 - u);
+  int k = 0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) k += cum[i] < r ? 1 : 0;
+  return k < N - 1 ? k : N - 1;
+}
+
 // categorical draw: first index whose cumulative weight exceeds u * total
 template <int N>
 __device__ __forceinline__ int lcm_categorical(const double* p, double u) {

@@ -139,9 +139,15 @@ class Model:
         log_keep_n_latest: int = 3,
         max_compilation_workers: int | None = None,
         precision: str = "fp64",
+        rng: str = "jax",
     ):
         """Forward simulation (``src/lcm/model.py:648-848``), solving first
         when ``period_to_regime_to_V_arr`` is None.
+
+        ``rng="jax"`` (default) draws from the reference's random stream (JAX's
+        Threefry-2x32 with its key threading: the same seed gives the
+        reference's draws); ``"philox"`` from a counter stream keyed by
+        (seed, subject, period, stream), the serving loop's.
 
         ``subject_batch_size`` only partitions the subject axis in the
         reference and leaves results unchanged; every subject is simulated in
@@ -161,6 +167,7 @@ class Model:
             seed=0 if seed is None else int(seed),
             precision=precision,
             log_level=log_level,
+            rng=rng,
         )
 
 

@@ -6,11 +6,19 @@ that regime takes the argmax of Q at its own (off-grid) state -- the same
 Q evaluation as the solve, reading next period's value function -- and then
 draws its next regime and next states.
 
-Draws use a counter-based Philox-4x32-10 stream keyed by the seed and
-indexed by (subject, period, stream id), so a subject's path does not depend
-on the batch it is simulated in.  The reference draws with JAX's threefry
-keys, so paths with stochastic draws agree with it in distribution, not
-bitwise; paths without draws agree exactly.
+Two random streams, both independent of the batch a subject is simulated
+in:
+
+- ``rng="jax"`` (``Model.simulate``'s default): the reference's own stream,
+  JAX's Threefry-2x32 with the reference's key threading
+  (``pylcm_b200.jaxrng``): the host walks the key chain of each simulation
+  (a handful of hashes per period and regime) and hands every (period,
+  regime) item the keys the reference splits per subject; the kernel derives
+  each subject's key and draw on the device.  Simulations reproduce the
+  reference's stored ones;
+- ``rng="philox"`` (the serving loop): a counter-based Philox-4x32-10 stream
+  keyed by the seed and indexed by (subject, period, stream id), with no
+  host-side key chain.
 """
 
 from __future__ import annotations
@@ -100,6 +108,77 @@ def _initial_arrays(model, initial_conditions: Mapping) -> tuple[np.ndarray, dic
     return rid, states
 
 
+def _stochastic_names(spec, specs, model, resolver) -> list[tuple[str, str, str]]:
+    """(qualified name, target, state) of the stochastic next-state functions
+    whose per-subject keys the reference splits for regime `spec`, sorted by
+    name (``transitions.py:111-125``): the Markov and process laws toward
+    every target the regime's transition reaches with positive probability in
+    some period and that it has a law for every state of."""
+    from pylcm_b200.regime import MarkovTransition
+    from pylcm_b200.spec import _unreachable
+    from pylcm_b200.validation import _regime_probs
+
+    reach = set()
+    for period in spec.active_periods:
+        if period + 1 >= model.n_periods:
+            continue
+        P, _ = _regime_probs(spec, specs, resolver, period, float(model.ages.values[period]))
+        for t in specs:
+            if np.any(np.nan_to_num(P[:, t.rid]) > 0):
+                reach.add(t.name)
+    out = []
+    for t in specs:
+        if t.name not in reach or not t.states or _unreachable(spec, t):
+            continue
+        for ax in t.states:
+            law = spec.functions.get(f"next_{ax.name}")
+            if ax.kind == "process" or isinstance(law, MarkovTransition):
+                out.append((f"{t.name}__next_{ax.name}", t.name, ax.name))
+    return sorted(out)
+
+
+def jax_key_chain(model, params, seed: int) -> dict:
+    """The reference's key threading over one simulation
+    (``simulate.py:275, 562-572, 630``, ``transitions.py:119, 260``):
+    {(period, regime): {"regime": key, "taste": key, (target, state): key}},
+    each the key the reference splits into one key per subject."""
+    from pylcm_b200 import jaxrng
+    from pylcm_b200.spec import ParamResolver
+
+    specs = model.regime_specs
+    res = ParamResolver(params, model.fixed_params, tuple(s.name for s in specs))
+    # the names depend on the params (reachability): cached for the last
+    # params object (kept alive with its entry, so its id is not reused)
+    cache = model.__dict__.setdefault("_jax_names", {})
+    hit = cache.get(id(params))
+    if hit is not None and hit[0] is params:
+        names = hit[1]
+    else:
+        names = {s.name: _stochastic_names(s, specs, model, res) for s in specs if not s.terminal}
+        cache.clear()
+        cache[id(params)] = (params, names)
+    by_name = {s.name: s for s in specs}
+    order = [by_name[n] for n in model.user_regimes]
+    key = jaxrng.key(seed)
+    chain = {}
+    for period in range(model.n_periods):
+        for s in order:
+            if period not in s.active_periods:
+                continue
+            d = {}
+            if s.taste_shocks:
+                d["taste"] = key
+                key = jaxrng.split(key, 1)[0]  # the running key: counters (0, 0)
+            if not s.terminal:
+                ks = jaxrng.split(key, 3)
+                run, d["regime"], key = ks[0], ks[1], ks[2]
+                for _, tname, state in names[s.name]:
+                    d[(tname, state)] = run
+                    run = jaxrng.split(run, 1)[0]
+            chain[(period, s.name)] = d
+    return chain
+
+
 class SimPlan:
     """Device buffers and launches of the simulations of solve instances.
 
@@ -112,18 +191,23 @@ class SimPlan:
     """
 
     def __init__(self, solve_plan, initial_conditions: Mapping | None = None, seed: int = 0,
-                 instances: list | None = None) -> None:
+                 instances: list | None = None, rng: str = "philox", params: Mapping | None = None) -> None:
+        """`rng="jax"` draws from the reference's stream and needs the
+        instances' `params` (one mapping, or one per instance) for its key
+        chain; "philox" draws from the counter stream."""
         import torch
 
         self.torch = torch
         self.plan = solve_plan
         dev = solve_plan.dev
+        if rng not in ("philox", "jax"):
+            raise ValueError("rng must be 'philox' or 'jax'")
         if instances is None:
             instances = [(0, initial_conditions, seed)]
         solve_plan.ensure_sim_records()
         nan = float("nan")
         self.inst = []
-        for idx, ic, sd in instances:
+        for ii, (idx, ic, sd) in enumerate(instances):
             if not 0 <= idx < solve_plan.n:
                 raise InvalidParamsError(f"instance {idx} outside the solve plan's batch of {solve_plan.n}")
             eng, records, row = solve_plan.instance(idx)
@@ -146,7 +230,11 @@ class SimPlan:
                 "anames": sorted({a.name for s in specs for a in s.actions}),
                 "rid0": rid0,
                 "states0": states0,
+                "chain": (jax_key_chain(model, params if isinstance(params, Mapping) or params is None else params[ii],
+                                        int(sd)) if rng == "jax" else None),
             })
+            if rng == "jax" and params is None:
+                raise InvalidParamsError("rng='jax' needs the instances' params for the key chain")
         # one (instances, periods, subjects) buffer per array for each group of
         # instances with the same horizon and subject count; each instance
         # works on its own slice (contiguous rows of N subjects)
@@ -190,6 +278,9 @@ class SimPlan:
         # simulation words, built per (instance, regime, kernel) for all its
         # periods at once, then grouped per (period, kernel) with one sort
         by_kernel: dict[tuple, list] = {}
+        jtabs: list[np.ndarray] = []  # JAX-stream key tables, laid out in one device buffer
+        jrefs: list[tuple] = []  # (rows array, row indices, table offsets in words)
+        jwords = 0
         for b in self.inst:
             N, T = b["N"], b["T"]
             sbytes = N * 8  # one period of a subject array (float64)
@@ -221,10 +312,34 @@ class SimPlan:
                         rows[:, rk.SW_SIN + k] = S0[a.name] + pa * sbytes
                     for k, name in enumerate(rk.sim_out_names):
                         rows[:, rk.SW_SOUT + k] = S0[name] + (pa + 1) * sbytes
+                    if b["chain"] is not None:
+                        offs = []
+                        for p_ in pa:
+                            tab = np.zeros((rk.sim_n_slots, 2), dtype=np.uint32)
+                            d = b["chain"].get((int(p_), s.name), {})
+                            if "regime" in d:
+                                tab[0] = d["regime"]
+                            if "taste" in d:
+                                tab[1] = d["taste"]
+                            for (tname, state), q in rk.sim_slot.items():
+                                if (tname, state) in d:
+                                    tab[q] = d[(tname, state)]
+                            # 16-byte aligned tables (uint32 words)
+                            jtabs.append(np.concatenate([tab.reshape(-1), np.zeros((-tab.size) % 4, np.uint32)]))
+                            offs.append(jwords)
+                            jwords += jtabs[-1].size
+                        jrefs.append((rows, rk.SW_JKEYS, np.asarray(offs, dtype=np.int64)))
                     g = by_kernel.setdefault((rk.sim_name(), rk.key), [rk, [], [], []])
                     g[1].append(rows)
                     g[2].append(pa)
                     g[3].append(np.full(len(pa), tiles, dtype=np.int64))
+        # the key tables' device buffer; the item words point into it
+        # uint32 words, moved bit for bit through an int32 view
+        self.jkeys = torch.from_numpy(np.concatenate(jtabs).view(np.int32)).to(dev) if jtabs else None
+        if jtabs:
+            base = self.jkeys.data_ptr()
+            for rows, w, offs in jrefs:
+                rows[:, w] = base + 4 * offs
         pieces = []  # (period, kernel order, rk, rows, tiles)
         for order, (rk, rows_l, per_l, til_l) in enumerate(by_kernel.values()):
             rows = np.concatenate(rows_l)
@@ -290,8 +405,9 @@ class SimPlan:
 
 
 def simulate(model, *, params, initial_conditions, V_arr=None, seed: int = 0, precision: str = "fp64",
-             log_level: str = "progress") -> SimulationResult:
-    """Solve (unless `V_arr` is given) and simulate `initial_conditions`."""
+             log_level: str = "progress", rng: str = "jax") -> SimulationResult:
+    """Solve (unless `V_arr` is given) and simulate `initial_conditions`
+    (random stream `rng`: "jax", the reference's, or "philox")."""
     import torch
 
     eng = model.engine(precision)
@@ -304,6 +420,6 @@ def simulate(model, *, params, initial_conditions, V_arr=None, seed: int = 0, pr
                 k = plan.slot[r].get(int(p))
                 if k is not None:
                     plan.V[r][0, k].copy_(torch.as_tensor(np.asarray(v, dtype=np.float64).reshape(-1)))
-    sim = SimPlan(plan, initial_conditions, seed)
+    sim = SimPlan(plan, initial_conditions, seed, rng=rng, params=params)
     sim.run()
     return sim.result(model)

@@ -93,10 +93,33 @@ def main() -> None:
         labor_supply=mort["labor_supply"].astype(str).to_numpy().astype("U"),
         age=mort["age"].to_numpy(np.float64),
     )
+    processes_simulations(data)
     # the independent `dcegm` package's solution of the IJRS retirement model
     # with taste shocks (the reference's cross-check fixture)
     df = pd.read_csv(data / "dcegm_reference" / "ijrs_taste_shocks_reference.csv")
     np.savez(OUT / "ijrs_taste_shocks_reference.npz", **{c: df[c].to_numpy(np.float64) for c in df.columns})
+
+
+def processes_simulations(data: Path) -> None:
+    """The stored stochastic simulations of the process models (2 subjects, 4
+    periods, seed 42): drawn from JAX's default stream, so they pin a
+    restatement of that stream (Markov health draws, process draws)."""
+    import pandas as pd
+
+    for kind in ("uniform", "normal", "lognormal", "tauchen", "rouwenhorst"):
+        sim = pd.read_pickle(data / "processes" / f"simulation_{kind}.pkl")
+        np.savez(
+            OUT / f"processes_simulation_{kind}.npz",
+            subject_id=sim["subject_id"].to_numpy(np.int64),
+            period=sim["period"].to_numpy(np.int64),
+            regime=sim["regime_name"].astype(str).to_numpy().astype("U"),
+            value=sim["value"].to_numpy(np.float64),
+            health=sim["health"].astype(str).to_numpy().astype("U"),
+            income=sim["income"].to_numpy(np.float64),
+            wealth=sim["wealth"].to_numpy(np.float64),
+            consumption=sim["consumption"].to_numpy(np.float64),
+            age=sim["age"].to_numpy(np.float64),
+        )
 
 
 if __name__ == "__main__":

@@ -92,7 +92,8 @@ def test_simulated_draws_have_the_process_moments():
     assert abs(np.std(y1) - 0.1) < 0.005
 
 
-def test_batched_simulation_equals_single_instance_runs():
+@pytest.mark.parametrize("rng", ["philox", "jax"])
+def test_batched_simulation_equals_single_instance_runs(rng):
     """One kernel (d) launch per (period, regime) over several solve instances,
     each with its own seed and subjects, gives each instance's single run."""
     from pylcm_b200.simulate import SimPlan
@@ -112,11 +113,11 @@ def test_batched_simulation_equals_single_instance_runs():
             "age": np.zeros(n),
             "regime_id": np.zeros(n, dtype=int),
         })
-    sim = SimPlan(plan, instances=[(k, ics[k], seeds[k]) for k in range(3)])
+    sim = SimPlan(plan, instances=[(k, ics[k], seeds[k]) for k in range(3)], rng=rng, params=plist)
     sim.run()
     for k in range(3):
         got = sim.result(model, k)
-        one = model.simulate(params=plist[k], initial_conditions=ics[k], seed=seeds[k])
+        one = model.simulate(params=plist[k], initial_conditions=ics[k], seed=seeds[k], rng=rng)
         for p in one.periods:
             np.testing.assert_array_equal(got.periods[p]["regime_id"], one.periods[p]["regime_id"])
             np.testing.assert_array_equal(got.periods[p]["value"], one.periods[p]["value"])
