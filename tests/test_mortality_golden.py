@@ -1,10 +1,13 @@
 """The reference's stored float64 simulation of its mortality example (three
 regimes, 10-year periods, survival probabilities indexed by period in Markov
-regime transitions), as in its ``test_regression_mortality``.  Survival is
-drawn, and this build draws from its own counter-based stream, so a subject is
-compared over the periods its regime path matches the stored one (every
-subject retires at 40; most survive to 60); there values, states and choices
-agree at the reference's atol of 1e-5."""
+regime transitions), as in its ``test_regression_mortality``.
+
+With the reference's own seed and subject count the simulation is reproduced
+row for row (``tests/test_jax_stream.py``).  Here a larger population under
+another seed: survival is drawn, so a subject is compared over the periods
+its regime path matches the stored one (every subject retires at 40; most
+survive to 60); there values, states and choices agree at the reference's
+atol of 1e-5."""
 
 import numpy as np
 import pytest
