@@ -296,6 +296,78 @@ def _boundary(roots: list[ir.Expr]) -> list[ir.Expr]:
     return list(out.values())
 
 
+def _affine_split(x, cnames: set) -> tuple | None:
+    """Split x = x0 + sum_k coef_k * a_k over the continuous actions a_k named
+    in `cnames`, with x0 and every coef_k free of those actions, by walking
+    the expression: sums, differences, negation, float casts, products with
+    an action-free factor and quotients by an action-free divisor keep the
+    form; any other node that reads a continuous action (a power, a
+    transcendental, a comparison, a select, floor ...) rejects it.  Returns
+    (x0, {name: coef}) or None.  The split is exact in real arithmetic."""
+    memo: dict[int, tuple | None] = {}
+    zero = ir.const(0.0)
+
+    def acts(e) -> bool:
+        return isinstance(e, ir.Expr) and any(k == "action" and nm in cnames for k, nm in e.deps())
+
+    def add(p, q, sign: float):
+        (a0, A), (b0, Bc) = p, q
+        if sign > 0:
+            c0 = b0 if ir.is_const(a0) and a0.args[0] == 0.0 else (a0 if ir.is_const(b0) and b0.args[0] == 0.0 else a0 + b0)
+        else:
+            c0 = -b0 if ir.is_const(a0) and a0.args[0] == 0.0 else (a0 if ir.is_const(b0) and b0.args[0] == 0.0 else a0 - b0)
+        C = dict(A)
+        for k, v in Bc.items():
+            C[k] = (C[k] + v if sign > 0 else C[k] - v) if k in C else (v if sign > 0 else -v)
+        return c0, C
+
+    def mul(v, f, div: bool):
+        if ir.is_const(v) and v.args[0] in (1.0, -1.0) and not div:
+            return f if v.args[0] == 1.0 else -f
+        return v / f if div else v * f
+
+    def scale(p, f, div: bool):
+        a0, A = p
+        s0 = zero if ir.is_const(a0) and a0.args[0] == 0.0 else mul(a0, f, div)
+        return s0, {k: mul(v, f, div) for k, v in A.items()}
+
+    def rec(e):
+        if not acts(e):
+            return (ir.const(e), {})
+        if id(e) in memo:
+            return memo[id(e)]
+        r = None
+        if e.dtype != "f":
+            r = None
+        elif e.op == "var":
+            r = (zero, {e.args[1]: ir.const(1.0)})
+        elif e.op == "cast":
+            r = rec(e.args[1]) if e.args[1].dtype == "f" else None
+        elif e.op == "un" and e.args[0] == "neg":
+            p = rec(e.args[1])
+            r = None if p is None else add((zero, {}), p, -1.0)
+        elif e.op == "bin" and e.args[0] in ("+", "-"):
+            p, q = rec(e.args[1]), rec(e.args[2])
+            r = None if p is None or q is None else add(p, q, 1.0 if e.args[0] == "+" else -1.0)
+        elif e.op == "bin" and e.args[0] == "*":
+            a, b = e.args[1], e.args[2]
+            if acts(a) and not acts(b):
+                p = rec(a)
+                r = None if p is None else scale(p, b, False)
+            elif acts(b) and not acts(a):
+                p = rec(b)
+                r = None if p is None else scale(p, a, False)
+        elif e.op == "bin" and e.args[0] == "/":
+            a, b = e.args[1], e.args[2]
+            if not acts(b):
+                p = rec(a)
+                r = None if p is None else scale(p, b, True)
+        memo[id(e)] = r
+        return r
+
+    return rec(x)
+
+
 @dataclasses.dataclass
 class TargetPlan:
     spec: RegimeSpec
@@ -379,6 +451,7 @@ class LaunchConfig:
     sb: int = 1  # states per thread (register blocking)
     min_blocks: int = 0  # __launch_bounds__ min CTAs per SM (0 = compiler's choice)
     prune: bool = True  # single-precision search: exact skipping of action groups where eligible
+    group: int = 16  # actions per skipped group (raised to `lanes` if smaller)
 
     @property
     def states_per_tile(self) -> int:
@@ -406,6 +479,7 @@ class RegimeKernels:
         self.targets = [_target_plan(tr, t) for t in order] if not self.spec.terminal else []
         self._layout()
         self._affine = self._affine_laws()
+        self._groups = self._group_plan()
         tag_src = repr(
             (self.spec.name, [t.spec.name for t in self.targets], precision, dataclasses.astuple(cfg))
         )
@@ -463,6 +537,10 @@ class RegimeKernels:
                 parts.append(self._expect_source(t))
         for t in tc:
             parts.append(self._expect_tc_source(t))
+        if any(self.group_stats(t) == 2 for t in self.targets):
+            parts.append(f'extern "C" __global__ void __launch_bounds__(256) {self.stats_name()}('
+                         "const i64* __restrict__ items, const int* __restrict__ tile_prefix, int n_items, "
+                         "int n_tiles) {\n  lcm_tile_stats2(items, tile_prefix, n_items, n_tiles);\n}")
         return "\n".join(parts)
 
     def e_words_for(self, t: TargetPlan) -> int:
@@ -573,12 +651,124 @@ class RegimeKernels:
                 if len(acts) != 1:
                     continue
                 cv = ir.var("action", next(iter(acts)), "f")
+                if _affine_split(x, {cv.args[1]}) is None:
+                    continue  # a non-affine piece (floor, select ...) that the derivative would miss
                 g = ir.const(ir.diff(x, cv))
                 if not isinstance(g, ir.Expr) or any(n is cv for n in ir.topo_order([g])):
                     continue
                 x0 = ir.substitute(x, cv, 0.0)
                 out[(ti, pos)] = (x0, g, cv)
         return out
+
+    # group skipping: tiles of the block statistics of a target with two
+    # continuous axes (axis 1 x axis 2); one continuous axis uses 16-column blocks
+    GROUP_TILE = (16, 2)
+    GROUP_MAX_CHUNK = 2048  # the whole continuous-action table in shared memory
+
+    def _group_plan(self) -> dict | None:
+        """Eligibility and the affine pieces of the exact skipping of action
+        groups in the single-precision search (kernel (a)).
+
+        A group is a run of consecutive values of one continuous action (the
+        scan action, the largest) with the other continuous actions fixed.
+        Its Q values are bounded above by its largest utility plus beta times
+        the largest expectation-table value among the nodes its next-state
+        coordinates can reach.  That needs: the utility and the continuous
+        actions in the action table (utility free of the state), a
+        state-free non-negative discount factor, and per reached target with
+        one or two continuous axes (linear grids, no deterministic discrete
+        axis) coordinates x = x0 + sum_k coef_k a_k with x0 and coef_k free of
+        the continuous actions, so that interval arithmetic over the group's
+        action ranges bounds them.  Constraints of the same affine form
+        (lhs - rhs) give a second test: a group all of whose members violate
+        one is skipped.  Returns None when nothing qualifies."""
+        spec, tr = self.spec, self.tr
+        if (self.precision != "fp32" or not self.cfg.prune or spec.terminal or spec.taste_shocks
+                or tr.regime_id is None or tr.beta is None):
+            return None
+        cacts = [a for a in spec.actions if a.kind == "continuous"]
+        if not cacts:
+            return None
+        cn = {a.name for a in cacts}
+        U, beta = ir.const(tr.U), ir.const(tr.beta)
+        if not isinstance(U, ir.Expr) or any(k == "state" for k, _ in U.deps()):
+            return None
+        if not any(k == "action" and nm in cn for k, nm in U.deps()):
+            return None
+        if isinstance(beta, ir.Expr) and any(k in ("state", "action") for k, _ in beta.deps()):
+            return None
+        axes: dict[int, list] = {}
+        for ti, t in enumerate(self.targets):
+            if t.scalar or t.unreachable or t.det_pos or not 1 <= len(t.cont_pos) <= 2:
+                continue
+            parts = []
+            for ci, pos in enumerate(t.cont_pos):
+                ax = t.spec.states[pos]
+                if ax.grid.kind != "lin":
+                    break
+                sp = _affine_split(ir.const(t.laws[ax.name].expr), cn)
+                if sp is None:
+                    break
+                parts.append((pos, ci, sp[0], sp[1]))
+            else:
+                axes[ti] = parts
+        if not axes:
+            return None
+        cons = []
+        F = ir.const(tr.F)
+        stack = [F] if isinstance(F, ir.Expr) else []
+        while stack:
+            n = stack.pop()
+            if n.op == "and":
+                stack.extend(a for a in n.args if isinstance(a, ir.Expr))
+                continue
+            if n.op != "cmp" or n.args[0] not in ("<", "<=", ">", ">="):
+                continue
+            lhs, rhs = ir.const(n.args[1]), ir.const(n.args[2])
+            if lhs.dtype != "f" and rhs.dtype != "f":
+                continue
+            sp = _affine_split(lhs - rhs, cn)
+            if sp is not None and sp[1]:
+                cons.append((n.args[0], sp[0], sp[1]))
+        used = set()
+        for parts in axes.values():
+            for _, _, _, co in parts:
+                used |= set(co)
+        for _, _, co in cons:
+            used |= set(co)
+        sizes = [a.size for a in cacts]
+        scan = int(np.argmax(sizes))
+        return {"axes": axes, "cons": cons, "acts": [a.name for a in cacts if a.name in used],
+                "scan": scan, "cacts": [a.name for a in cacts]}
+
+    def _group_roots(self) -> list:
+        g = self._groups
+        if not g:
+            return []
+        out = [ir.var("action", nm, "f") for nm in g["acts"]]
+        for parts in g["axes"].values():
+            for _, _, x0, co in parts:
+                out.append(x0)
+                out += list(co.values())
+        for _, y0, co in g["cons"]:
+            out.append(y0)
+            out += list(co.values())
+        return out
+
+    def group_stats(self, t: TargetPlan) -> int:
+        """Block statistics the search's group skipping reads for target `t`:
+        0 none, 1 per 16 columns (written by kernel (b)), 2 per GROUP_TILE
+        tile of the two continuous axes (written by the statistics kernel)."""
+        g = self._groups
+        if not g:
+            return 0
+        ti = next((i for i, x in enumerate(self.targets) if x is t), None)
+        if ti is None or ti not in g["axes"]:
+            return 0
+        return len(g["axes"][ti])
+
+    def stats_name(self) -> str:
+        return f"lcm_tile_stats_{self.tag}"
 
     def inner_flops(self) -> dict:
         """Floating-point operations of one (state, action) evaluation of
@@ -627,6 +817,7 @@ class RegimeKernels:
         roots = [tr.F, tr.U]
         for x0, g, cv in getattr(self, "_affine", {}).values():
             roots += [x0, g, cv]
+        roots += self._group_roots() if getattr(self, "_groups", None) else []
         if tr.beta is not None:
             roots.append(tr.beta)
         if tr.regime_id is not None and self.targets:
@@ -714,6 +905,8 @@ class RegimeKernels:
                 ni += 1
         NF, NI = max(nf, 1), max(ni, 1)
         B, LANES, CH, SB = cfg.block, cfg.lanes, cfg.chunk, cfg.sb
+        if self._groups:
+            CH = max(CH, self.GROUP_MAX_CHUNK)  # group skipping holds the whole table
         SPT = cfg.states_per_tile
         SPB = B // LANES
         dstates = [a for a in spec.states if a.kind != "continuous"]
@@ -1128,7 +1321,10 @@ class RegimeKernels:
             return o
 
         # ---- exact skipping of action groups (single-precision search)
-        G = max(16, LANES)
+        G = max(cfg.group, LANES)
+        GP = self._groups
+        GMAX = 2 * CH // G  # groups held in shared memory
+        MP = 8  # pilot actions per combination of the other continuous actions
 
         def provider(n, kb: str) -> str | None:
             """Kernel-scope expression of a hoisted boundary node (double)."""
@@ -1141,146 +1337,258 @@ class RegimeKernels:
                         return fmt.format(i=i)
             return None
 
-        def prune_info(ti: int):
-            # one continuous action: within a group of consecutive inner
-            # actions its value is monotone, so the group's coordinates lie
-            # between those of its first and last action
-            if not fp32 or taste or spec.terminal or not self.cfg.prune or len(cacts) != 1:
+        def group_info(ti: int) -> dict | None:
+            """Kernel-side pieces of the group plan of target ti (None: the
+            hoisted values it needs are not all available)."""
+            if GP is None or ti not in GP["axes"]:
                 return None
-            t = self.targets[ti]
-            if t.scalar or t.unreachable or t.det_pos or len(t.cont_pos) != 1:
-                return None
-            pos = t.cont_pos[0]
-            if (ti, pos) not in self._affine:
-                return None
-            x0, gr, cv = self._affine[(ti, pos)]
-            U = ir.const(self.tr.U)
             ia = {id(n): i for i, n in enumerate(bA)}
-            if not isinstance(U, ir.Expr) or id(U) not in ia or slot[ia[id(U)]][0] != "F":
+
+            def fslot(n):
+                i = ia.get(id(n))
+                return slot[i][1] if i is not None and slot[i][0] == "F" else None
+
+            uf = fslot(ir.const(self.tr.U))
+            avf = {nm: fslot(ir.var("action", nm, "f")) for nm in GP["acts"]}
+            if uf is None or any(v is None for v in avf.values()):
                 return None
-            if id(cv) not in ia or slot[ia[id(cv)]][0] != "F":
+            pb = provider(ir.const(self.tr.beta), "kb")
+            if pb is None or "[kb]" in pb:
                 return None
-            beta = ir.const(self.tr.beta)
-            pb = provider(beta, "kb")
-            if pb is None or not pb.startswith("PVd"):
-                return None
-            px0, pg = provider(ir.const(x0), "kb"), provider(ir.const(gr), "kb")
-            if px0 is None or pg is None:
-                return None
+
+            def prov_all(x0, co):
+                px = provider(ir.const(x0), "kb")
+                pc = {nm: provider(ir.const(c), "kb") for nm, c in co.items()}
+                if px is None or any(v is None for v in pc.values()):
+                    return None
+                return px, pc
+
+            axes = []
+            for pos, ci, x0, co in GP["axes"][ti]:
+                r = prov_all(x0, co)
+                if r is None:
+                    return None
+                axes.append((pos, ci, r[0], r[1]))
+            cons = []
+            for op, y0, co in GP["cons"]:
+                r = prov_all(y0, co)
+                if r is not None:
+                    cons.append((op, r[0], r[1]))
+            t = self.targets[ti]
             key = "0"
             for kind, name, size in t.key_vars:
                 iv = f"SI[kb][{[a.name for a in dstates].index(name)}]" if kind == "state" else f"DI_{name}"
                 key = f"({key}) * {size} + {iv}"
-            return {"uf": slot[ia[id(U)]][1], "cvf": slot[ia[id(cv)]][1], "beta": pb, "x0": px0, "g": pg,
-                    "key": key, "n": f"C.n{ti}_{pos}", "a": f"C.a{ti}_0", "b": f"C.b{ti}_0", "bst": f"C.bst{ti}"}
+            return {"uf": uf, "avf": avf, "beta": pb, "axes": axes, "cons": cons, "key": key, "ti": ti,
+                    "bst": f"C.bst{ti}"}
 
-        def inner_loop_pruned(sa_fn: str, pi: dict) -> list[str]:
-            """inner_loop with exact skipping of groups of G consecutive
-            continuous actions.  Per state, an upper bound of Q over a group
-            -- the group's largest utility (from the action table) plus beta
-            times the largest expectation-table value among the cells the
-            group's coordinates can read (from the table's block statistics),
-            plus a rounding margin -- is compared with the state's current
-            second-best value (or the second best of a pilot pass over the
-            group midpoints, which is never above the final second best).  A
-            group whose bound is below it cannot enter the top two: skipping
-            it leaves the search's two candidates, and so V and the policy,
-            exactly as without skipping.  Every lane still visits its own
-            actions in increasing order.  Groups whose coordinates leave
-            [0.5, n - 1.5] (extrapolation), NaN bounds and negative beta are
-            never skipped."""
-            o = []
+        def inner_loop_groups(sa_fn: str, gi: dict) -> list[str]:
+            """inner_loop with exact skipping of action groups.
+
+            The whole continuous-action table sits in shared memory.  A group
+            is a run of G consecutive values of the scan action with the other
+            continuous actions fixed; per group the block records its largest
+            utility and each action's range.  Per state and group, interval
+            arithmetic over those ranges bounds the next-state coordinates and
+            the constraints' left-minus-right sides: a group all of whose
+            members violate a constraint is skipped, and so is a group whose
+            Q bound -- largest utility + beta x the largest expectation-table
+            value (the block statistics) over the nodes its coordinates can
+            reach + a rounding margin -- is below the state's running second
+            best (or the second best of a pilot pass over a few spread
+            actions, never above the final second best).  Such a group cannot
+            enter the top two, so the search's two candidates, and V and the
+            policy, are exactly those of the full search.  Coordinates are
+            widened by 0.02 + 4e-6 x their magnitude (the float rounding of
+            the law as the search evaluates it); a group whose widened
+            coordinates leave the grid (extrapolation), and NaN bounds, are
+            never skipped.  Candidates are added with index-aware ties, as
+            the groups visit the flat action indices out of order."""
+            o: list[str] = []
+            acts = GP["acts"]
+            ks = {nm: k for k, nm in enumerate(acts)}
+            anames = [a.name for a in spec.actions]
+            cnames = GP["cacts"]
+            kscan = anames.index(cnames[GP["scan"]])
+            later = [anames.index(nm) for nm in cnames[GP["scan"] + 1:]]
             di_args = "".join(f"DI_{a.name}, " for a in dacts)
             call = f"{sa_fn}<float, float>(C, PV, PVd, DV, SV[kb], SDV[kb], af, SI[kb], {di_args}period, age, q)"
-            o.append(f"const float beta_f = (float)({pi['beta'].replace('kb', '0')});")
-            o.append(f"const bool pr_on = {pi['bst']} != nullptr && beta_f >= 0.0f;")
-            o.append(f"const int n_c = {pi['n']};")
-            o.append("const int nb16 = (n_c + 15) >> 4;")
-            o.append("const float c_hi_lim = (float)(n_c - 1) - 0.5f;")
-            o.append(f"float Kc[{SB}], Mc[{SB}]; int keyr[{SB}];")
-            o.append(f"#pragma unroll\nfor (int kb = 0; kb < {SB}; ++kb) {{")
-            o.append(f"  Kc[kb] = ((float)({pi['x0']}) - {pi['a']}) * {pi['b']};")
-            o.append(f"  Mc[kb] = (float)({pi['g']}) * {pi['b']};")
-            o.append(f"  keyr[kb] = {pi['key']};")
-            o.append("}")
-            o.append(f"for (int c0 = 0; c0 < n_ac; c0 += {CH}) {{")
-            o.append(f"  const int cn = min({CH}, n_ac - c0);")
-            o.append("  __syncthreads();")
-            o.append(f"  for (int j = threadIdx.x; j < cn; j += {B}) {{")
-            o.append("    const i64 a = (i64)ad * n_ac + c0 + j;")
+            ti = gi["ti"]
+            ninf = "-lcm_lim<float>::inf()"
+            o.append(f"const float beta_f = (float)({gi['beta']});")
+            o.append(f"const int gN = lcm_wi(it, {self.W_ASIZE + kscan});")
+            o.append("int gS = 1;")
+            for k in later:
+                o.append(f"gS *= lcm_wi(it, {self.W_ASIZE + k});")
+            o.append(f"const int gpc = (gN + {G - 1}) / {G};")
+            o.append("const int ncomb = gN > 0 ? n_ac / gN : 0;")
+            o.append("const int NG = ncomb * gpc;")
+            o.append(f"const bool grp = {gi['bst']} != nullptr && beta_f >= 0.0f && n_ac <= {CH} && gN >= {G} "
+                     f"&& NG <= {GMAX};  // uniform over the CTA (one item per tile)")
+            o.append("if (!grp) {")
+            o += ["  " + x for x in inner_loop(sa_fn)]
+            o.append("} else {")
+            b: list[str] = []
+            # per-state affine pieces (float), coordinates in grid units
+            b.append(f"float gK[{SB}][{len(gi['axes'])}], gE[{SB}][{len(gi['axes'])}]; int keyr[{SB}];")
+            nM = sum(len(pc) for _, _, _, pc in gi["axes"])
+            nY = len(gi["cons"])
+            nH = sum(len(pc) for _, _, pc in gi["cons"])
+            b.append(f"float gM[{SB}][{max(nM, 1)}], gY[{SB}][{max(nY, 1)}], gH[{SB}][{max(nH, 1)}];")
+            b.append(f"#pragma unroll\nfor (int kb = 0; kb < {SB}; ++kb) {{")
+            m_i = 0
+            for p, (pos, ci, px, pc) in enumerate(gi["axes"]):
+                A, Bs = f"C.a{ti}_{ci}", f"C.b{ti}_{ci}"
+                b.append(f"  {{ const float x0 = (float)({px});")
+                b.append(f"    gK[kb][{p}] = (x0 - {A}) * {Bs};")
+                b.append(f"    gE[kb][{p}] = (fabsf(x0) + fabsf({A})) * fabsf({Bs}); }}")
+                for nm, c in pc.items():
+                    b.append(f"  gM[kb][{m_i}] = (float)({c}) * {Bs};")
+                    m_i += 1
+            h_i = 0
+            for c_i, (op, py, pc) in enumerate(gi["cons"]):
+                b.append(f"  gY[kb][{c_i}] = (float)({py});")
+                for nm, c in pc.items():
+                    b.append(f"  gH[kb][{h_i}] = (float)({c});")
+                    h_i += 1
+            b.append(f"  keyr[kb] = {gi['key']};")
+            b.append("}")
+            # the continuous-action table of this discrete action, whole
+            b.append("__syncthreads();")
+            b.append(f"for (int j = threadIdx.x; j < n_ac; j += {B}) {{")
+            b.append("  const i64 a = (i64)ad * n_ac + j;")
             for k in range(nf):
-                o.append(f"    tabf[{k} * {CH} + j] = ({TT})atf[(i64){k} * n_actions + a];")
+                b.append(f"  tabf[{k} * {CH} + j] = ({TT})atf[(i64){k} * n_actions + a];")
             for k in range(ni):
-                o.append(f"    tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
-            o.append("  }")
-            o.append("  __syncthreads();")
-            o.append(f"  const int ng = (cn + {G - 1}) / {G};")
-            o.append(f"  for (int g = threadIdx.x; g < ng; g += {B}) {{")
-            o.append("    float m = -lcm_lim<float>::inf();")
-            o.append(f"    const int j1 = min(cn, g * {G} + {G});")
-            o.append(f"    for (int j = g * {G}; j < j1; ++j) m = lcm_nanmax(m, tabf[{pi['uf']} * {CH} + j]);")
-            o.append("    gumax[g] = m;")
-            o.append("  }")
-            o.append("  __syncthreads();")
-            o.append(f"  float thr[{SB}];")
-            o.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) "
-                     "thr[kb] = best[kb].idx2 >= 0 ? best[kb].v2 : -lcm_lim<float>::inf();")
-            o.append("  if (pr_on) {")
-            o.append(f"    float p1[{SB}], p2[{SB}];")
-            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) p1[kb] = p2[kb] = -lcm_lim<float>::inf();")
-            o.append(f"    for (int g = lane; g < ng; g += {LANES}) {{")
-            o.append(f"      const int j = min(g * {G} + {G // 2}, cn - 1);")
-            o.append(f"      AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
-            o.append(f"      #pragma unroll\n      for (int kb = 0; kb < {SB}; ++kb) {{")
-            o.append("        float q;")
-            o.append(f"        if (act[kb] && {call} && q > p2[kb]) {{")
-            o.append("          if (q > p1[kb]) { p2[kb] = p1[kb]; p1[kb] = q; } else { p2[kb] = q; }")
-            o.append("        }")
-            o.append("      }")
-            o.append("    }")
-            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) thr[kb] = fmaxf(thr[kb], p2[kb]);")
-            o.append("  }")
-            o.append("  for (int g = 0; g < ng; ++g) {")
-            o.append(f"    const int j0 = g * {G}, j1 = min(cn, j0 + {G});")
-            o.append(f"    bool run[{SB}]; bool any = false;")
-            o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
-            o.append("      bool skip = false;")
-            o.append("      if (pr_on && act[kb]) {")
-            o.append("        const float um = gumax[g];")
-            o.append(f"        const float cva = tabf[{pi['cvf']} * {CH} + j0], cvb = tabf[{pi['cvf']} * {CH} + j1 - 1];")
-            o.append("        const float ca = Kc[kb] + Mc[kb] * cva, cb = Kc[kb] + Mc[kb] * cvb;")
-            o.append("        const float lo = fminf(ca, cb), hi = fmaxf(ca, cb);")
-            o.append("        if (ca == ca && cb == cb && lo >= 0.5f && hi <= c_hi_lim) {")
-            o.append("          const int L0 = max((int)lo - 1, 0), H1 = min((int)hi + 2, n_c - 1);")
-            o.append(f"          const float2* row = {pi['bst']} + (i64)keyr[kb] * nb16;")
-            o.append("          float mx = -lcm_lim<float>::inf(), ab = 0.0f;")
-            o.append("          for (int b = L0 >> 4; b <= (H1 >> 4); ++b) {")
-            o.append("            const float2 st = __ldg(row + b);")
-            o.append("            mx = lcm_nanmax(mx, st.x);")
-            o.append("            ab = fmaxf(ab, st.y);")
-            o.append("          }")
-            o.append("          const float ub = um + beta_f * mx;")
-            o.append("          const float marg = 3.8e-6f * (fabsf(um) + beta_f * ab);")
-            o.append("          skip = ub + marg < thr[kb];")
-            o.append("        }")
-            o.append("      }")
-            o.append("      run[kb] = act[kb] && !skip;")
-            o.append("      any = any || run[kb];")
-            o.append("    }")
-            o.append("    if (!any) continue;")
-            o.append(f"    for (int j = j0 + lane; j < j1; j += {LANES}) {{")
-            o.append(f"      AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
-            o.append("      const int aidx = ad * n_ac + c0 + j;")
-            o.append(f"      #pragma unroll\n      for (int kb = 0; kb < {SB}; ++kb) {{")
-            o.append("        float q;")
-            o.append(f"        if (run[kb] && {call}) best[kb].push(q, aidx);")
-            o.append("      }")
-            o.append("    }")
-            o.append("  }")
+                b.append(f"  tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
+            b.append("}")
+            b.append("__syncthreads();")
+            # per-group utility maximum and action ranges
+            b.append(f"for (int g = threadIdx.x; g < NG; g += {B}) {{")
+            b.append("  const int o_ = g / gpc, gi_ = g - o_ * gpc;")
+            b.append(f"  const int jb = (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;")
+            b.append(f"  const int m = min({G}, gN - gi_ * {G});")
+            b.append(f"  float um = {ninf};")
+            for k in range(len(acts)):
+                b.append(f"  float lo{k} = lcm_lim<float>::inf(), hi{k} = {ninf};")
+            b.append("  for (int t = 0; t < m; ++t) {")
+            b.append("    const int j = jb + t * gS;")
+            b.append(f"    um = lcm_nanmax(um, tabf[{gi['uf']} * {CH} + j]);")
+            for nm, k in ks.items():
+                b.append(f"    {{ const float v = tabf[{gi['avf'][nm]} * {CH} + j]; lo{k} = fminf(lo{k}, v); "
+                         f"hi{k} = fmaxf(hi{k}, v); }}")
+            b.append("  }")
+            b.append("  gU[g] = um;")
+            for k in range(len(acts)):
+                b.append(f"  gLo[{k} * {GMAX} + g] = lo{k}; gHi[{k} * {GMAX} + g] = hi{k};")
+            b.append("}")
+            b.append("__syncthreads();")
+            # pilot pass: a few spread actions per combination give a first threshold
+            b.append(f"float thr[{SB}];")
+            b.append("{")
+            b.append(f"  float p1[{SB}], p2[{SB}];")
+            b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) p1[kb] = p2[kb] = {ninf};")
+            b.append(f"  for (int p = lane; p < ncomb * {MP}; p += {LANES}) {{")
+            b.append(f"    const int o_ = p / {MP}, m_ = p - o_ * {MP};")
+            b.append(f"    const int si = ((2 * m_ + 1) * gN) / {2 * MP};")
+            b.append("    const int j = (o_ / gS) * gN * gS + (o_ % gS) + si * gS;")
+            b.append(f"    AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
+            b.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
+            b.append("      float q;")
+            b.append(f"      if (act[kb] && {call} && q > p2[kb]) {{")
+            b.append("        if (q > p1[kb]) { p2[kb] = p1[kb]; p1[kb] = q; } else { p2[kb] = q; }")
+            b.append("      }")
+            b.append("    }")
+            b.append("  }")
+            b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) thr[kb] = p2[kb];")
+            b.append("}")
+            # the groups
+            b.append("for (int g = 0; g < NG; ++g) {")
+            b.append("  const int o_ = g / gpc, gi_ = g - o_ * gpc;")
+            b.append(f"  const int jb = (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;")
+            b.append(f"  const int m = min({G}, gN - gi_ * {G});")
+            b.append("  const float um = gU[g];")
+            for k in range(len(acts)):
+                b.append(f"  const float lo{k} = gLo[{k} * {GMAX} + g], hi{k} = gHi[{k} * {GMAX} + g];")
+                b.append(f"  const float am{k} = fmaxf(fabsf(lo{k}), fabsf(hi{k}));")
+            b.append(f"  bool run[{SB}]; bool any = false;")
+            b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{")
+            b.append("    bool skip = false;")
+            b.append("    if (act[kb]) {")
+            h_i = 0
+            for c_i, (op, py, pc) in enumerate(gi["cons"]):
+                b.append(f"      {{ float lo = gY[kb][{c_i}], hi = lo, mag = fabsf(lo);")
+                for nm in pc:
+                    k = ks[nm]
+                    b.append(f"        {{ const float h = gH[kb][{h_i}]; lo += h >= 0.0f ? h * lo{k} : h * hi{k}; "
+                             f"hi += h >= 0.0f ? h * hi{k} : h * lo{k}; mag += fabsf(h) * am{k}; }}")
+                    h_i += 1
+                if op in ("<", "<="):
+                    b.append("        skip = skip || lo > 4e-6f * mag; }  // every member has lhs > rhs")
+                else:
+                    b.append("        skip = skip || hi < -4e-6f * mag; }  // every member has lhs < rhs")
+            b.append("      if (!skip) {")
+            b.append(f"        const float th = fmaxf(thr[kb], best[kb].idx2 >= 0 ? best[kb].v2 : {ninf});")
+            b.append("        bool ok = true;")
+            m_i = 0
+            lohi = []
+            for p, (pos, ci, px, pc) in enumerate(gi["axes"]):
+                b.append(f"        float lo_{p} = gK[kb][{p}], hi_{p} = lo_{p}, e_{p} = gE[kb][{p}];")
+                for nm in pc:
+                    k = ks[nm]
+                    b.append(f"        {{ const float mm = gM[kb][{m_i}]; lo_{p} += mm >= 0.0f ? mm * lo{k} : mm * hi{k}; "
+                             f"hi_{p} += mm >= 0.0f ? mm * hi{k} : mm * lo{k}; e_{p} += fabsf(mm) * am{k}; }}")
+                    m_i += 1
+                b.append(f"        e_{p} = 0.02f + 4e-6f * e_{p};")
+                b.append(f"        const int n_{p} = C.n{ti}_{pos};")
+                b.append(f"        ok = ok && lo_{p} - e_{p} >= 0.0f && hi_{p} + e_{p} <= (float)(n_{p} - 1);")
+                lohi.append(p)
+            b.append("        if (ok) {")
+            for p in lohi:
+                b.append(f"          const int L_{p} = (int)(lo_{p} - e_{p}), H_{p} = min((int)(hi_{p} + e_{p}) + 1, n_{p} - 1);")
+            b.append(f"          float mx = {ninf}, ab = 0.0f;")
+            if len(lohi) == 1:
+                b.append(f"          const float2* row = {gi['bst']} + (i64)keyr[kb] * ((n_0 + 15) >> 4);")
+                b.append("          for (int b1 = L_0 >> 4; b1 <= (H_0 >> 4); ++b1) {")
+                b.append("            const float2 st = __ldg(row + b1);")
+                b.append("            mx = lcm_nanmax(mx, st.x); ab = fmaxf(ab, st.y);")
+                b.append("          }")
+            else:
+                T1, T2 = self.GROUP_TILE
+                b.append(f"          const int nb1 = (n_0 + {T1 - 1}) / {T1}, nb2 = (n_1 + {T2 - 1}) / {T2};")
+                b.append(f"          const float2* base = {gi['bst']} + (i64)keyr[kb] * nb1 * nb2;")
+                b.append(f"          for (int b1 = L_0 / {T1}; b1 <= H_0 / {T1}; ++b1) {{")
+                b.append(f"            for (int b2 = L_1 / {T2}; b2 <= H_1 / {T2}; ++b2) {{")
+                b.append("              const float2 st = __ldg(base + (i64)b1 * nb2 + b2);")
+                b.append("              mx = lcm_nanmax(mx, st.x); ab = fmaxf(ab, st.y);")
+                b.append("            }")
+                b.append("          }")
+            b.append("          const float ub = um + beta_f * mx;")
+            b.append("          const float marg = 3.8e-6f * (fabsf(um) + beta_f * ab);")
+            b.append("          skip = ub + marg < th;")
+            b.append("        }")
+            b.append("      }")
+            b.append("    }")
+            b.append("    run[kb] = act[kb] && !skip;")
+            b.append("    any = any || run[kb];")
+            b.append("  }")
+            b.append("  if (!any) continue;")
+            b.append(f"  for (int t = lane; t < m; t += {LANES}) {{")
+            b.append("    const int j = jb + t * gS;")
+            b.append(f"    AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
+            b.append("    const int aidx = ad * n_ac + j;")
+            b.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
+            b.append("      float q;")
+            b.append(f"      if (run[kb] && {call}) {{ if (q != q) best[kb].nan = 1; else best[kb].add(q, aidx); }}")
+            b.append("    }")
+            b.append("  }")
+            b.append("}")
+            o += ["  " + x for x in b]
             o.append("}")
             return o
 
         any_pruned = False
+        n_gacts = 0
         if unswitch:
             rid_expr = f"(int)PVd[{[id(x) for x in bP].index(id(self.tr.regime_id))}]" if rid_phase == "P" else None
             if rid_phase == "D":
@@ -1290,10 +1598,11 @@ class RegimeKernels:
             for ti, t in enumerate(self.targets):
                 ap(f"      {'if' if first else 'else if'} (rid == {t.spec.rid}) {{")
                 first = False
-                pi = prune_info(ti)
-                if pi is not None:
+                gi = group_info(ti)
+                if gi is not None:
                     any_pruned = True
-                body = inner_loop(SA.format(ti + 1)) if pi is None else inner_loop_pruned(SA.format(ti + 1), pi)
+                    n_gacts = max(n_gacts, len(GP["acts"]))
+                body = inner_loop(SA.format(ti + 1)) if gi is None else inner_loop_groups(SA.format(ti + 1), gi)
                 for s_ in body:
                     ap("        " + s_)
                 ap("      }")
@@ -1306,7 +1615,7 @@ class RegimeKernels:
                 ap("      " + s_)
         ap("    }")
         if any_pruned:
-            L.insert(gumax_at, f"  __shared__ float gumax[{(CH + G - 1) // G}];")
+            L.insert(gumax_at, f"  __shared__ float gU[{GMAX}], gLo[{max(n_gacts, 1) * GMAX}], gHi[{max(n_gacts, 1) * GMAX}];")
         self.prunes_groups = any_pruned
 
         # ---- reduction and epilogue

@@ -271,6 +271,47 @@ __device__ __forceinline__ int lcm_find_item(const int* __restrict__ prefix, int
   return lo;
 }
 
+// Tile statistics of float expectation rows over two continuous axes, for the
+// exact skipping of action groups in the single-precision search.  Each row k
+// is an (n1 x n2) row-major block; per tile of 16 (axis 1) x 2 (axis 2) nodes
+// it records (maximum -- NaN when any value is NaN --, largest finite |value|)
+// at bst[(k * nb1 + b1) * nb2 + b2], nb1 = ceil(n1 / 16), nb2 = ceil(n2 / 2).
+// Item words: 0 the float table, 1 the statistics, 2 K (rows), 3 n1, 4 n2.
+// One CTA (a multiple of 32 threads) per (item, row, 16-node band of axis 1):
+// tile_prefix counts K * nb1 tiles per item.  The threads walk axis 2 (unit
+// stride, coalesced) and pair up by a shuffle.
+__device__ __forceinline__ void lcm_tile_stats2(const i64* __restrict__ items, const int* __restrict__ tile_prefix,
+                                                int n_items, int n_tiles) {
+  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int item = lcm_find_item(tile_prefix, n_items, tile);
+    const i64* it = items + (i64)item * 5;
+    const float* __restrict__ ev = lcm_wp<const float>(it, 0);
+    float2* bst = lcm_wp<float2>(it, 1);
+    const int n1 = lcm_wi(it, 3), n2 = lcm_wi(it, 4);
+    const int nb1 = (n1 + 15) >> 4, nb2 = (n2 + 1) >> 1;
+    const int r = tile - tile_prefix[item];  // k * nb1 + b1
+    const int k = r / nb1, b1 = r - k * nb1;
+    const float* rowk = ev + (i64)k * n1 * n2;
+    const int i1a = b1 * 16, i1b = min(n1, i1a + 16);
+    for (int c0 = 0; c0 < n2; c0 += blockDim.x) {  // uniform over the CTA
+      const int i2 = c0 + (int)threadIdx.x;
+      float mx = -lcm_lim<float>::inf(), ab = 0.0f;
+      if (i2 < n2) {
+        for (int i1 = i1a; i1 < i1b; ++i1) {
+          const float v = __ldg(rowk + (i64)i1 * n2 + i2);
+          mx = lcm_nanmax(mx, v);
+          if (lcm_isfinite(v)) ab = fmaxf(ab, fabsf(v));
+        }
+      }
+      const float omx = __shfl_xor_sync(0xffffffffu, mx, 1);
+      const float oab = __shfl_xor_sync(0xffffffffu, ab, 1);
+      mx = lcm_nanmax(mx, omx);
+      ab = fmaxf(ab, oab);
+      if (i2 < n2 && (i2 & 1) == 0) bst[(i64)r * nb2 + (i2 >> 1)] = make_float2(mx, ab);
+    }
+  }
+}
+
 // Logsum over discrete choices with max shift (logsum.py:32-64).
 template <typename T, int ND>
 __device__ __forceinline__ T lcm_logsum(const T* vals, T scale) {

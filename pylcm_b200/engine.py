@@ -393,10 +393,18 @@ class SolvePlan:
                 e64 = torch.empty((n, t.K, ncols), dtype=torch.float64, device=dev)
                 e32 = torch.empty((n, t.K, ncols), dtype=torch.float32, device=dev) if fp32 else None
                 self.ev[k] = (e64, e32, ncols, cblk)
-                # block statistics of the float table rows (max, finite |max|
-                # per 16 columns) for the search's exact group skipping
-                if fp32 and not t.det_pos:
+                # block statistics of the float table rows (max, finite |max|)
+                # for the search's exact group skipping: per 16 columns of a
+                # one-axis table (kernel b), per 16 x 2 tile of a two-axis one
+                # (the statistics kernel)
+                gs = rk.group_stats(t)
+                if gs == 1:
                     self.bst[k] = torch.empty((n, t.K, (ncols + 15) // 16, 2), dtype=torch.float32, device=dev)
+                elif gs == 2:
+                    n1, n2 = (t.spec.states[p].size for p in t.cont_pos)
+                    T1, T2 = rk.GROUP_TILE
+                    nt = ((n1 + T1 - 1) // T1) * ((n2 + T2 - 1) // T2)
+                    self.bst[k] = torch.empty((n, t.K, nt, 2), dtype=torch.float32, device=dev)
 
         # action tables (kernel a0 output) per (regime, target set), reused across periods
         self.atab: dict[tuple, Any] = {}
@@ -448,7 +456,7 @@ class SolvePlan:
         resolvers = self.resolvers
         age = float(self.eng.model.ages.values[period])
         pbuf = self.params[pkey]
-        out = {"expect": [], "tv": []}
+        out = {"expect": [], "tv": [], "stats": []}
         # kernel (b) records
         for t in rk.targets:
             if t.scalar:
@@ -459,10 +467,19 @@ class SolvePlan:
             bst = self.bst.get((s.name, targets, t.spec.name))
             Vt = self.V[t.spec.name]
             tslot = self.slot[t.spec.name][period + 1]
+            gs = rk.group_stats(t) if bst is not None else 0
+            if gs == 2:
+                # the statistics kernel's records (the same every period)
+                n1, n2 = (t.spec.states[p].size for p in t.cont_pos)
+                srec = np.zeros((n, 5), dtype=np.int64)
+                srec[:, 0] = [e32[i].data_ptr() for i in range(n)]
+                srec[:, 1] = [bst[i].data_ptr() for i in range(n)]
+                srec[:, 2], srec[:, 3], srec[:, 4] = t.K, n1, n2
+                out["stats"].append((t, srec, [t.K * ((n1 + rk.GROUP_TILE[0] - 1) // rk.GROUP_TILE[0])] * n))
             recs = []
             for i in range(n):
                 r = np.zeros(rk.e_words_for(t), dtype=np.int64)
-                r[8 + len(t.spec.states)] = bst[i].data_ptr() if bst is not None else 0
+                r[8 + len(t.spec.states)] = bst[i].data_ptr() if gs == 1 else 0
                 r[0] = Vt[i, tslot].data_ptr()
                 r[1] = e64[i].data_ptr()
                 r[2] = e32[i].data_ptr() if e32 is not None else 0
@@ -633,6 +650,7 @@ class SolvePlan:
             X[:, :, 4] = pa[:, None]
             X[:, :, 5] = agew[:, None]
             g["expect"].append((t, X, tiles))
+        g["stats"] = {id(t): (srec, tiles) for t, srec, tiles in tm["stats"]}
         return g
 
     def _gs_launches(self, b: "_Records", rk: RegimeKernels, period: int, s: RegimeSpec, targets, pkey) -> None:
@@ -658,6 +676,9 @@ class SolvePlan:
                       sh["smem"], period)
             else:
                 b.add("expect", rk, rk.expect_name(t), X[k], tiles, 256, 0, period)
+            st = g["stats"].get(id(t))
+            if st is not None:
+                b.add("stats", rk, rk.stats_name(), st[0], st[1], 256, 0, period)
         rows = g["rows"][k]
         self.records[(period, s.name)] = (rk, rows)
         b.add("atab", rk, rk.atab_name(), rows, g["atab_tiles"], 256, 0, period)

@@ -174,6 +174,7 @@ class Module:
             "atab": self.ctx.lib.lcmx_bellman_step,
             "expect": self.ctx.lib.lcmx_expectation,
             "expect_tc": self.ctx.lib.lcmx_expectation,
+            "stats": self.ctx.lib.lcmx_expectation,
             "egm": self.ctx.lib.lcmx_egm_step,
         }[kind]
         args = LaunchArgs(items_ptr, prefix_ptr, n_items, n_tiles, grid, block, smem)

@@ -1,20 +1,44 @@
 """Exact skipping of action groups in the single-precision search.
 
-A group of consecutive continuous actions is skipped only when an upper bound
-of its Q values is below the state's current second-best value, so the
+A group (a run of consecutive values of one continuous action, the others
+fixed) is skipped only when all its members violate a constraint or an upper
+bound of its Q values is below the state's current second-best value, so the
 search's two candidates -- and the published V and policy -- are exactly
-those of the full search.  CPU: which kernels skip (eligibility); GPU: the
-skipping kernels give bit-identical V and policies to the same kernels with
-skipping turned off, on models with infeasible regions (-inf values), several
-parameter draws and launch shapes."""
+those of the full search.  CPU: the affine split of next-state laws and
+constraints, which kernels skip (eligibility); GPU: the skipping kernels give
+bit-identical V and policies to the same kernels with skipping turned off, on
+models with one and two continuous actions and one- and two-axis targets,
+infeasible regions (-inf values), several parameter draws and launch shapes."""
 
 import dataclasses
 
 import numpy as np
 import pytest
 
+from pylcm_b200 import ir
+from pylcm_b200.codegen import _affine_split
 from pylcm_b200.engine import SolveEngine, default_config
 from tests import models as M
+
+
+def test_affine_split():
+    c, h = ir.var("action", "c", "f"), ir.var("action", "h", "f")
+    w, z, r = ir.var("state", "w", "f"), ir.var("state", "z", "f"), ir.param("r")
+    env = {("action", "c"): 3.0, ("action", "h"): 0.5, ("state", "w"): 7.0, ("state", "z"): -0.3}
+    x = (1 + r) * (w - c) + ir.un("exp", z) * w * h - c / 4.0 + (h * 2.0).astype(float)
+    x0, co = _affine_split(x, {"c", "h"})
+    assert set(co) == {"c", "h"}
+    for k in ("c", "h"):
+        assert not any(kind == "action" for kind, _ in ir.const(co[k]).deps())
+    ev = lambda e: float(ir.evaluate(e, env, {"r": 0.04}))  # noqa: E731
+    got = ev(x0) + ev(co["c"]) * 3.0 + ev(co["h"]) * 0.5
+    assert abs(got - ev(x)) < 1e-12
+    # pieces that are not affine in the actions are rejected
+    for bad in (w - ir.un("floor", c), c * h, ir.where(c > 1.0, c, 0.0), c ** 2.0, w / c, ir.un("log", c)):
+        assert _affine_split(bad, {"c", "h"}) is None
+    # an expression free of the actions is its own x0
+    x0, co = _affine_split(w * 2.0, {"c"})
+    assert co == {} and x0 is (w * 2.0)
 
 
 def _kernels(model, params, precision, **cfg):
@@ -39,9 +63,14 @@ def test_eligibility():
     assert not any(r.prunes_groups for r in k.values())
     k = _kernels(M.stochastic_model(4, 30, 40), M.stochastic_params(), "fp32", prune=False)
     assert not any(r.prunes_groups for r in k.values())
-    # two continuous target states: not eligible
+    # two continuous actions, two continuous target states: tile statistics
     k = _kernels(M.hc_model(3, 10, 4, 4, 8), M.hc_params(0, 4), "fp32")
-    assert not any(r.prunes_groups for r in k.values())
+    assert k["alive"].prunes_groups and not k["terminal"].prunes_groups
+    assert [k["alive"].group_stats(t) for t in k["alive"].targets] == [2]
+    assert "lcm_tile_stats_" in k["alive"].source()
+    g = k["alive"]._groups
+    assert g["cacts"][g["scan"]] == "consumption" and set(g["acts"]) == {"consumption", "hours"}
+    assert [op for op, _, _ in g["cons"]] == ["<="]  # the borrowing constraint
     # a stochastic regime transition (several targets per action): not eligible
     k = _kernels(M.mass_model(), M.mass_params(), "fp32")
     assert not any(r.prunes_groups for r in k.values())
@@ -52,6 +81,8 @@ CASES = {
                    lambda: [M.stochastic_params(beta=b, crra=c) for b, c in ((0.95, 2.0), (0.9, 3.5), (0.97, 1.2))]),
     "retirement": (lambda: M.retirement_model(6, 150, 150), lambda: [M.retirement_params(b) for b in (0.95, 0.8)]),
     "regression": (lambda: M.regression_model(4), lambda: [M.regression_params(4)]),
+    # two continuous actions (consumption x hours), wealth x human capital targets
+    "human_capital": (lambda: M.hc_model(5, 120, 12, 6, 90), lambda: [M.hc_params(s, 6) for s in range(3)]),
 }
 
 
@@ -76,3 +107,32 @@ def test_skipping_is_exact(case, lanes, sb):
     for r in a.V:
         assert torch.equal(torch.nan_to_num(a.V[r], nan=7.0), torch.nan_to_num(b.V[r], nan=7.0)), r
         assert torch.equal(a.pol[r], b.pol[r]), r
+
+
+@pytest.mark.gpu
+def test_tile_statistics_match_the_float_table():
+    """The statistics kernel's (max, largest finite |value|) per 16 x 2 tile
+    of a two-axis float table, against NumPy over the table it read."""
+    import torch
+
+    model = M.hc_model(4, 70, 9, 5, 40)
+    plan = SolveEngine(model, "fp32").plan([M.hc_params(s, 5) for s in range(2)])
+    plan.run()
+    torch.cuda.synchronize()
+    checked = 0
+    for key, bst in plan.bst.items():
+        e64, e32, ncols, cblk = plan.ev[key]
+        if bst.shape[2] == (ncols + 15) // 16:
+            continue  # one-axis statistics (kernel b)
+        n1, n2 = 70, 9
+        ev = e32.cpu().numpy().reshape(e32.shape[0], e32.shape[1], n1, n2)
+        p1, p2 = (-n1) % 16, (-n2) % 2
+        pad = np.pad(ev, ((0, 0), (0, 0), (0, p1), (0, p2)), constant_values=-np.inf)
+        t = pad.reshape(ev.shape[0], ev.shape[1], (n1 + p1) // 16, 16, (n2 + p2) // 2, 2)
+        mx = t.max(axis=(3, 5))
+        ab = np.where(np.isfinite(t), np.abs(t), 0.0).max(axis=(3, 5))
+        got = bst.cpu().numpy().reshape(mx.shape + (2,))
+        np.testing.assert_array_equal(got[..., 0], mx.astype(np.float32))
+        np.testing.assert_array_equal(got[..., 1], ab.astype(np.float32))
+        checked += 1
+    assert checked == 1
