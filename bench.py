@@ -699,7 +699,7 @@ def run_hc(args, local: int):
     from pylcm_b200.engine import SolveEngine
 
     stream = torch.cuda.current_stream()
-    model = E.hc_model(60, 1000, 50, 32, 300)
+    model = E.hc_model(args.hc_periods, 1000, 50, 32, 300)
     plist = [E.hc_params(seed=k) for k in range(args.hc_batch)]
     chunk = min(args.hc_chunk, args.hc_batch)
     fast_eng = SolveEngine(model, "fp32", device=local)
@@ -1086,6 +1086,7 @@ def main() -> None:
     ap.add_argument("--dcegm-batch", type=int, default=32)
     ap.add_argument("--hc-batch", type=int, default=256)
     ap.add_argument("--hc-chunk", type=int, default=32)
+    ap.add_argument("--hc-periods", type=int, default=60, help="periods of the two-state model (60: the config)")
     ap.add_argument("--only", choices=["serving", "dcegm", "hc"], default=None,
                     help="run one extra section alone on GPU 0 and print its JSON (for profiling)")
     args = ap.parse_args()
