@@ -147,6 +147,35 @@ int lcmx_fues_scan(lcmx_ctx* ctx, const double* grid, const double* policy, cons
 int lcmx_fues_step(lcmx_ctx* ctx, const void* items, const int* tile_prefix, int n_items, int n_rows,
                    int max_n_in, void* stream);
 
+/* Kernel (c), part 2, the LTM envelope (LTMEnvelope): the local-upper-bound
+ * brute method of src/_lcm/egm/upper_envelope/ltm.py:35-190 (refine_envelope),
+ * on `n_rows` contiguous candidate rows of length n_in.  Segments join
+ * consecutive candidates in input order; at each live candidate abscissa
+ * (ascending) the envelope is the largest interpolant over the bracketing
+ * segments.  Outputs as lcmx_fues_scan's.  Rows of up to 4096 candidates. */
+int lcmx_ltm_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value, int n_rows,
+                  int n_in, double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
+                  void* stream);
+
+/* Kernel (c), part 2, the RFC envelope (RFCEnvelope): the rooftop cut of
+ * src/_lcm/egm/upper_envelope/rfc.py:40-220 (refine_envelope) with the
+ * candidates' marginal utility (the value rows' supgradient) as tangent
+ * slopes, `search_radius` neighbours on each side and the policy-jump
+ * threshold `jump_thresh`.  Outputs as lcmx_fues_scan's (a subset of the
+ * sorted candidates).  Rows of up to 4096 candidates. */
+int lcmx_rfc_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
+                  const double* marginal_utility, int n_rows, int n_in, int search_radius, double jump_thresh,
+                  double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept, void* stream);
+
+/* Item form of the LTM (kind 1) and RFC (kind 2) envelopes, one launch over
+ * the rows of n_items candidate blocks; item records of 13 64-bit words:
+ * grid, policy, value, marginal utility (RFC; 0 for LTM), grid_out,
+ * policy_out, value_out, n_kept (int32) device pointers, then n_rows, n_in,
+ * n_out, jump_thresh (double bits) and the search radius; tile_prefix[i] is
+ * the first row of item i.  max_n_in (at most 4096) sizes the shared memory. */
+int lcmx_envelope_step(lcmx_ctx* ctx, int kind, const void* items, const int* tile_prefix, int n_items,
+                       int n_rows, int max_n_in, void* stream);
+
 /* lcmx_fues_scan without a caller workspace: for callers that cannot call
  * cudaMalloc on this path (code running inside another runtime's execution,
  * such as an XLA FFI custom-call handler).  No counterpart in the reference.

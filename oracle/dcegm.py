@@ -1,4 +1,5 @@
-"""Oracle: DC-EGM backward induction with the FUES envelope (test infrastructure only).
+"""Oracle: DC-EGM backward induction with the FUES, LTM or RFC envelope (test
+infrastructure only).
 
 Restates the reference's endogenous-grid step
 (``src/_lcm/egm/step_core.py:156-616``) in NumPy float64, per (discrete
@@ -13,7 +14,9 @@ state x discrete action) row:
 2. Euler inversion c = (u')^{-1}(max(beta E[mu'], eps)), R = A + c,
    v = u(c) + beta E[V'] (``egm/euler.py:18-68``);
 3. constrained candidates c_k = span 1e-4 ratio^k (``step_core.py:443-514``);
-4. FUES upper envelope (``oracle/fues.py``);
+4. the upper envelope: FUES (``oracle/fues.py``), or LTM / RFC
+   (``oracle/envelopes.py``; RFC with the candidates' u'(c) as supgradient,
+   0 for dead candidates, ``step_core.py:414-440``);
 5. publication on the state grid: the refined value row read with a
    Fritsch-Carlson-limited cubic Hermite interpolant whose node slopes are
    u'(c), floored at (and below the first refined point replaced by) the
@@ -34,6 +37,7 @@ import math
 
 import numpy as np
 
+from oracle.envelopes import refine_ltm, refine_rfc
 from oracle.fues import refine
 from oracle.grid_search import _process_tables, bellman_step
 from pylcm_b200 import ir
@@ -309,8 +313,19 @@ def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R, value_mu=N
         cand_c = np.where(dead, np.nan, cand_c)
         cand_v = np.where(dead, np.nan, cand_v)
         cand_s = np.where(dead, np.nan, cand_s)
-        rg, rc, rv, n_kept = refine(cand_g, cand_c, cand_v, cand_s, er.n_pad, er.jump_thresh,
-                                    er.scan_window or None)
+        if er.envelope == "ltm":
+            rg, rc, rv, n_kept = refine_ltm(cand_g, cand_c, cand_v, er.n_pad)
+        elif er.envelope == "rfc":
+            # candidate supgradient u'(c), 0 for dead candidates (step_core.py:414-440)
+            envm = dict(env)
+            envm[("action", er.C)] = np.where(dead, 1.0, cand_c)
+            with np.errstate(all="ignore"):
+                cm = np.broadcast_to(np.asarray(_eval(er.dU, envm, tr), dtype=np.float64), cand_c.shape)
+            cm = np.where(dead, 0.0, cm)
+            rg, rc, rv, n_kept = refine_rfc(cand_g, cand_c, cand_v, cm, er.n_pad, er.search_radius, er.jump_thresh)
+        else:
+            rg, rc, rv, n_kept = refine(cand_g, cand_c, cand_v, cand_s, er.n_pad, er.jump_thresh,
+                                        er.scan_window or None)
         envr = dict(env)
         envr[("action", er.C)] = np.where(np.isnan(rc), 1.0, rc)
         with np.errstate(all="ignore"):

@@ -50,7 +50,7 @@ from pylcm_b200.regime import (
     MarkovTransition,
     Regime,
 )
-from pylcm_b200.solvers import DCEGM, FUESEnvelope, GridSearch
+from pylcm_b200.solvers import DCEGM, FUESEnvelope, GridSearch, LTMEnvelope, MSSEnvelope, RFCEnvelope
 
 __all__ = [
     "DCEGM",
@@ -60,6 +60,9 @@ __all__ = [
     "DiscreteGrid",
     "ExtremeValueTasteShocks",
     "FUESEnvelope",
+    "LTMEnvelope",
+    "MSSEnvelope",
+    "RFCEnvelope",
     "GridInitializationError",
     "GridSearch",
     "InvalidInitialConditionsError",

@@ -17,7 +17,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_lib"
 LIB = OUT_DIR / "liblcmx.so"
-SOURCES = ["lcmx.cu", "fues.cu"]
+SOURCES = ["lcmx.cu", "fues.cu", "envelopes.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

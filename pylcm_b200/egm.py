@@ -115,6 +115,8 @@ class EgmRegime:
     taste_scale: float | None
     feasible: ir.Expr
     tracer: Any
+    envelope: str = "fues"  # the upper envelope: "fues" | "ltm" | "rfc"
+    search_radius: int = 10  # RFC: neighbours inspected on each side
 
     @property
     def n_rows(self) -> int:
@@ -254,8 +256,10 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
         n_constrained=nc,
         ratio=ratio,
         n_pad=n_pad,
-        jump_thresh=float(solver.envelope.jump_thresh),
-        scan_window=int(solver.envelope.n_points_to_scan or 0),
+        jump_thresh=float(getattr(solver.envelope, "jump_thresh", 2.0)),
+        scan_window=int(getattr(solver.envelope, "n_points_to_scan", None) or 0),
+        envelope={"FUESEnvelope": "fues", "LTMEnvelope": "ltm", "RFCEnvelope": "rfc"}[type(solver.envelope).__name__],
+        search_radius=int(getattr(solver.envelope, "search_radius", 10)),
         taste_scale=taste,
         feasible=feasible,
         tracer=t,

@@ -60,6 +60,9 @@ class EgmKernels:
         self.W_NGRID = take()
         self.W_GRID = take()
         self.W_CG, self.W_CC, self.W_CV, self.W_CS = take(), take(), take(), take()
+        # candidate marginal utility u'(c) (the value rows' supgradient, read
+        # by the RFC envelope; 0 for dead candidates)
+        self.W_CM = take() if self.er.envelope == "rfc" else -1
         self.W_EV0 = take()
         self.W_RG, self.W_RC, self.W_RV, self.W_MU, self.W_NK = take(), take(), take(), take(), take()
         self.W_V = take()
@@ -330,6 +333,14 @@ class EgmKernels:
             ue = e3.emit(er.U)
             return e3.lines, ue
 
+        def marginal_at(cexpr: str, pref: str) -> tuple[list, str]:
+            p2 = dict(em.vals)
+            p2[id(cvar)] = cexpr
+            e3 = Emitter("double", self.param_off, p2, pref)
+            de = e3.emit(er.dU)
+            return e3.lines, de
+
+        rfc = er.envelope == "rfc"
         ul, ue = utility_at("cj", "u")
         body += ul
         body.append(f"const double vj = (double)({ue}) + ({beta}) * EV;")
@@ -339,7 +350,12 @@ class EgmKernels:
         body.append(f"double* CS = lcm_wp<double>(it, {self.W_CS}) + (i64)row * n_cand;")
         body.append("if (live) { const bool dead = vj == -LCM_INF;")
         body.append("  CG[nc + j] = dead ? LCM_NAN : mj; CC[nc + j] = dead ? LCM_NAN : cj;")
-        body.append("  CV[nc + j] = dead ? LCM_NAN : vj; CS[nc + j] = dead ? LCM_NAN : A; }")
+        body.append("  CV[nc + j] = dead ? LCM_NAN : vj; CS[nc + j] = dead ? LCM_NAN : A;")
+        if rfc:
+            ml, me = marginal_at("cj", "w")
+            body += ["  " + x for x in ml]
+            body.append(f"  lcm_wp<double>(it, {self.W_CM})[(i64)row * n_cand + nc + j] = dead ? 0.0 : (double)({me});")
+        body.append("}")
         body.append("if (live && j == 0) {")
         body.append(f"  lcm_wp<double>(it, {self.W_EV0})[row] = EV;")
         body.append(f"  const int ng = lcm_wi(it, {self.W_NGRID});")
@@ -354,6 +370,10 @@ class EgmKernels:
         body.append("    const bool dead = empty || vk == -LCM_INF;")
         body.append("    CG[k] = dead ? LCM_NAN : A + ck; CC[k] = dead ? LCM_NAN : ck;")
         body.append("    CV[k] = dead ? LCM_NAN : vk; CS[k] = dead ? LCM_NAN : A;")
+        if rfc:
+            ml2, me2 = marginal_at("ck", "z")
+            body += ["    " + x for x in ml2]
+            body.append(f"    lcm_wp<double>(it, {self.W_CM})[(i64)row * n_cand + k] = dead ? 0.0 : (double)({me2});")
         body.append(f"    ck *= {er.ratio!r};")
         body.append("  }")
         body.append("}")

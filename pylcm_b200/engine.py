@@ -128,6 +128,7 @@ class _Records:
 SM_COUNT = 148
 RESIDENT_THREADS_PER_SM = 1024
 FUES_SMEM_MAX_N = 4096  # longest candidate row of the item-form FUES launch
+ENVELOPE_MAX_N = 4096  # longest candidate row of the LTM / RFC envelope kernels
 
 
 def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> LaunchConfig:
@@ -349,6 +350,8 @@ class SolvePlan:
                 "mu": torch.full((nslot, n, nrow, npad), float("nan"), **f64),
                 "nk": torch.zeros((nslot, n, nrow), dtype=torch.int32, device=dev),
                 "cand": [torch.empty((n, nrow, ncand), **f64) for _ in range(4)],
+                # candidate marginal utilities (the RFC envelope's tangent slopes)
+                "cm": torch.empty((n, nrow, ncand), **f64) if er.envelope == "rfc" else None,
                 "ev0": torch.empty((n, nrow), **f64),
                 "npad": npad,
                 "nrow": nrow,
@@ -436,7 +439,7 @@ class SolvePlan:
                 self._vmu_launch(b, s, targets, period)
         self.launches = b.launches
         self._rec = b
-        for rk in {id(l.module): l.module for l in self.launches if l.kind != "fues"}.values():
+        for rk in {id(l.module): l.module for l in self.launches if l.kind not in ("fues", "env")}.values():
             eng.module(rk)
         if upload:
             self.items, self.prefix = b.tensors(torch, dev)
@@ -793,6 +796,8 @@ class SolvePlan:
             r[ek.W_GRID] = grid.data_ptr()
             for wname, arr in zip(("W_CG", "W_CC", "W_CV", "W_CS"), b["cand"]):
                 r[getattr(ek, wname)] = arr[i].data_ptr()
+            if b["cm"] is not None:
+                r[ek.W_CM] = b["cm"][i].data_ptr()
             r[ek.W_EV0] = b["ev0"][i].data_ptr()
             cslot = period % 2
             r[ek.W_RG] = b["rg"][cslot, i].data_ptr()
@@ -840,10 +845,17 @@ class SolvePlan:
         frecs = []
         for i in range(n):
             fr = np.zeros(13, dtype=np.int64)
-            fr[0], fr[1], fr[2], fr[3] = cg[i].data_ptr(), cc[i].data_ptr(), cv[i].data_ptr(), cs[i].data_ptr()
+            fr[0], fr[1], fr[2] = cg[i].data_ptr(), cc[i].data_ptr(), cv[i].data_ptr()
             fr[8], fr[9], fr[10] = nrow, ncand, npad
             fr[11] = _f2w(er.jump_thresh)
-            fr[12] = er.scan_window
+            if er.envelope == "fues":
+                fr[3] = cs[i].data_ptr()  # exogenous savings sources
+                fr[12] = er.scan_window
+            else:
+                # LTM / RFC item words: 3 the candidates' marginal utility
+                # (RFC), 12 the search radius
+                fr[3] = b["cm"][i].data_ptr() if er.envelope == "rfc" else 0
+                fr[12] = er.search_radius
             frecs.append(fr)
         out["recs"] = np.stack(recs).astype(np.int64)
         out["fues"] = np.stack(frecs).astype(np.int64)
@@ -902,7 +914,14 @@ class SolvePlan:
         # FUES over every instance's candidate rows (one tile per row)
         b = self.egm[name]
         ncand = b["ncand"]
-        if ncand <= FUES_SMEM_MAX_N:
+        if er.envelope != "fues":
+            if ncand > ENVELOPE_MAX_N:
+                raise NotImplementedError(
+                    f"{name}: the {er.envelope.upper()} envelope handles candidate rows of up to "
+                    f"{ENVELOPE_MAX_N} points ({ncand} here)")
+            rec.add("env", None, f"lcmx_envelope_step:{1 if er.envelope == 'ltm' else 2}", g["fues"][k],
+                    g["tiles_f"], 0, ncand, period)
+        elif ncand <= FUES_SMEM_MAX_N:
             rec.add("fues", None, "lcmx_fues_step", g["fues"][k], g["tiles_f"], 0, ncand, period)
         else:
             rec.append(
@@ -920,6 +939,19 @@ class SolvePlan:
 
         def launch(stream):
             ctx.fues_step(*args, stream)
+
+        return launch
+
+    def _env_item_launch(self, l: Launch, ib: int, pb: int):
+        """The LTM / RFC envelope over item records (kind in the kernel name)."""
+        from pylcm_b200.runtime import get_context
+
+        ctx = get_context(self.eng.device if hasattr(self, "eng") else self.plans[0].eng.device)
+        kind = int(l.kernel.rsplit(":", 1)[1])
+        args = (ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.smem)
+
+        def launch(stream):
+            ctx.envelope_step(kind, *args, stream)
 
         return launch
 
@@ -959,6 +991,9 @@ class SolvePlan:
         for l in launches:
             if l.kind == "fues":
                 out.append(self._fues_item_launch(l, ib, pb) if l.module is None else self._fues_launch(*l.module[1:5]))
+                continue
+            if l.kind == "env":
+                out.append(self._env_item_launch(l, ib, pb))
                 continue
             out.append(
                 l.module.module.prepared(
@@ -1170,6 +1205,9 @@ class BatchPlan:
                 else:
                     pl, name, slot, thr, window, sl = l.module
                     out.append(pl._fues_launch(name, slot, thr, window, sl))
+                continue
+            if l.kind == "env":
+                out.append(SolvePlan._env_item_launch(self, l, ib, pb))
                 continue
             out.append(
                 l.module.module.prepared(

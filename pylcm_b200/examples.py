@@ -339,12 +339,14 @@ def _egm_nr_ret(period, last_decision_period):
     return jnp.where(period >= last_decision_period, EgmRegimeId.dead, EgmRegimeId.retired)
 
 
-def dcegm_model(n_periods=40, n_savings=2000, n_wealth=2000, taste=False, n_constrained=20, n_points_to_scan=None):
+def dcegm_model(n_periods=40, n_savings=2000, n_wealth=2000, taste=False, n_constrained=20, n_points_to_scan=None,
+                envelope=None):
     """Savings grid 500 (i/(n-1))^3, wealth grid linspace(0, 500, n_wealth);
-    FUES with an exhaustive look-ahead unless `n_points_to_scan` is given."""
+    FUES with an exhaustive look-ahead unless `n_points_to_scan` is given, or
+    the given `envelope` configuration."""
     sav = IrregSpacedGrid(points=tuple(500.0 * (i / (n_savings - 1)) ** 3 for i in range(n_savings)))
     solver = DCEGM(savings_grid=sav, n_constrained_points=n_constrained,
-                   envelope=FUESEnvelope(n_points_to_scan=n_points_to_scan))
+                   envelope=envelope if envelope is not None else FUESEnvelope(n_points_to_scan=n_points_to_scan))
     margin = LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings")
     wealth = LinSpacedGrid(start=0, stop=500, n_points=n_wealth)
     cons = LinSpacedGrid(start=0.1, stop=500, n_points=200)

@@ -33,6 +33,9 @@ EXPORTED = (
     "lcmx_fues_step",
     "lcmx_copy_rows_d2h",
     "lcmx_module_status",
+    "lcmx_ltm_scan",
+    "lcmx_rfc_scan",
+    "lcmx_envelope_step",
 )
 
 
@@ -90,6 +93,9 @@ def load_library() -> ctypes.CDLL:
             "lcmx_fues_scan_static": ([vp, vp, vp, vp, vp, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
             "lcmx_fues_step": ([vp, vp, vp, ip, ip, ip, vp], ip),
             "lcmx_module_status": ([vp, cp, ctypes.POINTER(ip), ip], ip),
+            "lcmx_ltm_scan": ([vp, vp, vp, vp, ip, ip, vp, vp, vp, ip, vp, vp], ip),
+            "lcmx_rfc_scan": ([vp, vp, vp, vp, vp, ip, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
+            "lcmx_envelope_step": ([vp, ip, vp, vp, ip, ip, ip, vp], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
@@ -159,6 +165,24 @@ class Context:
                                     int(n_points_to_scan), grid_out, policy_out, value_out, n_out, n_kept,
                                     workspace, workspace_bytes, stream)
         )
+
+
+    def ltm_scan(self, grid, policy, value, n_rows, n_in, grid_out, policy_out, value_out, n_out, n_kept,
+                 stream) -> None:
+        """LTM envelope of contiguous candidate rows (device pointers)."""
+        self.check(self.lib.lcmx_ltm_scan(self.h, grid, policy, value, n_rows, n_in, grid_out, policy_out,
+                                          value_out, n_out, n_kept, stream))
+
+    def rfc_scan(self, grid, policy, value, marginal_utility, n_rows, n_in, search_radius, jump_thresh, grid_out,
+                 policy_out, value_out, n_out, n_kept, stream) -> None:
+        """RFC envelope of contiguous candidate rows (device pointers)."""
+        self.check(self.lib.lcmx_rfc_scan(self.h, grid, policy, value, marginal_utility, n_rows, n_in,
+                                          int(search_radius), float(jump_thresh), grid_out, policy_out, value_out,
+                                          n_out, n_kept, stream))
+
+    def envelope_step(self, kind: int, items, prefix, n_items, n_rows, max_n_in, stream) -> None:
+        """Item form of the LTM (kind 1) / RFC (kind 2) envelopes."""
+        self.check(self.lib.lcmx_envelope_step(self.h, kind, items, prefix, n_items, n_rows, max_n_in, stream))
 
 
 class Module:

@@ -30,10 +30,38 @@ class FUESEnvelope:
 
 
 @dataclasses.dataclass(frozen=True, kw_only=True)
+class RFCEnvelope:
+    """Rooftop-Cut upper envelope (``dcegm.py:113-126``): a candidate below a
+    neighbour's tangent line across a policy jump is deleted."""
+
+    jump_thresh: float = 2.0
+    search_radius: int = 10
+
+    def __post_init__(self) -> None:
+        if self.jump_thresh <= 0:
+            raise ValueError("jump_thresh must be positive")
+        if int(self.search_radius) < 1:
+            raise ValueError("search_radius must be >= 1")
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
+class LTMEnvelope:
+    """Local-upper-bound brute-force envelope (``dcegm.py:129-132``)."""
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
+class MSSEnvelope:
+    """HARK-style left-to-right segment envelope (``dcegm.py:135-138``); not
+    implemented on the GPU path."""
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
 class DCEGM:
     """Discrete-continuous EGM with an upper envelope (``dcegm.py:151-255``).
 
-    Only ``FUESEnvelope`` is implemented by this solver.
+    ``FUESEnvelope`` (the default), ``RFCEnvelope`` and ``LTMEnvelope`` are
+    implemented by this solver (RFC and LTM on candidate rows of up to 4096
+    points).
     """
 
     savings_grid: Any
@@ -43,8 +71,10 @@ class DCEGM:
     stochastic_node_batch_size: int = 0
 
     def __post_init__(self) -> None:
-        if not isinstance(self.envelope, FUESEnvelope):
-            raise NotImplementedError("only FUESEnvelope is implemented on the GPU path")
+        if not isinstance(self.envelope, (FUESEnvelope, RFCEnvelope, LTMEnvelope)):
+            raise NotImplementedError(
+                f"{type(self.envelope).__name__} is not implemented on the GPU path "
+                "(FUESEnvelope, RFCEnvelope and LTMEnvelope are)")
         if self.refined_grid_factor < 1.0:
             raise ValueError("refined_grid_factor must be >= 1")
         if self.n_constrained_points < 1:

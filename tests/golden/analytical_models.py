@@ -119,7 +119,7 @@ def _inv_mu_log(marginal_continuation):
     return 1.0 / marginal_continuation
 
 
-def get_dcegm_model(n_periods: int, n_savings: int = 200, n_constrained: int = 64) -> Model:
+def get_dcegm_model(n_periods: int, n_savings: int = 200, n_constrained: int = 64, envelope=None) -> Model:
     from pylcm_b200 import DCEGM, ConsumptionSavingsRegime, FUESEnvelope, IrregSpacedGrid, LiquidMargin
 
     wealth = LinSpacedGrid(start=1, stop=400, n_points=100)
@@ -127,7 +127,8 @@ def get_dcegm_model(n_periods: int, n_savings: int = 200, n_constrained: int = 6
     ages = AgeGrid(start=40, stop=40 + (n_periods - 1) * 10, step="10Y")
     last = ages.exact_values[-1]
     sav = IrregSpacedGrid(points=tuple(400.0 * (i / (n_savings - 1)) ** 3 for i in range(n_savings)))
-    solver = DCEGM(savings_grid=sav, n_constrained_points=n_constrained, envelope=FUESEnvelope())
+    solver = DCEGM(savings_grid=sav, n_constrained_points=n_constrained,
+                   envelope=envelope if envelope is not None else FUESEnvelope())
     margin = LiquidMargin(state="wealth", action="consumption", resources="wealth", post_decision_state="savings")
     work = ConsumptionSavingsRegime(
         actions={"labor_supply": DiscreteGrid(Labor), "consumption": cons},
@@ -159,6 +160,6 @@ def get_dcegm_model(n_periods: int, n_savings: int = 200, n_constrained: int = 6
     return Model(regimes={"working_life": work, "retirement": ret, "dead": dead}, ages=ages, regime_id_class=Rid)
 
 
-def dcegm_model_and_params(case: str):
+def dcegm_model_and_params(case: str, envelope=None):
     kw = CASES[case]
-    return get_dcegm_model(kw["n_periods"]), get_params(**kw)
+    return get_dcegm_model(kw["n_periods"], envelope=envelope), get_params(**kw)

@@ -168,3 +168,40 @@ def test_dcegm_with_an_income_process_matches_oracle(taste):
             np.testing.assert_allclose(res.periods[p]["states"][name], ora[p]["states"][name], rtol=1e-9, atol=1e-9,
                                        equal_nan=True)
         np.testing.assert_allclose(res.periods[p]["value"], ora[p]["value"], rtol=1e-9, atol=1e-9, equal_nan=True)
+
+
+@pytest.mark.parametrize("envelope", ["ltm", "rfc"])
+@pytest.mark.parametrize("case", ["five_periods", "low_delta"])
+def test_dcegm_other_envelopes_match_oracle_and_closed_form(envelope, case):
+    """DCEGM(envelope=LTMEnvelope() / RFCEnvelope()) on the GPU against the
+    oracle with the same envelope (1e-10), and within 1e-3 of the closed form:
+    neither inserts the segment crossing, so a kink is recovered to within the
+    grid spacing."""
+    from pylcm_b200 import LTMEnvelope, RFCEnvelope
+
+    env = LTMEnvelope() if envelope == "ltm" else RFCEnvelope()
+    model, params = AM.dcegm_model_and_params(case, env)
+    V = model.solve(params=params, log_level="off")
+    Vo, _ = oracle_solve(model, params)
+    for p in Vo:
+        for r in Vo[p]:
+            assert rel_err(V[p][r], Vo[p][r]) < 1e-10, (envelope, p, r)
+    periods = sorted(V)
+    for kind, reg in (("worker", "working_life"), ("retired", "retirement")):
+        num = np.stack([V[p][reg] for p in periods[:-1]])
+        ana = np.load(f"tests/golden/analytical_{case}__values_{kind}.npy")
+        assert np.abs(num - ana)[:, 2:].max() < 1e-3
+
+
+@pytest.mark.parametrize("taste", [None, 0.05])
+def test_dcegm_rfc_income_shock_model_matches_oracle(taste):
+    from pylcm_b200 import RFCEnvelope
+
+    model = M.dcegm_model(n_periods=5, n_savings=200, n_wealth=100, taste=taste is not None,
+                          envelope=RFCEnvelope(search_radius=6, jump_thresh=1.5))
+    params = M.dcegm_params(2, taste_scale=taste)
+    V = model.solve(params=params, log_level="off")
+    Vo, _ = oracle_solve(model, params)
+    for p in Vo:
+        for r in Vo[p]:
+            assert rel_err(V[p][r], Vo[p][r]) < 1e-10, (taste, p, r)
