@@ -167,7 +167,17 @@ int lcmx_rfc_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const
                   const double* marginal_utility, int n_rows, int n_in, int search_radius, double jump_thresh,
                   double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept, void* stream);
 
-/* Item form of the LTM (kind 1) and RFC (kind 2) envelopes, one launch over
+/* Kernel (c), part 2, the MSS envelope (MSSEnvelope): HARK's EGM upper
+ * envelope as src/_lcm/egm/upper_envelope/mss.py:72-629 (refine_envelope)
+ * states it -- LTM's evaluation over the monotone links (a grid or value
+ * decrease starts a new branch), plus the exact crossing of the two winning
+ * links, inserted twice (left, right policy), where the winning branch
+ * changes.  Outputs as lcmx_fues_scan's.  Rows of up to 4096 candidates. */
+int lcmx_mss_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value, int n_rows,
+                  int n_in, double* grid_out, double* policy_out, double* value_out, int n_out, int* n_kept,
+                  void* stream);
+
+/* Item form of the LTM (kind 1), RFC (kind 2) and MSS (kind 3) envelopes, one launch over
  * the rows of n_items candidate blocks; item records of 13 64-bit words:
  * grid, policy, value, marginal utility (RFC; 0 for LTM), grid_out,
  * policy_out, value_out, n_kept (int32) device pointers, then n_rows, n_in,

@@ -1,4 +1,4 @@
-"""Oracle: DC-EGM backward induction with the FUES, LTM or RFC envelope (test
+"""Oracle: DC-EGM backward induction with the FUES, LTM, RFC or MSS envelope (test
 infrastructure only).
 
 Restates the reference's endogenous-grid step
@@ -14,7 +14,7 @@ state x discrete action) row:
 2. Euler inversion c = (u')^{-1}(max(beta E[mu'], eps)), R = A + c,
    v = u(c) + beta E[V'] (``egm/euler.py:18-68``);
 3. constrained candidates c_k = span 1e-4 ratio^k (``step_core.py:443-514``);
-4. the upper envelope: FUES (``oracle/fues.py``), or LTM / RFC
+4. the upper envelope: FUES (``oracle/fues.py``), or LTM / RFC / MSS
    (``oracle/envelopes.py``; RFC with the candidates' u'(c) as supgradient,
    0 for dead candidates, ``step_core.py:414-440``);
 5. publication on the state grid: the refined value row read with a
@@ -37,7 +37,7 @@ import math
 
 import numpy as np
 
-from oracle.envelopes import refine_ltm, refine_rfc
+from oracle.envelopes import refine_ltm, refine_mss, refine_rfc
 from oracle.fues import refine
 from oracle.grid_search import _process_tables, bellman_step
 from pylcm_b200 import ir
@@ -315,6 +315,8 @@ def egm_step(er, specs, res, period, age, carry_next, V_next, grid_R, value_mu=N
         cand_s = np.where(dead, np.nan, cand_s)
         if er.envelope == "ltm":
             rg, rc, rv, n_kept = refine_ltm(cand_g, cand_c, cand_v, er.n_pad)
+        elif er.envelope == "mss":
+            rg, rc, rv, n_kept = refine_mss(cand_g, cand_c, cand_v, er.n_pad)
         elif er.envelope == "rfc":
             # candidate supgradient u'(c), 0 for dead candidates (step_core.py:414-440)
             envm = dict(env)

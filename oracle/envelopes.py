@@ -1,5 +1,5 @@
-"""Oracle: the LTM and RFC upper envelopes, one row at a time (test
-infrastructure only).
+"""Oracle: the LTM, RFC and MSS upper envelopes, one row at a time (test
+infrastructure only; MSS is documented at `refine_mss`).
 
 LTM, the local-upper-bound brute method, as the reference implements it in
 ``src/_lcm/egm/upper_envelope/ltm.py``:
@@ -114,6 +114,97 @@ def refine_rfc(grid, policy, value, marginal_utility, n_refined: int, search_rad
             if not deleted:
                 keep.append(l_)
     return _publish([g[i] for i in keep], [p[i] for i in keep], [v[i] for i in keep], n_refined)
+
+
+def _mss_links(g, v, dead):
+    """Per link k (candidates k, k+1 in input order): live flag and branch id
+    (HARK's monotone split: a link across a grid decrease, or a value decrease
+    past 16 eps max(|v_k|, |v_k+1|), starts a new branch and is not live)
+    (``mss.py:153-171, 549-570``)."""
+    gl, gr, vl, vr = g[:-1], g[1:], v[:-1], v[1:]
+    with np.errstate(invalid="ignore"):
+        floor = 16.0 * EPS * np.maximum(np.abs(vl), np.abs(vr))
+        dec = (gr < gl) | (vr < vl - floor)
+    seg = np.cumsum(dec.astype(np.int64))
+    live = ~dead[:-1] & ~dead[1:] & ~dec
+    return live, seg
+
+
+def _mss_eval(q, g, p, v, live, seg):
+    """(envelope value, policy, winning link, winning branch) at abscissa q:
+    the largest finite interpolant over the live links bracketing q; the
+    winner is the first link within 16 eps max(1, |max|) of it; no bracketing
+    link: (-inf, NaN, 0, -1) (``mss.py:478-547``)."""
+    gl, gr, vl, vr, pl, pr = g[:-1], g[1:], v[:-1], v[1:], p[:-1], p[1:]
+    with np.errstate(invalid="ignore", divide="ignore", over="ignore"):
+        br = live & (q >= np.minimum(gl, gr)) & (q <= np.maximum(gl, gr))
+        w = gr - gl
+        rel = np.where(w == 0.0, 0.0, (q - gl) / np.where(w == 0.0, 1.0, w))
+        vi = vl + rel * (vr - vl)
+        pi = pl + rel * (pr - pl)
+        masked = np.where(br & np.isfinite(vi), vi, -np.inf)
+        env = masked.max() if masked.size else -np.inf
+        floor = 16.0 * EPS * max(1.0, abs(env))
+        tie = br & (masked >= env - floor)
+    if not br.any():
+        return env, np.nan, 0, -1
+    k = int(np.argmax(tie))
+    return env, pi[k], k, int(seg[k])
+
+
+def _line_slope(xa, ya, xb, yb):
+    dx = xb - xa
+    return 0.0 if dx == 0.0 else (yb - ya) / dx
+
+
+def refine_mss(grid, policy, value, n_refined: int):
+    """MSS (HARK's EGM upper envelope) as the reference implements it in
+    ``src/_lcm/egm/upper_envelope/mss.py:72-310``: the LTM evaluation at the
+    sorted live abscissae over the live monotone links (finite interpolants
+    only), plus, where the winning branch changes between two consecutive
+    live queries, the crossing of the two winning links' value lines --
+    inserted twice (left, right policy) when it falls strictly between them
+    and the envelope there matches it (finite, within 1e-7 + 1e-5 |value|)."""
+    g = np.asarray(grid, dtype=np.float64)
+    p = np.asarray(policy, dtype=np.float64)
+    v = np.asarray(value, dtype=np.float64)
+    n = g.size
+    dead = np.isnan(g) | np.isnan(v)
+    order = np.argsort(np.where(dead, np.inf, g), kind="stable")
+    if n > 1:
+        live, seg = _mss_links(g, v, dead)
+    else:
+        live, seg = np.zeros(0, dtype=bool), np.zeros(0, dtype=np.int64)
+    atol = max(1e-7, 8.0 * EPS)
+    rows = []
+    prev_link, prev_seg, prev_grid = 0, -1, -np.inf
+    for i in order:
+        q = np.nan if dead[i] else g[i]
+        env, pol, link, sg = _mss_eval(q, g, p, v, live, seg) if not dead[i] else (-np.inf, np.nan, 0, -1)
+        node_live = (not dead[i]) and env != -np.inf
+        if node_live and prev_seg >= 0 and sg != prev_seg:
+            a, b = prev_link, link
+            sa = _line_slope(g[a], v[a], g[a + 1], v[a + 1])
+            sb = _line_slope(g[b], v[b], g[b + 1], v[b + 1])
+            den = sa - sb
+            with np.errstate(invalid="ignore", divide="ignore", over="ignore"):
+                if den == 0.0:
+                    x, y = np.nan, v[a]
+                else:
+                    x = (v[b] - v[a] + sa * g[a] - sb * g[b]) / den
+                    y = v[a] + sa * (x - g[a])
+                psa = _line_slope(g[a], p[a], g[a + 1], p[a + 1])
+                psb = _line_slope(g[b], p[b], g[b + 1], p[b + 1])
+                pa = p[a] + psa * (x - g[a])
+                pb = p[b] + psb * (x - g[b])
+            if x > prev_grid and x < q:
+                ce = _mss_eval(x, g, p, v, live, seg)[0]
+                if np.isfinite(ce) and np.isfinite(y) and abs(ce - y) <= atol + 1e-5 * abs(y):
+                    rows += [(x, pa, y), (x, pb, y)]
+        if node_live:
+            rows.append((q, pol, env))
+            prev_link, prev_seg, prev_grid = link, sg, q
+    return _publish([r[0] for r in rows], [r[1] for r in rows], [r[2] for r in rows], n_refined)
 
 
 def _publish(gs, ps, vs, n_refined):

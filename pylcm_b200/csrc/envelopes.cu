@@ -1,5 +1,6 @@
-// envelopes.cu -- the LTM and RFC upper envelopes of DC-EGM candidate rows
-// (kernel c, part 2, the alternatives to FUES).
+// envelopes.cu -- the LTM, RFC and MSS upper envelopes of DC-EGM candidate
+// rows (kernel c, part 2, the alternatives to FUES; MSS is described at
+// mss_kernel).
 //
 // LTM restates the local-upper-bound brute method the reference implements in
 // src/_lcm/egm/upper_envelope/ltm.py:35-190: the queries are the live candidate
@@ -18,7 +19,7 @@
 // v_l - v_j < mu_j (R_l - R_j) - 16 eps max(|v_l - v_j|, |mu_j (R_l - R_j)|),
 // across a policy jump |dc/dR| > jump_thresh.
 //
-// Both publish the survivors in sorted order, NaN-padded to n_out, with their
+// All publish the survivors in sorted order, NaN-padded to n_out, with their
 // count (n_kept > n_out: overflow, the row holds a truncated prefix).
 //
 // GPU mapping: one CTA per row, the row staged in shared memory and sorted by
@@ -165,6 +166,31 @@ __device__ __forceinline__ int env_block_scan(int x, int* warp_sums, int& tot) {
   return x + before;
 }
 
+// bitonic sort of (key, index) pairs ascending, np2 a power of two; the
+// caller synchronises before (the keys are written) and it synchronises after
+__device__ __forceinline__ void env_sort(unsigned long long* key, int* idx, int np2) {
+  for (int size = 2; size <= np2; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int t = threadIdx.x; t < np2; t += kEnvBlock) {
+        const int u = t ^ stride;
+        if (u > t) {
+          const unsigned long long ka = key[t], kb = key[u];
+          const int ia = idx[t], ib = idx[u];
+          const bool a_gt = ka > kb || (ka == kb && ia > ib);
+          const bool up = (t & size) == 0;
+          if (a_gt == up) {
+            key[t] = kb;
+            key[u] = ka;
+            idx[t] = ib;
+            idx[u] = ia;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
 template <class Rows, int KIND>
 __global__ void __launch_bounds__(kEnvBlock) envelope_kernel(Rows rows) {
   extern __shared__ __align__(16) unsigned char env_smem[];
@@ -201,27 +227,7 @@ __global__ void __launch_bounds__(kEnvBlock) envelope_kernel(Rows rows) {
       }
     }
     __syncthreads();
-    // bitonic sort of (key, index) ascending
-    for (int size = 2; size <= np2; size <<= 1) {
-      for (int stride = size >> 1; stride > 0; stride >>= 1) {
-        for (int t = threadIdx.x; t < np2; t += kEnvBlock) {
-          const int u = t ^ stride;
-          if (u > t) {
-            const unsigned long long ka = key[t], kb = key[u];
-            const int ia = idx[t], ib = idx[u];
-            const bool a_gt = ka > kb || (ka == kb && ia > ib);
-            const bool up = (t & size) == 0;
-            if (a_gt == up) {
-              key[t] = kb;
-              key[u] = ka;
-              idx[t] = ib;
-              idx[u] = ia;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    }
+    env_sort(key, idx, np2);
     if (KIND == kRfc) {
       // rows in sorted order, through the key buffer (no longer needed)
       double* tmp = reinterpret_cast<double*>(key);
@@ -331,6 +337,221 @@ __global__ void __launch_bounds__(kEnvBlock) envelope_kernel(Rows rows) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// MSS (HARK's EGM upper envelope), src/_lcm/egm/upper_envelope/mss.py:72-629:
+// the links join consecutive candidates in input order; a link across a grid
+// decrease, or a value decrease past 16 eps max(|v_k|, |v_k+1|), starts a new
+// branch and is not live (HARK's monotone split).  At each live abscissa
+// (ascending) the envelope is the largest finite interpolant over the live
+// bracketing links; the winner is the first link within 16 eps max(1, |max|)
+// of it.  Where the winning branch changes between two consecutive live
+// queries, the crossing of the two winning links' value lines is inserted
+// twice (left, then right policy) when it falls strictly between them and the
+// envelope there matches it (finite, within 1e-7 + 1e-5 |value|).
+constexpr int kMss = 3;
+
+// extra shared memory of MSS: the winning branch per query (n ints)
+__host__ __device__ constexpr size_t mss_smem_bytes(int n) { return env_smem_bytes(n) + (size_t)4 * n; }
+
+// value at q of the live link k: vi (rounded step by step), and whether it brackets q
+__device__ __forceinline__ bool mss_link_at(const double* g, const double* v, const int* lseg, int k, double q,
+                                            double& vi, double& rel) {
+  if (lseg[k] < 0) return false;
+  const double gl = g[k], gr = g[k + 1];
+  const bool br = (gl <= gr) ? (gl <= q && q <= gr) : (gr <= q && q <= gl);
+  if (!br) return false;
+  const double w = __dsub_rn(gr, gl);
+  rel = (w == 0.0) ? 0.0 : __ddiv_rn(__dsub_rn(q, gl), w);
+  vi = __dadd_rn(v[k], __dmul_rn(rel, __dsub_rn(v[k + 1], v[k])));
+  return true;
+}
+
+// envelope value at q (-inf: no finite bracketing interpolant); `link` the
+// winner (first link within the tie band), -1 when no live link brackets q
+__device__ double mss_eval(const double* g, const double* v, const int* lseg, int n, double q, int& link) {
+  const double inf = __longlong_as_double(0x7ff0000000000000LL);
+  double env = -inf;
+  bool any = false;
+  for (int k = 0; k + 1 < n; ++k) {
+    double vi, rel;
+    if (mss_link_at(g, v, lseg, k, q, vi, rel)) {
+      any = true;
+      if (isfinite(vi) && vi > env) env = vi;
+    }
+  }
+  link = -1;
+  if (!any) return env;
+  const double floor_ = __dmul_rn(16.0 * 2.220446049250313e-16, fmax(1.0, fabs(env)));
+  const double lo = __dsub_rn(env, floor_);
+  for (int k = 0; k + 1 < n; ++k) {
+    double vi, rel;
+    if (mss_link_at(g, v, lseg, k, q, vi, rel)) {
+      const double mv = isfinite(vi) ? vi : -inf;
+      if (mv >= lo) {
+        link = k;
+        break;
+      }
+    }
+  }
+  return env;
+}
+
+__device__ __forceinline__ double mss_slope(double xa, double ya, double xb, double yb) {
+  const double dx = __dsub_rn(xb, xa);
+  return dx == 0.0 ? 0.0 : __ddiv_rn(__dsub_rn(yb, ya), dx);
+}
+
+template <class Rows>
+__global__ void __launch_bounds__(kEnvBlock) mss_kernel(Rows rows) {
+  extern __shared__ __align__(16) unsigned char env_smem[];
+  __shared__ int warp_sums[kEnvBlock / 32];
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  const double inf = __longlong_as_double(0x7ff0000000000000LL);
+  const double eps16 = 16.0 * 2.220446049250313e-16;
+  const int total = rows.count();
+  for (int row = blockIdx.x; row < total; row += gridDim.x) {
+    const EnvRow io = rows.row(row);
+    const int n = io.n_in;
+    const int np2 = env_pow2(n);
+    double* g = reinterpret_cast<double*>(env_smem);
+    double* p = g + n;
+    double* v = p + n;
+    int* lseg = reinterpret_cast<int*>(v + n);  // branch id of each live link, -1: not live
+    int* wl = lseg + n;                         // winning link per sorted query, -1: dropped
+    unsigned long long* key = reinterpret_cast<unsigned long long*>(v + 2 * n);
+    double* ev = reinterpret_cast<double*>(key);  // envelope value per sorted query (after the sort)
+    int* idx = reinterpret_cast<int*>(key + np2);
+    int* ws = idx + np2;                          // winning branch per sorted query
+    __syncthreads();  // the previous row is done with shared memory
+    for (int t = threadIdx.x; t < n; t += kEnvBlock) {
+      g[t] = io.G[t];
+      p[t] = io.P[t];
+      v[t] = io.V[t];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < np2; t += kEnvBlock) {
+      idx[t] = t;
+      key[t] = t >= n ? ~0ULL : ((env_isnan(g[t]) || env_isnan(v[t])) ? env_key(inf) : env_key(g[t]));
+    }
+    __syncthreads();
+    env_sort(key, idx, np2);
+    // links: branch ids (a running count of decreases) and liveness
+    int base = 0;
+    for (int k0 = 0; k0 < n - 1; k0 += kEnvBlock) {
+      const int k = k0 + (int)threadIdx.x;
+      bool dec = false, live = false;
+      if (k < n - 1) {
+        const double vl = v[k], vr = v[k + 1];
+        const double al = fabs(vl), ar = fabs(vr);
+        const double mx = (env_isnan(al) || env_isnan(ar)) ? nan : (al > ar ? al : ar);
+        dec = (g[k + 1] < g[k]) || (vr < __dsub_rn(vl, __dmul_rn(eps16, mx)));
+        const bool dead = env_isnan(g[k]) || env_isnan(vl) || env_isnan(g[k + 1]) || env_isnan(vr);
+        live = !dead && !dec;
+      }
+      int tot = 0;
+      const int incl = env_block_scan(dec ? 1 : 0, warp_sums, tot);
+      if (k < n - 1) lseg[k] = live ? base + incl : -1;
+      base += tot;
+    }
+    __syncthreads();
+    // the envelope at every sorted query
+    for (int t = threadIdx.x; t < n; t += kEnvBlock) {
+      const int i = idx[t];
+      int link = -1;
+      double e = -inf;
+      if (!(env_isnan(g[i]) || env_isnan(v[i]))) e = mss_eval(g, v, lseg, n, g[i], link);
+      const bool node = link >= 0 && !(e == -inf);
+      ev[t] = e;
+      wl[t] = node ? link : -1;
+      ws[t] = node ? lseg[link] : -1;
+    }
+    __syncthreads();
+    // emission: per query the crossing (twice) before it, then its node
+    int out = 0;
+    for (int r0 = 0; r0 < n; r0 += kEnvBlock) {
+      const int t = r0 + (int)threadIdx.x;
+      bool node = false, cross = false;
+      double q = nan, x = nan, y = nan, pa = nan, pb = nan, pol = nan;
+      if (t < n && wl[t] >= 0) {
+        node = true;
+        const int b = wl[t];
+        q = g[idx[t]];
+        {
+          const double w = __dsub_rn(g[b + 1], g[b]);
+          const double rel = (w == 0.0) ? 0.0 : __ddiv_rn(__dsub_rn(q, g[b]), w);
+          pol = __dadd_rn(p[b], __dmul_rn(rel, __dsub_rn(p[b + 1], p[b])));
+        }
+        int pr = t - 1;
+        while (pr >= 0 && wl[pr] < 0) --pr;
+        if (pr >= 0 && ws[pr] != ws[t]) {
+          const int a = wl[pr];
+          const double qp = g[idx[pr]];
+          const double sa = mss_slope(g[a], v[a], g[a + 1], v[a + 1]);
+          const double sb = mss_slope(g[b], v[b], g[b + 1], v[b + 1]);
+          const double den = __dsub_rn(sa, sb);
+          if (den != 0.0) {
+            x = __ddiv_rn(__dsub_rn(__dadd_rn(__dsub_rn(v[b], v[a]), __dmul_rn(sa, g[a])), __dmul_rn(sb, g[b])), den);
+            y = __dadd_rn(v[a], __dmul_rn(sa, __dsub_rn(x, g[a])));
+            const double psa = mss_slope(g[a], p[a], g[a + 1], p[a + 1]);
+            const double psb = mss_slope(g[b], p[b], g[b + 1], p[b + 1]);
+            pa = __dadd_rn(p[a], __dmul_rn(psa, __dsub_rn(x, g[a])));
+            pb = __dadd_rn(p[b], __dmul_rn(psb, __dsub_rn(x, g[b])));
+            if (x > qp && x < q) {
+              int lk;
+              const double ce = mss_eval(g, v, lseg, n, x, lk);
+              cross = isfinite(ce) && isfinite(y) &&
+                      fabs(__dsub_rn(ce, y)) <= __dadd_rn(1e-7, __dmul_rn(1e-5, fabs(y)));
+            }
+          }
+        }
+      }
+      const int nrow = (cross ? 2 : 0) + (node ? 1 : 0);
+      int tot = 0;
+      const int incl = env_block_scan(nrow, warp_sums, tot);
+      int pos = out + incl - nrow;
+      if (cross) {
+        if (pos < io.n_out) { io.GO[pos] = x; io.PO[pos] = pa; io.VO[pos] = y; }
+        ++pos;
+        if (pos < io.n_out) { io.GO[pos] = x; io.PO[pos] = pb; io.VO[pos] = y; }
+        ++pos;
+      }
+      if (node && pos < io.n_out) {
+        io.GO[pos] = q;
+        io.PO[pos] = pol;
+        io.VO[pos] = ev[t];
+      }
+      out += tot;
+    }
+    for (int t = out + (int)threadIdx.x; t < io.n_out; t += kEnvBlock) {
+      io.GO[t] = nan;
+      io.PO[t] = nan;
+      io.VO[t] = nan;
+    }
+    if (threadIdx.x == 0) *io.nk = out;
+  }
+}
+
+template <class Rows>
+int mss_launch(const Rows& rows, int n_tiles, int max_n, cudaStream_t stream, std::string& err) {
+  cudaError_t e = cudaFuncSetAttribute(mss_kernel<Rows>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)mss_smem_bytes(kEnvMaxN));
+  if (e != cudaSuccess) {
+    err = std::string("MSS kernel attribute: ") + cudaGetErrorString(e);
+    return LCMX_ERR_LAUNCH;
+  }
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = n_tiles < sms * 8 ? n_tiles : sms * 8;
+  mss_kernel<Rows><<<grid, kEnvBlock, mss_smem_bytes(max_n), stream>>>(rows);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    err = std::string("MSS launch: ") + cudaGetErrorString(e);
+    return LCMX_ERR_LAUNCH;
+  }
+  return LCMX_OK;
+}
+
 template <class Rows, int KIND>
 int env_attr(std::string& err) {
   const cudaError_t e = cudaFuncSetAttribute(envelope_kernel<Rows, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -400,9 +621,25 @@ extern "C" int lcmx_rfc_scan(lcmx_ctx* ctx, const double* grid, const double* po
   return rc ? lcmx_set_error_from(ctx, rc, err) : LCMX_OK;
 }
 
+extern "C" int lcmx_mss_scan(lcmx_ctx* ctx, const double* grid, const double* policy, const double* value,
+                             int n_rows, int n_in, double* grid_out, double* policy_out, double* value_out,
+                             int n_out, int* n_kept, void* stream) {
+  if (!ctx || !grid || !policy || !value || !grid_out || !policy_out || !value_out || !n_kept || n_rows < 0 ||
+      n_in < 1 || n_out < 1)
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_mss_scan: bad arguments");
+  if (n_in > kEnvMaxN)
+    return lcmx_set_error_from(ctx, LCMX_ERR_ARGS,
+                               "lcmx_mss_scan: rows longer than " + std::to_string(kEnvMaxN) + " candidates");
+  if (n_rows == 0) return LCMX_OK;
+  EnvContig rows{grid, policy, value, nullptr, grid_out, policy_out, value_out, n_kept, n_rows, n_in, n_out, 0.0, 0};
+  std::string err;
+  const int rc = mss_launch<EnvContig>(rows, n_rows, n_in, (cudaStream_t)stream, err);
+  return rc ? lcmx_set_error_from(ctx, rc, err) : LCMX_OK;
+}
+
 extern "C" int lcmx_envelope_step(lcmx_ctx* ctx, int kind, const void* items, const int* tile_prefix, int n_items,
                                   int n_rows, int max_n_in, void* stream) {
-  if (!ctx || (kind != kLtm && kind != kRfc) || n_items < 0 || n_rows < 0 ||
+  if (!ctx || (kind != kLtm && kind != kRfc && kind != kMss) || n_items < 0 || n_rows < 0 ||
       (n_items > 0 && (!items || !tile_prefix)))
     return lcmx_set_error_from(ctx, LCMX_ERR_ARGS, "lcmx_envelope_step: bad arguments");
   if (max_n_in < 1 || max_n_in > kEnvMaxN)
@@ -411,7 +648,8 @@ extern "C" int lcmx_envelope_step(lcmx_ctx* ctx, int kind, const void* items, co
   if (n_items == 0 || n_rows == 0) return LCMX_OK;
   EnvItems rows{static_cast<const int64_t*>(items), tile_prefix, n_items, n_rows};
   std::string err;
-  const int rc = kind == kLtm ? env_launch<EnvItems, kLtm>(rows, n_rows, max_n_in, (cudaStream_t)stream, err)
-                              : env_launch<EnvItems, kRfc>(rows, n_rows, max_n_in, (cudaStream_t)stream, err);
+  const int rc = kind == kLtm   ? env_launch<EnvItems, kLtm>(rows, n_rows, max_n_in, (cudaStream_t)stream, err)
+                 : kind == kRfc ? env_launch<EnvItems, kRfc>(rows, n_rows, max_n_in, (cudaStream_t)stream, err)
+                                : mss_launch<EnvItems>(rows, n_rows, max_n_in, (cudaStream_t)stream, err);
   return rc ? lcmx_set_error_from(ctx, rc, err) : LCMX_OK;
 }

@@ -115,7 +115,7 @@ class EgmRegime:
     taste_scale: float | None
     feasible: ir.Expr
     tracer: Any
-    envelope: str = "fues"  # the upper envelope: "fues" | "ltm" | "rfc"
+    envelope: str = "fues"  # the upper envelope: "fues" | "ltm" | "rfc" | "mss"
     search_radius: int = 10  # RFC: neighbours inspected on each side
 
     @property
@@ -258,7 +258,8 @@ def trace_egm_regime(spec: RegimeSpec, specs: list, resolver: ParamResolver, tar
         n_pad=n_pad,
         jump_thresh=float(getattr(solver.envelope, "jump_thresh", 2.0)),
         scan_window=int(getattr(solver.envelope, "n_points_to_scan", None) or 0),
-        envelope={"FUESEnvelope": "fues", "LTMEnvelope": "ltm", "RFCEnvelope": "rfc"}[type(solver.envelope).__name__],
+        envelope={"FUESEnvelope": "fues", "LTMEnvelope": "ltm", "RFCEnvelope": "rfc",
+                  "MSSEnvelope": "mss"}[type(solver.envelope).__name__],
         search_radius=int(getattr(solver.envelope, "search_radius", 10)),
         taste_scale=taste,
         feasible=feasible,

@@ -128,7 +128,7 @@ class _Records:
 SM_COUNT = 148
 RESIDENT_THREADS_PER_SM = 1024
 FUES_SMEM_MAX_N = 4096  # longest candidate row of the item-form FUES launch
-ENVELOPE_MAX_N = 4096  # longest candidate row of the LTM / RFC envelope kernels
+ENVELOPE_MAX_N = 4096  # longest candidate row of the LTM / RFC / MSS envelope kernels
 
 
 def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> LaunchConfig:
@@ -919,7 +919,7 @@ class SolvePlan:
                 raise NotImplementedError(
                     f"{name}: the {er.envelope.upper()} envelope handles candidate rows of up to "
                     f"{ENVELOPE_MAX_N} points ({ncand} here)")
-            rec.add("env", None, f"lcmx_envelope_step:{1 if er.envelope == 'ltm' else 2}", g["fues"][k],
+            rec.add("env", None, f"lcmx_envelope_step:{ {'ltm': 1, 'rfc': 2, 'mss': 3}[er.envelope]}", g["fues"][k],
                     g["tiles_f"], 0, ncand, period)
         elif ncand <= FUES_SMEM_MAX_N:
             rec.add("fues", None, "lcmx_fues_step", g["fues"][k], g["tiles_f"], 0, ncand, period)

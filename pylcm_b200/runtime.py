@@ -35,6 +35,7 @@ EXPORTED = (
     "lcmx_module_status",
     "lcmx_ltm_scan",
     "lcmx_rfc_scan",
+    "lcmx_mss_scan",
     "lcmx_envelope_step",
 )
 
@@ -95,6 +96,7 @@ def load_library() -> ctypes.CDLL:
             "lcmx_module_status": ([vp, cp, ctypes.POINTER(ip), ip], ip),
             "lcmx_ltm_scan": ([vp, vp, vp, vp, ip, ip, vp, vp, vp, ip, vp, vp], ip),
             "lcmx_rfc_scan": ([vp, vp, vp, vp, vp, ip, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
+            "lcmx_mss_scan": ([vp, vp, vp, vp, ip, ip, vp, vp, vp, ip, vp, vp], ip),
             "lcmx_envelope_step": ([vp, ip, vp, vp, ip, ip, ip, vp], ip),
         }
         for name, (args, res) in sig.items():
@@ -180,8 +182,14 @@ class Context:
                                           int(search_radius), float(jump_thresh), grid_out, policy_out, value_out,
                                           n_out, n_kept, stream))
 
+    def mss_scan(self, grid, policy, value, n_rows, n_in, grid_out, policy_out, value_out, n_out, n_kept,
+                 stream) -> None:
+        """MSS envelope of contiguous candidate rows (device pointers)."""
+        self.check(self.lib.lcmx_mss_scan(self.h, grid, policy, value, n_rows, n_in, grid_out, policy_out,
+                                          value_out, n_out, n_kept, stream))
+
     def envelope_step(self, kind: int, items, prefix, n_items, n_rows, max_n_in, stream) -> None:
-        """Item form of the LTM (kind 1) / RFC (kind 2) envelopes."""
+        """Item form of the LTM (kind 1) / RFC (kind 2) / MSS (kind 3) envelopes."""
         self.check(self.lib.lcmx_envelope_step(self.h, kind, items, prefix, n_items, n_rows, max_n_in, stream))
 
 

@@ -51,17 +51,17 @@ class LTMEnvelope:
 
 @dataclasses.dataclass(frozen=True, kw_only=True)
 class MSSEnvelope:
-    """HARK-style left-to-right segment envelope (``dcegm.py:135-138``); not
-    implemented on the GPU path."""
+    """HARK-style left-to-right segment envelope with crossing insertion
+    (``dcegm.py:135-138``)."""
 
 
 @dataclasses.dataclass(frozen=True, kw_only=True)
 class DCEGM:
     """Discrete-continuous EGM with an upper envelope (``dcegm.py:151-255``).
 
-    ``FUESEnvelope`` (the default), ``RFCEnvelope`` and ``LTMEnvelope`` are
-    implemented by this solver (RFC and LTM on candidate rows of up to 4096
-    points).
+    ``FUESEnvelope`` (the default), ``RFCEnvelope``, ``LTMEnvelope`` and
+    ``MSSEnvelope`` are implemented by this solver (RFC, LTM and MSS on
+    candidate rows of up to 4096 points).
     """
 
     savings_grid: Any
@@ -71,10 +71,10 @@ class DCEGM:
     stochastic_node_batch_size: int = 0
 
     def __post_init__(self) -> None:
-        if not isinstance(self.envelope, (FUESEnvelope, RFCEnvelope, LTMEnvelope)):
+        if not isinstance(self.envelope, (FUESEnvelope, RFCEnvelope, LTMEnvelope, MSSEnvelope)):
             raise NotImplementedError(
                 f"{type(self.envelope).__name__} is not implemented on the GPU path "
-                "(FUESEnvelope, RFCEnvelope and LTMEnvelope are)")
+                "(FUESEnvelope, RFCEnvelope, LTMEnvelope and MSSEnvelope are)")
         if self.refined_grid_factor < 1.0:
             raise ValueError("refined_grid_factor must be >= 1")
         if self.n_constrained_points < 1:

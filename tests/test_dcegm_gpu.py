@@ -170,16 +170,16 @@ def test_dcegm_with_an_income_process_matches_oracle(taste):
         np.testing.assert_allclose(res.periods[p]["value"], ora[p]["value"], rtol=1e-9, atol=1e-9, equal_nan=True)
 
 
-@pytest.mark.parametrize("envelope", ["ltm", "rfc"])
+@pytest.mark.parametrize("envelope", ["ltm", "rfc", "mss"])
 @pytest.mark.parametrize("case", ["five_periods", "low_delta"])
 def test_dcegm_other_envelopes_match_oracle_and_closed_form(envelope, case):
-    """DCEGM(envelope=LTMEnvelope() / RFCEnvelope()) on the GPU against the
-    oracle with the same envelope (1e-10), and within 1e-3 of the closed form:
-    neither inserts the segment crossing, so a kink is recovered to within the
-    grid spacing."""
-    from pylcm_b200 import LTMEnvelope, RFCEnvelope
+    """DCEGM(envelope=LTMEnvelope() / RFCEnvelope() / MSSEnvelope()) on the
+    GPU against the oracle with the same envelope (1e-10), and within 1e-3 of
+    the closed form (LTM and RFC insert no segment crossing, so a kink is
+    recovered to within the grid spacing)."""
+    from pylcm_b200 import LTMEnvelope, MSSEnvelope, RFCEnvelope
 
-    env = LTMEnvelope() if envelope == "ltm" else RFCEnvelope()
+    env = {"ltm": LTMEnvelope(), "rfc": RFCEnvelope(), "mss": MSSEnvelope()}[envelope]
     model, params = AM.dcegm_model_and_params(case, env)
     V = model.solve(params=params, log_level="off")
     Vo, _ = oracle_solve(model, params)

@@ -1,5 +1,5 @@
-"""The LTM and RFC envelope kernels (liblcmx.so, through the C ABI) against
-the oracle restatements, row by row: bit-identical rows and counts (both
+"""The LTM, RFC and MSS envelope kernels (liblcmx.so, through the C ABI) against
+the oracle restatements, row by row: bit-identical rows and counts (the
 kernels round every step as the oracle does), on the reference's known-answer
 cases and on EGM-like candidate rows -- two runs (the constrained and the
 Euler branch) that fold back over each other, some dead (NaN) candidates,
@@ -8,7 +8,7 @@ lengths 2 .. 4096 -- in the contiguous and the item form."""
 import numpy as np
 import pytest
 
-from oracle.envelopes import refine_ltm, refine_rfc
+from oracle.envelopes import refine_ltm, refine_mss, refine_rfc
 from tests.test_envelopes_oracle import _crossing
 
 pytestmark = pytest.mark.gpu
@@ -44,9 +44,10 @@ def _gpu(kind, G, P, V, M, n_out, radius=10, thr=2.0):
     g, p, v = _dev(G), _dev(P), _dev(V)
     go, po, vo, nk = _outs(n_rows, n_out)
     stream = torch.cuda.current_stream().cuda_stream
-    if kind == "ltm":
-        ctx.ltm_scan(g.data_ptr(), p.data_ptr(), v.data_ptr(), n_rows, n_in, go.data_ptr(), po.data_ptr(),
-                     vo.data_ptr(), n_out, nk.data_ptr(), stream)
+    if kind in ("ltm", "mss"):
+        fn = ctx.ltm_scan if kind == "ltm" else ctx.mss_scan
+        fn(g.data_ptr(), p.data_ptr(), v.data_ptr(), n_rows, n_in, go.data_ptr(), po.data_ptr(),
+           vo.data_ptr(), n_out, nk.data_ptr(), stream)
     else:
         m = _dev(M)
         ctx.rfc_scan(g.data_ptr(), p.data_ptr(), v.data_ptr(), m.data_ptr(), n_rows, n_in, radius, thr,
@@ -57,6 +58,8 @@ def _gpu(kind, G, P, V, M, n_out, radius=10, thr=2.0):
 def _oracle(kind, g, p, v, m, n_out, radius=10, thr=2.0):
     if kind == "ltm":
         return refine_ltm(g, p, v, n_out)
+    if kind == "mss":
+        return refine_mss(g, p, v, n_out)
     return refine_rfc(g, p, v, m, n_out, search_radius=radius, jump_thresh=thr)
 
 
@@ -93,7 +96,7 @@ def _same(got, want):
     assert got[3] == want[3]
 
 
-@pytest.mark.parametrize("kind", ["ltm", "rfc"])
+@pytest.mark.parametrize("kind", ["ltm", "rfc", "mss"])
 def test_known_answer_cases(kind):
     g, p, v, mu = _crossing()
     thr = 0.6 if kind == "rfc" else 2.0
@@ -106,11 +109,11 @@ def test_known_answer_cases(kind):
     _same([x[0] for x in got], _oracle(kind, lg[0], lg[0] * 0.5, [1.0, 2.0, 5.0, 7.0], [0.5] * 4, 8))
 
 
-@pytest.mark.parametrize("kind", ["ltm", "rfc"])
+@pytest.mark.parametrize("kind", ["ltm", "rfc", "mss"])
 @pytest.mark.parametrize("n", [2, 37, 300, 2020, 4096])
 def test_rows_match_the_oracle(kind, n):
     G, P, V, M = _rows(5 if n < 4096 else 2, n, seed=n)
-    n_out = n + 3
+    n_out = 2 * n + 3
     got = _gpu(kind, G, P, V, M, n_out)
     for r in range(G.shape[0]):
         _same([x[r] for x in got], _oracle(kind, G[r], P[r], V[r], M[r], n_out))
@@ -124,7 +127,7 @@ def test_rfc_radius_and_threshold():
             _same([x[r] for x in got], _oracle("rfc", G[r], P[r], V[r], M[r], 600, radius=radius, thr=thr))
 
 
-@pytest.mark.parametrize("kind", ["ltm", "rfc"])
+@pytest.mark.parametrize("kind", ["ltm", "rfc", "mss"])
 def test_item_form_equals_the_contiguous_form(kind):
     """Two candidate blocks of different row lengths in one launch."""
     import torch
@@ -136,7 +139,7 @@ def test_item_form_equals_the_contiguous_form(kind):
     keep, recs, prefix = [], [], [0]
     for G, P, V, M in blocks:
         n_rows, n_in = G.shape
-        n_out = n_in + 5
+        n_out = 2 * n_in + 5
         ins = [_dev(x) for x in (G, P, V, M)]
         outs = _outs(n_rows, n_out)
         keep.append((ins, outs, n_out))
@@ -148,8 +151,8 @@ def test_item_form_equals_the_contiguous_form(kind):
         prefix.append(prefix[-1] + n_rows)
     items = torch.as_tensor(np.array(recs, dtype=np.int64), device="cuda")
     pre = torch.as_tensor(np.array(prefix, dtype=np.int32), device="cuda")
-    ctx.envelope_step(1 if kind == "ltm" else 2, items.data_ptr(), pre.data_ptr(), len(blocks), prefix[-1], 700,
-                      torch.cuda.current_stream().cuda_stream)
+    ctx.envelope_step({"ltm": 1, "rfc": 2, "mss": 3}[kind], items.data_ptr(), pre.data_ptr(), len(blocks),
+                      prefix[-1], 700, torch.cuda.current_stream().cuda_stream)
     torch.cuda.synchronize()
     for (G, P, V, M), (_, outs, n_out) in zip(blocks, keep):
         got = _host(*outs)

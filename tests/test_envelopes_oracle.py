@@ -1,11 +1,12 @@
-"""The LTM and RFC upper-envelope oracles against the reference's own
-known-answer cases (``tests/solution/test_ltm.py`` and
-``tests/solution/test_rfc.py``: crossing linear segments, concave
-pass-through, a loop-back segment, value dips, dead candidates, overflow)."""
+"""The LTM, RFC and MSS upper-envelope oracles against the reference's own
+known-answer cases (``tests/solution/test_ltm.py``, ``tests/solution/test_rfc.py``
+and ``tests/solution/test_backend_oracle_parity.py``: crossing linear segments,
+concave pass-through, a loop-back segment, a strictly dominated branch, value
+dips, dead candidates, overflow)."""
 
 import numpy as np
 
-from oracle.envelopes import refine_ltm, refine_rfc
+from oracle.envelopes import refine_ltm, refine_mss, refine_rfc
 
 
 def _kept(a):
@@ -119,8 +120,9 @@ def test_envelope_configurations():
     sav = IrregSpacedGrid(points=(0.0, 1.0, 2.0))
     assert DCEGM(savings_grid=sav, envelope=LTMEnvelope()).envelope == LTMEnvelope()
     assert DCEGM(savings_grid=sav, envelope=RFCEnvelope(search_radius=3)).envelope.search_radius == 3
-    with pytest.raises(NotImplementedError, match="MSSEnvelope"):
-        DCEGM(savings_grid=sav, envelope=MSSEnvelope())
+    assert DCEGM(savings_grid=sav, envelope=MSSEnvelope()).envelope == MSSEnvelope()
+    with pytest.raises(NotImplementedError, match="str is not implemented"):
+        DCEGM(savings_grid=sav, envelope="fues")
     with pytest.raises(ValueError):
         RFCEnvelope(jump_thresh=0.0)
     with pytest.raises(ValueError):
@@ -128,14 +130,14 @@ def test_envelope_configurations():
 
 
 def test_oracle_dcegm_with_each_envelope_tracks_the_closed_form():
-    """The oracle's DC-EGM solve with LTM and RFC stays within 1e-3 of the
-    Iskhakov et al. (2017) closed form (no crossing insertion: kinks within
-    the grid spacing)."""
+    """The oracle's DC-EGM solve with LTM, RFC and MSS stays within 1e-3 of
+    the Iskhakov et al. (2017) closed form (LTM and RFC insert no crossing:
+    kinks within the grid spacing)."""
     from oracle.dcegm import solve
-    from pylcm_b200 import LTMEnvelope, RFCEnvelope
+    from pylcm_b200 import LTMEnvelope, MSSEnvelope, RFCEnvelope
     from tests.golden import analytical_models as AM
 
-    for env in (LTMEnvelope(), RFCEnvelope()):
+    for env in (LTMEnvelope(), RFCEnvelope(), MSSEnvelope()):
         model, params = AM.dcegm_model_and_params("five_periods", env)
         V, _ = solve(model, params)
         periods = sorted(V)
@@ -143,3 +145,48 @@ def test_oracle_dcegm_with_each_envelope_tracks_the_closed_form():
             num = np.stack([V[p][reg] for p in periods[:-1]])
             ana = np.load(f"tests/golden/analytical_five_periods__values_{kind}.npy")
             assert np.abs(num - ana)[:, 2:].max() < 1e-3, (type(env).__name__, kind)
+
+
+# ---------------------------------------------------------------- MSS
+def test_mss_inserts_the_crossing_twice():
+    g, p, v, _ = _crossing()
+    rg, rp, rv, n = refine_mss(g, p, v, 16)
+    kg, kp, kv = _kept(rg), _kept(rp), _kept(rv)
+    assert n == 10
+    at = np.flatnonzero(np.isclose(kg, 2.25, atol=1e-12))
+    assert at.size == 2
+    np.testing.assert_allclose(kv[at], 1.9, atol=1e-12)
+    np.testing.assert_allclose(kp[at], [0.30 * 2.25, 0.55 * 2.25], atol=1e-12)  # left, then right policy
+    nodes = np.delete(kg, at)
+    np.testing.assert_allclose(np.delete(kv, at), np.maximum(1.0 + 0.4 * nodes, 0.1 + 0.8 * nodes), atol=1e-12)
+    _check_tail(rg)
+    assert refine_mss(g, p, v, 5)[3] == 10  # overflow: the count says so
+
+
+def test_every_envelope_deletes_a_strictly_dominated_branch():
+    """Branch 0: V = R, c = 0.3 R; branch 1: V = R - 1, c = 10, below it
+    everywhere; the envelope is branch 0."""
+    x = [0.0, 1.0, 2.0, 3.0]
+    g = np.array(x + x)
+    v = np.array(x + [t - 1.0 for t in x])
+    p = np.array([0.3 * t for t in x] + [10.0] * 4)
+    q = np.linspace(0.0, 3.0, 13)
+    for name, (rg, rp, rv, _) in {
+        "ltm": refine_ltm(g, p, v, 32), "mss": refine_mss(g, p, v, 32),
+        "rfc": refine_rfc(g, p, v, np.ones_like(g), 32, search_radius=32),
+    }.items():
+        keep = ~np.isnan(rg)
+        np.testing.assert_allclose(np.interp(q, rg[keep], rv[keep]), q, atol=1e-9, err_msg=name)
+        np.testing.assert_allclose(np.interp(q, rg[keep], rp[keep]), 0.3 * q, atol=1e-9, err_msg=name)
+
+
+def test_every_envelope_is_the_identity_on_one_concave_branch():
+    g = np.array([0.0, 1.0, 2.0, 3.0, 4.0])
+    v = np.array([0.0, 1.0, 1.7, 2.2, 2.5])
+    p = np.array([0.0, 0.6, 1.0, 1.3, 1.5])
+    mu = np.array([1.0, 0.85, 0.6, 0.45, 0.3])
+    q = np.linspace(0.0, 4.0, 17)
+    for rg, _, rv, n in (refine_ltm(g, p, v, 16), refine_mss(g, p, v, 16), refine_rfc(g, p, v, mu, 16)):
+        keep = ~np.isnan(rg)
+        assert n == 5
+        np.testing.assert_allclose(np.interp(q, rg[keep], rv[keep]), np.interp(q, g, v), atol=1e-12)
