@@ -65,7 +65,8 @@ def _oracle(kind, g, p, v, m, n_out, radius=10, thr=2.0):
 
 def _rows(n_rows, n, seed):
     """EGM-like rows: a constrained run (c = R, value log c) then an Euler run
-    whose endogenous grid folds back (a discrete-choice kink), dead entries."""
+    whose endogenous grid folds back (a discrete-choice kink) onto a branch
+    that crosses the first, dead entries."""
     rng = np.random.default_rng(seed)
     G, P, V, M = [], [], [], []
     for _ in range(n_rows):
@@ -76,7 +77,9 @@ def _rows(n_rows, n, seed):
         fold = ne // 2
         c = np.where(np.arange(ne) < fold, 0.6 + 0.35 * a, 0.2 + 0.55 * a)
         re_ = a + c - np.where(np.arange(ne) < fold, 0.0, rng.uniform(1.0, 3.0))
-        ve = np.log(c) + 0.3 * np.sqrt(a + 1.0) + np.where(np.arange(ne) < fold, 0.0, 0.25)
+        # the folded branch starts below the first and ends above it: the
+        # winning branch switches inside the overlap (a crossing)
+        ve = np.log(c) + 0.3 * np.sqrt(a + 1.0) + np.where(np.arange(ne) < fold, 0.0, 0.08 * a - 0.4)
         g = np.concatenate([rc, re_])
         pol = np.concatenate([rc, c])
         val = np.concatenate([np.log(rc) - 0.1, ve])
@@ -87,6 +90,26 @@ def _rows(n_rows, n, seed):
         pol = np.where(dead, np.nan, pol)
         mu = np.where(dead, 0.0, mu)
         G.append(g); P.append(pol); V.append(val); M.append(mu)
+    return np.array(G), np.array(P), np.array(V), np.array(M)
+
+
+def _crossing_rows(n_rows, n, seed):
+    """Two overlapping branches on [0, 10], one run each, whose values cross
+    (at a random point) between grid points: the MSS crossing insertion."""
+    rng = np.random.default_rng(seed)
+    G, P, V, M = [], [], [], []
+    for _ in range(n_rows):
+        na = n // 2
+        xa = np.sort(rng.uniform(0.0, 10.0, na))
+        xb = np.sort(rng.uniform(0.0, 10.0, n - na))
+        s = rng.uniform(0.05, 0.25)
+        va = np.log1p(xa) + 0.1 * xa
+        vb = np.log1p(xb) + (0.1 + s) * xb - s * rng.uniform(2.0, 8.0)
+        g = np.concatenate([xa, xb])
+        G.append(g)
+        P.append(np.concatenate([0.3 * xa, 0.5 * xb + 0.2]))
+        V.append(np.concatenate([va, vb]))
+        M.append(np.concatenate([1.0 / (1.0 + xa) + 0.1, 1.0 / (1.0 + xb) + 0.1 + s]))
     return np.array(G), np.array(P), np.array(V), np.array(M)
 
 
@@ -117,6 +140,17 @@ def test_rows_match_the_oracle(kind, n):
     got = _gpu(kind, G, P, V, M, n_out)
     for r in range(G.shape[0]):
         _same([x[r] for x in got], _oracle(kind, G[r], P[r], V[r], M[r], n_out))
+
+
+@pytest.mark.parametrize("kind", ["ltm", "rfc", "mss"])
+def test_crossing_branches_match_the_oracle(kind):
+    G, P, V, M = _crossing_rows(6, 900, seed=5)
+    got = _gpu(kind, G, P, V, M, 1900)
+    for r in range(G.shape[0]):
+        want = _oracle(kind, G[r], P[r], V[r], M[r], 1900)
+        _same([x[r] for x in got], want)
+        if kind == "mss":
+            assert want[3] > _oracle("ltm", G[r], P[r], V[r], M[r], 1900)[3]  # crossings were inserted
 
 
 def test_rfc_radius_and_threshold():
