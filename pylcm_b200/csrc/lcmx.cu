@@ -40,6 +40,7 @@ struct DriverApi {
   CUresult (*LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned,
                            CUstream, void**, void**) = nullptr;
   CUresult (*ModuleGetGlobal)(CUdeviceptr*, size_t*, CUmodule, const char*) = nullptr;
+  CUresult (*FuncGetAttribute)(int*, CUfunction_attribute, CUfunction) = nullptr;
   bool ok = false;
 };
 static DriverApi g_drv;
@@ -62,7 +63,8 @@ static bool drv_init() {
             drv_get("cuModuleUnload", g_drv.ModuleUnload) && drv_get("cuModuleGetFunction", g_drv.ModuleGetFunction) &&
             drv_get("cuFuncSetAttribute", g_drv.FuncSetAttribute) &&
             drv_get("cuOccupancyMaxActiveBlocksPerMultiprocessor", g_drv.OccupancyMaxActiveBlocksPerMultiprocessor) &&
-            drv_get("cuLaunchKernel", g_drv.LaunchKernel) && drv_get("cuModuleGetGlobal", g_drv.ModuleGetGlobal);
+            drv_get("cuLaunchKernel", g_drv.LaunchKernel) && drv_get("cuModuleGetGlobal", g_drv.ModuleGetGlobal) &&
+            drv_get("cuFuncGetAttribute", g_drv.FuncGetAttribute);
   g_drv.ok = ok;
   return ok;
 }
@@ -301,12 +303,21 @@ static int get_func(lcmx_module* mod, const char* name, CUfunction* f) {
   return LCMX_OK;
 }
 
+// A launch whose static plus dynamic shared memory exceeds the 48 KB default
+// needs the dynamic part opted in first (the static part counts against it).
+static CUresult opt_in_smem(CUfunction f, int dyn_bytes) {
+  int stat = 0;
+  if (g_drv.FuncGetAttribute(&stat, CU_FUNC_ATTRIBUTE_SHARED_SIZE_BYTES, f) != CUDA_SUCCESS) stat = 0;
+  if ((long long)dyn_bytes + stat <= 48 * 1024) return CUDA_SUCCESS;
+  return g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn_bytes);
+}
+
 extern "C" int lcmx_occupancy(lcmx_module* mod, const char* kernel, int block, int smem_bytes, int* blocks_per_sm) {
   if (!mod || !kernel || !blocks_per_sm || block <= 0) return set_err(mod ? mod->ctx : nullptr, LCMX_ERR_ARGS, "lcmx_occupancy: bad args");
   CUfunction f;
   int rc = get_func(mod, kernel, &f);
   if (rc) return rc;
-  if (smem_bytes > 48 * 1024) g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, smem_bytes);
+  opt_in_smem(f, smem_bytes);
   int n = 0;
   CUresult r = g_drv.OccupancyMaxActiveBlocksPerMultiprocessor(&n, f, block, (size_t)smem_bytes);
   if (r != CUDA_SUCCESS) return set_err(mod->ctx, LCMX_ERR_CUDA, "occupancy: " + cu_msg(r));
@@ -323,8 +334,8 @@ static int launch_items(lcmx_module* mod, const char* kernel, const lcmx_launch_
   CUfunction f;
   int rc = get_func(mod, kernel, &f);
   if (rc) return rc;
-  if (a->smem_bytes > 48 * 1024) {
-    CUresult r = g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, a->smem_bytes);
+  {
+    CUresult r = opt_in_smem(f, a->smem_bytes);
     if (r != CUDA_SUCCESS) return set_err(mod->ctx, LCMX_ERR_LAUNCH, "smem attribute: " + cu_msg(r));
   }
   int grid = a->grid;
