@@ -50,7 +50,15 @@ from pylcm_b200.regime import (
     MarkovTransition,
     Regime,
 )
-from pylcm_b200.solvers import DCEGM, FUESEnvelope, GridSearch, LTMEnvelope, MSSEnvelope, RFCEnvelope
+from pylcm_b200.solvers import (
+    DCEGM,
+    ExactEnvelope,
+    FUESEnvelope,
+    GridSearch,
+    LTMEnvelope,
+    MSSEnvelope,
+    RFCEnvelope,
+)
 
 __all__ = [
     "DCEGM",
@@ -59,6 +67,7 @@ __all__ = [
     "ConsumptionSavingsRegime",
     "DiscreteGrid",
     "ExtremeValueTasteShocks",
+    "ExactEnvelope",
     "FUESEnvelope",
     "LTMEnvelope",
     "MSSEnvelope",

@@ -12,6 +12,21 @@ class GridSearch:
 
 
 @dataclasses.dataclass(frozen=True, kw_only=True)
+class ExactEnvelope:
+    """Certified segment-envelope configuration (``dcegm.py:71-88``); not
+    implemented on the GPU path (``DCEGM`` refuses it)."""
+
+    max_runs: int = 24
+    cell_batch_size: int | None = None
+
+    def __post_init__(self) -> None:
+        if int(self.max_runs) < 2:
+            raise ValueError("max_runs must be >= 2")
+        if self.cell_batch_size is not None and int(self.cell_batch_size) < 1:
+            raise ValueError("cell_batch_size must be a positive integer or None")
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
 class FUESEnvelope:
     """Fast Upper-Envelope Scan (``dcegm.py:93-110``)."""
 

@@ -123,6 +123,12 @@ def test_envelope_configurations():
     assert DCEGM(savings_grid=sav, envelope=MSSEnvelope()).envelope == MSSEnvelope()
     with pytest.raises(NotImplementedError, match="str is not implemented"):
         DCEGM(savings_grid=sav, envelope="fues")
+    from pylcm_b200 import ExactEnvelope
+
+    with pytest.raises(NotImplementedError, match="ExactEnvelope is not implemented"):
+        DCEGM(savings_grid=sav, envelope=ExactEnvelope())
+    with pytest.raises(ValueError):
+        ExactEnvelope(max_runs=1)
     with pytest.raises(ValueError):
         RFCEnvelope(jump_thresh=0.0)
     with pytest.raises(ValueError):
