@@ -1132,7 +1132,9 @@ class RegimeKernels:
                 out.append("}")
             if not det:
                 out.append(f"bool valid = (fabs(mass - ({T})1) <= ({T})1e-3) && !neg;")
-                out.append(f"ce = (mass == ({T})1) ? ce : (valid ? ce / mass : lcm_lim<{T}>::nan());")
+                # a negative weight poisons the row even when the weights sum
+                # to exactly one (Q_and_F.py:1401-1432, 646-653)
+                out.append(f"ce = valid ? ((mass == ({T})1) ? ce : ce / mass) : lcm_lim<{T}>::nan();")
             out.append(f"Q = ({T})({uexpr}) + ({T})({bexpr}) * ce;")
             return out
 
