@@ -215,7 +215,10 @@ class EgmKernels:
         ap("    const int row = e / n_sav, j = e % n_sav;")
         # one candidate row for the whole warp: its carry-row reads share
         # their bracket search (lcm_row_bracket_warp)
-        ap("    const bool warp_row = __all_sync(0xffffffffu, live && row == __shfl_sync(0xffffffffu, row, 0));")
+        # (the shuffle runs on every lane: a shuffle inside the short-circuit
+        # of `live && ...` would leave the warp's non-live lanes out of it)
+        ap("    const int row_l0 = __shfl_sync(0xffffffffu, row, 0);")
+        ap("    const bool warp_row = __all_sync(0xffffffffu, live && row == row_l0);")
         body: list[str] = []
         prov = dict(base_prov)
         prov.update(self._row_decode(body, "row"))

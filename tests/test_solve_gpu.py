@@ -34,6 +34,8 @@ def _action_values(spec, flat):
     """Action values of flat action indices (row-major over the declared
     actions): one column per action."""
     flat = np.asarray(flat, dtype=np.int64)
+    if not spec.actions:
+        return np.zeros(flat.shape + (1,))
     cols = []
     for ax in reversed(spec.actions):
         i = flat % ax.size
