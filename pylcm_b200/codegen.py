@@ -1485,14 +1485,17 @@ class RegimeKernels:
                 b.append(f"  gLo[{k} * {GMAX} + g] = lo{k}; gHi[{k} * {GMAX} + g] = hi{k};")
             b.append("}")
             b.append("__syncthreads();")
-            # pilot pass: a few spread actions per combination give a first threshold
+            # pilot pass: a few spread actions per combination (every lane of
+            # the state one of them) give a first threshold, the state's
+            # second best over them (a top-2 reduction over its lanes)
+            b.append("const int MPr = max(8, ncomb > 0 ? 32 / ncomb : 8);")
             b.append(f"float thr[{SB}];")
             b.append("{")
             b.append(f"  float p1[{SB}], p2[{SB}];")
             b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) p1[kb] = p2[kb] = {ninf};")
-            b.append(f"  for (int p = lane; p < ncomb * {MP}; p += {LANES}) {{")
-            b.append(f"    const int o_ = p / {MP}, m_ = p - o_ * {MP};")
-            b.append(f"    const int si = ((2 * m_ + 1) * gN) / {2 * MP};")
+            b.append(f"  for (int p = lane; p < ncomb * MPr; p += {LANES}) {{")
+            b.append("    const int o_ = p / MPr, m_ = p - o_ * MPr;")
+            b.append("    const int si = ((2 * m_ + 1) * gN) / (2 * MPr);")
             b.append("    const int j = (o_ / gS) * gN * gS + (o_ % gS) + si * gS;")
             b.append(f"    AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
             b.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
@@ -1502,89 +1505,133 @@ class RegimeKernels:
             b.append("      }")
             b.append("    }")
             b.append("  }")
-            b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) thr[kb] = p2[kb];")
-            b.append("}")
-            # the groups
-            b.append("for (int g = 0; g < NG; ++g) {")
-            b.append("  const int o_ = g / gpc, gi_ = g - o_ * gpc;")
-            b.append(f"  const int jb = (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;")
-            b.append(f"  const int m = min({G}, gN - gi_ * {G});")
-            b.append("  const float um = gU[g];")
-            for k in range(len(acts)):
-                b.append(f"  const float lo{k} = gLo[{k} * {GMAX} + g], hi{k} = gHi[{k} * {GMAX} + g];")
-                b.append(f"  const float am{k} = fmaxf(fabsf(lo{k}), fabsf(hi{k}));")
-            b.append(f"  bool run[{SB}]; bool any = false;")
             b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{")
-            b.append("    bool skip = false;")
-            b.append("    if (act[kb]) {")
-            h_i = 0
-            for c_i, (op, py, pc) in enumerate(gi["cons"]):
-                b.append(f"      {{ float lo = gY[kb][{c_i}], hi = lo, mag = fabsf(lo);")
-                for nm in pc:
-                    k = ks[nm]
-                    b.append(f"        {{ const float h = gH[kb][{h_i}]; lo += h >= 0.0f ? h * lo{k} : h * hi{k}; "
-                             f"hi += h >= 0.0f ? h * hi{k} : h * lo{k}; mag += fabsf(h) * am{k}; }}")
-                    h_i += 1
-                if op in ("<", "<="):
-                    b.append("        skip = skip || lo > 4e-6f * mag; }  // every member has lhs > rhs")
-                else:
-                    b.append("        skip = skip || hi < -4e-6f * mag; }  // every member has lhs < rhs")
-            b.append("      if (!skip) {")
-            b.append(f"        const float th = fmaxf(thr[kb], best[kb].idx2 >= 0 ? best[kb].v2 : {ninf});")
-            b.append("        bool ok = true;")
-            m_i = 0
-            lohi = []
-            for p, (pos, ci, px, pc) in enumerate(gi["axes"]):
-                b.append(f"        float lo_{p} = gK[kb][{p}], hi_{p} = lo_{p}, e_{p} = gE[kb][{p}];")
-                for nm in pc:
-                    k = ks[nm]
-                    b.append(f"        {{ const float mm = gM[kb][{m_i}]; lo_{p} += mm >= 0.0f ? mm * lo{k} : mm * hi{k}; "
-                             f"hi_{p} += mm >= 0.0f ? mm * hi{k} : mm * lo{k}; e_{p} += fabsf(mm) * am{k}; }}")
-                    m_i += 1
-                b.append(f"        e_{p} = 0.02f + 4e-6f * e_{p};")
-                b.append(f"        const int n_{p} = C.n{ti}_{pos};")
-                b.append(f"        ok = ok && lo_{p} - e_{p} >= 0.0f && hi_{p} + e_{p} <= (float)(n_{p} - 1);")
-                lohi.append(p)
-            b.append("        if (ok) {")
-            for p in lohi:
-                b.append(f"          const int L_{p} = (int)(lo_{p} - e_{p}), H_{p} = min((int)(hi_{p} + e_{p}) + 1, n_{p} - 1);")
-            b.append(f"          float mx = {ninf}, ab = 0.0f;")
-            if len(lohi) == 1:
-                b.append(f"          const float2* row = {gi['bst']} + (i64)keyr[kb] * ((n_0 + 15) >> 4);")
-                b.append("          for (int b1 = L_0 >> 4; b1 <= (H_0 >> 4); ++b1) {")
-                b.append("            const float2 st = __ldg(row + b1);")
-                b.append("            mx = lcm_nanmax(mx, st.x); ab = fmaxf(ab, st.y);")
-                b.append("          }")
-            else:
-                T1, T2 = self.GROUP_TILE
-                b.append(f"          const int nb1 = (n_0 + {T1 - 1}) / {T1}, nb2 = (n_1 + {T2 - 1}) / {T2};")
-                b.append(f"          const float2* base = {gi['bst']} + (i64)keyr[kb] * nb1 * nb2;")
-                b.append(f"          for (int b1 = L_0 / {T1}; b1 <= H_0 / {T1}; ++b1) {{")
-                b.append(f"            for (int b2 = L_1 / {T2}; b2 <= H_1 / {T2}; ++b2) {{")
-                b.append("              const float2 st = __ldg(base + (i64)b1 * nb2 + b2);")
-                b.append("              mx = lcm_nanmax(mx, st.x); ab = fmaxf(ab, st.y);")
-                b.append("            }")
-                b.append("          }")
-            b.append("          const float ub = um + beta_f * mx;")
-            b.append("          const float marg = 3.8e-6f * (fabsf(um) + beta_f * ab);")
-            b.append("          skip = ub + marg < th;")
-            b.append("        }")
-            b.append("      }")
+            b.append(f"    #pragma unroll\n    for (int o = {LANES} >> 1; o > 0; o >>= 1) {{")
+            b.append("      const float b1 = __shfl_xor_sync(0xffffffffu, p1[kb], o), b2 = __shfl_xor_sync(0xffffffffu, p2[kb], o);")
+            b.append("      p2[kb] = fmaxf(fminf(p1[kb], b1), fmaxf(p2[kb], b2));")
+            b.append("      p1[kb] = fmaxf(p1[kb], b1);")
             b.append("    }")
-            b.append("    run[kb] = act[kb] && !skip;")
-            b.append("    any = any || run[kb];")
-            b.append("  }")
-            b.append("  if (!any) continue;")
-            b.append(f"  for (int t = lane; t < m; t += {LANES}) {{")
-            b.append("    const int j = jb + t * gS;")
-            b.append(f"    AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
-            b.append("    const int aidx = ad * n_ac + j;")
-            b.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
-            b.append("      float q;")
-            b.append(f"      if (run[kb] && {call}) {{ if (q != q) best[kb].nan = 1; else best[kb].add(q, aidx); }}")
-            b.append("    }")
+            b.append("    thr[kb] = p2[kb];")
             b.append("  }")
             b.append("}")
+
+            def skip_lines(ind: str, th_expr: str) -> list[str]:
+                """`skip` of group (um, lo_k, hi_k, am_k) for state kb."""
+                L2: list[str] = []
+                h_i = 0
+                for c_i, (op, py, pc) in enumerate(gi["cons"]):
+                    L2.append(f"{{ float lo = gY[kb][{c_i}], hi = lo, mag = fabsf(lo);")
+                    for nm in pc:
+                        k = ks[nm]
+                        L2.append(f"  {{ const float h = gH[kb][{h_i}]; lo += h >= 0.0f ? h * lo{k} : h * hi{k}; "
+                                  f"hi += h >= 0.0f ? h * hi{k} : h * lo{k}; mag += fabsf(h) * am{k}; }}")
+                        h_i += 1
+                    if op in ("<", "<="):
+                        L2.append("  skip = skip || lo > 4e-6f * mag; }  // every member has lhs > rhs")
+                    else:
+                        L2.append("  skip = skip || hi < -4e-6f * mag; }  // every member has lhs < rhs")
+                L2.append("if (!skip) {")
+                L2.append(f"  const float th = {th_expr};")
+                L2.append("  bool ok = true;")
+                m_i = 0
+                lohi = []
+                for p, (pos, ci, px, pc) in enumerate(gi["axes"]):
+                    L2.append(f"  float lo_{p} = gK[kb][{p}], hi_{p} = lo_{p}, e_{p} = gE[kb][{p}];")
+                    for nm in pc:
+                        k = ks[nm]
+                        L2.append(f"  {{ const float mm = gM[kb][{m_i}]; lo_{p} += mm >= 0.0f ? mm * lo{k} : mm * hi{k}; "
+                                  f"hi_{p} += mm >= 0.0f ? mm * hi{k} : mm * lo{k}; e_{p} += fabsf(mm) * am{k}; }}")
+                        m_i += 1
+                    L2.append(f"  e_{p} = 0.02f + 4e-6f * e_{p};")
+                    L2.append(f"  const int n_{p} = C.n{ti}_{pos};")
+                    L2.append(f"  ok = ok && lo_{p} - e_{p} >= 0.0f && hi_{p} + e_{p} <= (float)(n_{p} - 1);")
+                    lohi.append(p)
+                L2.append("  if (ok) {")
+                for p in lohi:
+                    L2.append(f"    const int L_{p} = (int)(lo_{p} - e_{p}), H_{p} = min((int)(hi_{p} + e_{p}) + 1, n_{p} - 1);")
+                L2.append(f"    float mx = {ninf}, ab = 0.0f;")
+                if len(lohi) == 1:
+                    L2.append(f"    const float2* row = {gi['bst']} + (i64)keyr[kb] * ((n_0 + 15) >> 4);")
+                    L2.append("    for (int b1 = L_0 >> 4; b1 <= (H_0 >> 4); ++b1) {")
+                    L2.append("      const float2 st = __ldg(row + b1);")
+                    L2.append("      mx = lcm_nanmax(mx, st.x); ab = fmaxf(ab, st.y);")
+                    L2.append("    }")
+                else:
+                    T1, T2 = self.GROUP_TILE
+                    L2.append(f"    const int nb1 = (n_0 + {T1 - 1}) / {T1}, nb2 = (n_1 + {T2 - 1}) / {T2};")
+                    L2.append(f"    const float2* base = {gi['bst']} + (i64)keyr[kb] * nb1 * nb2;")
+                    L2.append(f"    for (int b1 = L_0 / {T1}; b1 <= H_0 / {T1}; ++b1) {{")
+                    L2.append(f"      for (int b2 = L_1 / {T2}; b2 <= H_1 / {T2}; ++b2) {{")
+                    L2.append("        const float2 st = __ldg(base + (i64)b1 * nb2 + b2);")
+                    L2.append("        mx = lcm_nanmax(mx, st.x); ab = fmaxf(ab, st.y);")
+                    L2.append("      }")
+                    L2.append("    }")
+                L2.append("    const float ub = um + beta_f * mx;")
+                L2.append("    const float marg = 3.8e-6f * (fabsf(um) + beta_f * ab);")
+                L2.append("    skip = ub + marg < th;")
+                L2.append("  }")
+                L2.append("}")
+                return [ind + x for x in L2]
+
+            def group_vars(ind: str, g: str) -> list[str]:
+                L2 = [f"const float um = gU[{g}];"]
+                for k in range(len(acts)):
+                    L2.append(f"const float lo{k} = gLo[{k} * {GMAX} + {g}], hi{k} = gHi[{k} * {GMAX} + {g}];")
+                    L2.append(f"const float am{k} = fmaxf(fabsf(lo{k}), fabsf(hi{k}));")
+                return [ind + x for x in L2]
+
+            def eval_members(ind: str, cond: str) -> list[str]:
+                L2 = [f"const int o_ = gg / gpc, gi_ = gg - o_ * gpc;",
+                      f"const int jb = (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;",
+                      f"const int m = min({G}, gN - gi_ * {G});",
+                      f"for (int t = lane; t < m; t += {LANES}) {{",
+                      "  const int j = jb + t * gS;",
+                      f"  AFTab_{self.tag}<float> af{{tabf, tabi, j}};",
+                      "  const int aidx = ad * n_ac + j;",
+                      f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{",
+                      "    float q;",
+                      f"    if ({cond} && {call}) {{ if (q != q) best[kb].nan = 1; else best[kb].add(q, aidx); }}",
+                      "  }",
+                      "}"]
+                return [ind + x for x in L2]
+
+            if LANES == 32:
+                # a warp per state: lane i tests group g0 + i against the
+                # pilot threshold; the warp then evaluates the surviving
+                # groups, one member per lane -- every decision is uniform
+                # over the warp
+                b.append("for (int g0 = 0; g0 < NG; g0 += 32) {")
+                b.append("  const int gl = min(g0 + lane, NG - 1);")
+                b += group_vars("  ", "gl")
+                b.append(f"  unsigned need[{SB}]; unsigned anyb = 0u;")
+                b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{")
+                b.append("    bool skip = false;")
+                b += skip_lines("    ", f"fmaxf(thr[kb], best[kb].idx2 >= 0 ? best[kb].v2 : {ninf})")
+                b.append("    need[kb] = __ballot_sync(0xffffffffu, act[kb] && g0 + lane < NG && !skip);")
+                b.append("    anyb |= need[kb];")
+                b.append("  }")
+                b.append("  while (anyb) {")
+                b.append("    const int bit = __ffs(anyb) - 1;")
+                b.append("    anyb &= anyb - 1u;")
+                b.append("    const int gg = g0 + bit;")
+                b += eval_members("    ", "((need[kb] >> bit) & 1u)")
+                b.append("  }")
+                b.append("}")
+            else:
+                b.append("for (int gg = 0; gg < NG; ++gg) {")
+                b += group_vars("  ", "gg")
+                b.append(f"  bool run[{SB}]; bool any = false;")
+                b.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{")
+                b.append("    bool skip = false;")
+                b.append("    if (act[kb]) {")
+                b += skip_lines("      ", f"fmaxf(thr[kb], best[kb].idx2 >= 0 ? best[kb].v2 : {ninf})")
+                b.append("    }")
+                b.append("    run[kb] = act[kb] && !skip;")
+                b.append("    any = any || run[kb];")
+                b.append("  }")
+                b.append("  if (!any) continue;")
+                b += eval_members("  ", "run[kb]")
+                b.append("}")
             o += ["  " + x for x in b]
             o.append("}")
             return o
