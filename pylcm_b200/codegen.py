@@ -451,6 +451,9 @@ class LaunchConfig:
     sb: int = 1  # states per thread (register blocking)
     min_blocks: int = 0  # __launch_bounds__ min CTAs per SM (0 = compiler's choice)
     prune: bool = True  # single-precision search: exact skipping of action groups where eligible
+    # ... also in regimes with several continuous actions (measured slower than
+    # the full search on the human-capital model: off unless asked for)
+    prune_multi: bool = False
     group: int = 16  # actions per skipped group (raised to `lanes` if smaller)
 
     @property
@@ -687,7 +690,7 @@ class RegimeKernels:
                 or tr.regime_id is None or tr.beta is None):
             return None
         cacts = [a for a in spec.actions if a.kind == "continuous"]
-        if not cacts:
+        if not cacts or (len(cacts) > 1 and not self.cfg.prune_multi):
             return None
         cn = {a.name for a in cacts}
         U, beta = ir.const(tr.U), ir.const(tr.beta)

@@ -132,9 +132,7 @@ ENVELOPE_MAX_N = 4096  # longest candidate row of the LTM / RFC / MSS envelope k
 
 
 def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> LaunchConfig:
-    """Launch shape of kernel (a).  Single-precision search over several
-    continuous actions: a warp per state (32 lanes).  Otherwise preferred: 2
-    lanes per state and, in the
+    """Launch shape of kernel (a).  Preferred: 2 lanes per state and, in the
     single-precision search, 4 states per thread (each thread's states share
     the shared-memory action loads and give the scheduler independent work --
     the fastest shapes measured on the B200; in double precision more states
@@ -144,11 +142,6 @@ def default_config(spec: RegimeSpec, precision: str, n_items: int = 1) -> Launch
     n_a = spec.n_actions
     total = max(1, spec.n_states * n_items)
     want = SM_COUNT * RESIDENT_THREADS_PER_SM
-    n_cont = sum(1 for a in spec.actions if a.kind == "continuous")
-    if precision == "fp32" and n_cont >= 2 and not spec.taste_shocks and total >= want // 32:
-        # several continuous actions: a warp per state, the form in which the
-        # exact group skipping decides each group for the whole warp at once
-        return LaunchConfig(block=256, lanes=32, chunk=512, sb=1)
     lanes = 2 if n_a >= 64 else 1
     sb = 4 if precision == "fp32" else 1
     while sb > 1 and total * lanes < want * sb:

@@ -67,7 +67,10 @@ def test_eligibility():
     k = _kernels(M.stochastic_model(4, 30, 40), M.stochastic_params(), "fp32", prune=False)
     assert not any(r.prunes_groups for r in k.values())
     # two continuous actions, two continuous target states: tile statistics
+    # (only when asked for)
     k = _kernels(M.hc_model(3, 10, 4, 4, 8), M.hc_params(0, 4), "fp32")
+    assert not k["alive"].prunes_groups
+    k = _kernels(M.hc_model(3, 10, 4, 4, 8), M.hc_params(0, 4), "fp32", prune_multi=True)
     assert k["alive"].prunes_groups and not k["terminal"].prunes_groups
     assert [k["alive"].group_stats(t) for t in k["alive"].targets] == [2]
     assert "lcm_tile_stats_" in k["alive"].source()
@@ -99,8 +102,8 @@ def test_skipping_is_exact(case, lanes, sb):
     ps = CASES[case][1]()
     res = []
     for prune in (True, False):
-        cfg = {s.name: dataclasses.replace(default_config(s, "fp32", len(ps)), lanes=lanes, sb=sb, prune=prune)
-               for s in model.regime_specs}
+        cfg = {s.name: dataclasses.replace(default_config(s, "fp32", len(ps)), lanes=lanes, sb=sb, prune=prune,
+                                           prune_multi=prune) for s in model.regime_specs}
         plan = SolveEngine(model, "fp32", configs=cfg).plan(ps)
         plan.run()
         torch.cuda.synchronize()
@@ -129,7 +132,8 @@ def test_tile_statistics_match_the_float_table():
     import torch
 
     model = M.hc_model(4, 70, 9, 5, 40)
-    plan = SolveEngine(model, "fp32").plan([M.hc_params(s, 5) for s in range(2)])
+    cfg = {s.name: dataclasses.replace(default_config(s, "fp32", 2), prune_multi=True) for s in model.regime_specs}
+    plan = SolveEngine(model, "fp32", configs=cfg).plan([M.hc_params(s, 5) for s in range(2)])
     plan.run()
     torch.cuda.synchronize()
     checked = 0

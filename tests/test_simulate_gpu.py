@@ -103,13 +103,13 @@ def test_batched_simulation_equals_single_instance_runs(rng):
     eng = model.engine("fp64")
     plan = eng.plan(plist)
     plan.run()
-    rng = np.random.default_rng(8)
+    gen = np.random.default_rng(8)
     ics, seeds = [], [3, 4, 3]
     for k in range(3):
         n = 40 + 17 * k
         ics.append({
-            "wealth": rng.uniform(1, 50, n),
-            "income": rng.normal(0, 0.1, n),
+            "wealth": gen.uniform(1, 50, n),
+            "income": gen.normal(0, 0.1, n),
             "age": np.zeros(n),
             "regime_id": np.zeros(n, dtype=int),
         })
