@@ -309,7 +309,11 @@ static CUresult opt_in_smem(CUfunction f, int dyn_bytes) {
   int stat = 0;
   if (g_drv.FuncGetAttribute(&stat, CU_FUNC_ATTRIBUTE_SHARED_SIZE_BYTES, f) != CUDA_SUCCESS) stat = 0;
   if ((long long)dyn_bytes + stat <= 48 * 1024) return CUDA_SUCCESS;
-  return g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn_bytes);
+  const CUresult r = g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, dyn_bytes);
+  if (r != CUDA_SUCCESS) return r;
+  // such a kernel is limited by shared memory: ask for the largest carveout
+  // so that as many CTAs fit per SM as its registers allow
+  return g_drv.FuncSetAttribute(f, CU_FUNC_ATTRIBUTE_PREFERRED_SHARED_MEMORY_CARVEOUT, 100);
 }
 
 extern "C" int lcmx_occupancy(lcmx_module* mod, const char* kernel, int block, int smem_bytes, int* blocks_per_sm) {
