@@ -1227,14 +1227,7 @@ class RegimeKernels:
         ap(f"    const int n_ac = n_actions / {ND};")
         ap(f"    const double* __restrict__ atf = lcm_wp<const double>(it, {self.W_ATAB});")
         ap(f"    const int* __restrict__ ati = reinterpret_cast<const int*>(atf + (i64){nf} * n_actions);")
-        # a thread's state slots: SPB apart (the default), or -- with group
-        # skipping -- SB consecutive states, so that a warp's states are
-        # neighbours whose surviving groups coincide
-        consecutive = bool(self._groups) and SB > 1
-        if consecutive:
-            ap(f"    const int sbase = (tile - tile_prefix[item]) * {SPT} + ((int)threadIdx.x / {LANES}) * {SB};")
-        else:
-            ap(f"    const int sbase = (tile - tile_prefix[item]) * {SPT} + (int)threadIdx.x / {LANES};")
+        ap(f"    const int sbase = (tile - tile_prefix[item]) * {SPT} + (int)threadIdx.x / {LANES};")
         ap(f"    const int lane = (int)threadIdx.x % {LANES};")
         cache_at = len(L)  # the action-table cache block goes here
         ap("    (void)period; (void)age; (void)ati; (void)PV;")
@@ -1247,7 +1240,7 @@ class RegimeKernels:
             ap("    PVd[0] = 0.0;")
         ap(f"    int SI[{SB}][{NDS}]; double SV[{SB}][{nS}]; bool act[{SB}]; int sidx[{SB}];")
         ap(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
-        ap(f"      const int s = sbase + kb * {1 if consecutive else SPB};")
+        ap(f"      const int s = sbase + kb * {SPB};")
         ap("      act[kb] = s < n_states; sidx[kb] = s;")
         ap("      int srem = act[kb] ? s : 0;")
         for k in range(len(spec.states) - 1, -1, -1):
