@@ -540,6 +540,47 @@ __device__ __forceinline__ void lcm_bracket_read(double x0, double x1, double f0
 // instead of searching the row in memory.  The result equals
 // lcm_row_bracket's on every lane (a NaN query gets L - 1, as there); with a
 // wider window every lane falls back to its own search.
+// lcm_row_bracket of two warp-uniform queries qa, qb (same xp and L on every
+// lane of a converged warp) by a 32-ary search: each round every lane tests
+// one node of the current interval and a ballot keeps the sub-interval that
+// holds the first node above the query -- ceil(log32(L)) + 1 dependent rounds
+// instead of log2(L).  Invariant: the first node above q lies in [lo, hi],
+// where hi == L or xp[hi] > q; a probe at or past hi is "above" without a
+// load, so no lane reads past the row.
+__device__ __forceinline__ void lcm_row_bracket_coop2(const double* __restrict__ xp, int L, double qa, double qb,
+                                                      int& ia, int& ib) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int alo = 0, ahi = L, blo = 0, bhi = L;
+  while (alo < ahi || blo < bhi) {
+    const int sa = (ahi - alo + 31) >> 5, sb = (bhi - blo + 31) >> 5;
+    const int ma = alo + (lane + 1) * sa - 1, mb = blo + (lane + 1) * sb - 1;
+    const bool up_a = alo < ahi && (ma >= ahi || xp[ma] > qa);
+    const bool up_b = blo < bhi && (mb >= bhi || xp[mb] > qb);
+    const unsigned ba = __ballot_sync(full, up_a), bb = __ballot_sync(full, up_b);
+    if (alo < ahi) {
+      if (ba == 0u) {
+        alo = ahi;
+      } else {
+        const int f = __ffs(ba) - 1, mf = alo + (f + 1) * sa - 1;
+        alo += f * sa;
+        ahi = mf < ahi ? mf : ahi;
+      }
+    }
+    if (blo < bhi) {
+      if (bb == 0u) {
+        blo = bhi;
+      } else {
+        const int f = __ffs(bb) - 1, mf = blo + (f + 1) * sb - 1;
+        blo += f * sb;
+        bhi = mf < bhi ? mf : bhi;
+      }
+    }
+  }
+  ia = alo - 1;
+  ib = blo - 1;
+}
+
 __device__ __forceinline__ int lcm_row_bracket_warp(const double* __restrict__ xp, int L, double xq) {
   const unsigned full = 0xffffffffu;
   double qmin = xq, qmax = xq;  // fmin / fmax skip NaN queries
@@ -549,10 +590,16 @@ __device__ __forceinline__ int lcm_row_bracket_warp(const double* __restrict__ x
     qmax = fmax(qmax, __shfl_xor_sync(full, qmax, o));
   }
   if (qmin != qmin) return L - 1;  // every query is NaN
-  const int i_lo = lcm_row_bracket(xp, L, qmin);
-  const int i_hi = lcm_row_bracket(xp, L, qmax);
+  int i_lo, i_hi;
+  lcm_row_bracket_coop2(xp, L, qmin, qmax, i_lo, i_hi);
   const int W = i_hi - i_lo;  // nodes in (i_lo, i_hi]
-  if (W > 32) return xq != xq ? L - 1 : lcm_row_bracket(xp, L, xq);
+  if (W > 32) {
+    // every lane's first node above its query lies in [i_lo + 1, i_hi + 1]
+    if (xq != xq) return L - 1;
+    int lo = i_lo + 1, hi = i_hi + 1;
+    while (lo < hi) { const int mid = (lo + hi) >> 1; if (xp[mid] > xq) hi = mid; else lo = mid + 1; }
+    return lo - 1;
+  }
   const int lane = threadIdx.x & 31;
   const double node = lane < W ? xp[i_lo + 1 + lane] : LCM_INF;
   int lo = 0, hi = W;
