@@ -509,11 +509,14 @@ def run_serving(args, local: int) -> dict:
     srv = Server(device=local, precision="fp32", max_batch=args.serve_batch, n_streams=args.serve_streams)
     srv.run([dataclasses.replace(r) for r in reqs], realtime=False)  # kernels compiled, pools built
     srv.job_gpu_ms, srv.batch_sizes = [], []
+    srv.host_phase_s, srv.host_launch_s, srv.host_finish_s, srv.jobs_run = {}, 0.0, 0.0, 0
     t = time.perf_counter()
     srv.run([dataclasses.replace(r) for r in reqs], realtime=False)
     cap_wall = time.perf_counter() - t
     capacity = n / cap_wall
     cap_gpu = sum(srv.job_gpu_ms)
+    cap_host = {"launch_s": srv.host_launch_s, "finish_s": srv.host_finish_s, "jobs": srv.jobs_run,
+                "phases_s": dict(srv.host_phase_s)}
     rate = 0.75 * capacity  # offered load within 70-90 % of the measured capacity
     arr = np.cumsum(np.random.default_rng(8).exponential(1.0 / rate, size=n))
     reqs_p = [dataclasses.replace(r, arrival=float(a)) for r, a in zip(reqs, arr)]
@@ -552,6 +555,7 @@ def run_serving(args, local: int) -> dict:
         "p99_ms": summ["p99_ms"],
         "mean_batch": summ["mean_batch"],
         "gpu_busy_frac_at_capacity": cap_gpu / 1e3 / cap_wall,
+        "host_at_capacity": cap_host,
         "host_launch_s": srv.host_launch_s,
         "plain": {
             "solves_per_s": plain_rate,
