@@ -1214,7 +1214,6 @@ class RegimeKernels:
         gumax_at = len(L)  # a per-group utility maximum is declared here when groups are skipped
         ap(f"  {TT}* tabf = reinterpret_cast<{TT}*>(lcm_smem);")
         ap(f"  int* tabi = reinterpret_cast<int*>(lcm_smem + {NF * CH * (4 if fp32 else 8)});")
-        citem_at = len(L)  # the cached item's index is declared here when the action table is cached
         ap("  for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {")
         ap("    const int item = lcm_find_item(tile_prefix, n_items, tile);")
         ap(f"    const i64* __restrict__ it = items + (i64)item * {self.n_words};")
@@ -1229,7 +1228,6 @@ class RegimeKernels:
         ap(f"    const int* __restrict__ ati = reinterpret_cast<const int*>(atf + (i64){nf} * n_actions);")
         ap(f"    const int sbase = (tile - tile_prefix[item]) * {SPT} + (int)threadIdx.x / {LANES};")
         ap(f"    const int lane = (int)threadIdx.x % {LANES};")
-        cache_at = len(L)  # the action-table cache block goes here
         ap("    (void)period; (void)age; (void)ati; (void)PV;")
         for s_ in eP.lines:
             ap("    " + s_)
@@ -1327,29 +1325,6 @@ class RegimeKernels:
             o.append("}")
             return o
 
-        def inner_loop_cached(sa_fn: str) -> list[str]:
-            """inner_loop over the action table cached in shared memory
-            (no loads, no barriers)."""
-            o = []
-            di_args = "".join(f"DI_{a.name}, " for a in dacts)
-            call = f"{sa_fn}<{ST}, {ST}>(C, PV, PVd, DV, SV[kb], SDV[kb], af, SI[kb], {di_args}period, age, q)"
-            push = "bd[kb][ad].push(q, aidx);" if taste else "best[kb].push(q, aidx);"
-            o.append(f"for (int j = lane; j < n_ac; j += {LANES}) {{")
-            o.append("  const int aidx = ad * n_ac + j;")
-            o.append(f"  AFTab_{self.tag}<{ST}> af{{tabf, tabi, aidx}};")
-            o.append(f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{")
-            o.append(f"    {ST} q;")
-            o.append(f"    if ({call}) {push}")
-            o.append("  }")
-            o.append("}")
-            return o
-
-        def inner_loop_any(sa_fn: str) -> list[str]:
-            if not cache_on:
-                return inner_loop(sa_fn)
-            return ["if (use_cache) {"] + ["  " + x for x in inner_loop_cached(sa_fn)] + ["} else {"] + \
-                ["  " + x for x in inner_loop(sa_fn)] + ["}"]
-
         # ---- exact skipping of action groups (single-precision search)
         G = max(cfg.group, LANES)
         GP = self._groups
@@ -1446,9 +1421,17 @@ class RegimeKernels:
             ti = gi["ti"]
             ninf = "-lcm_lim<float>::inf()"
             o.append(f"const float beta_f = (float)({gi['beta']});")
-            o.append(f"const bool grp = use_cache && {gi['bst']} != nullptr && beta_f >= 0.0f;  // uniform over the CTA")
+            o.append(f"const int gN = lcm_wi(it, {self.W_ASIZE + kscan});")
+            o.append("int gS = 1;")
+            for k in later:
+                o.append(f"gS *= lcm_wi(it, {self.W_ASIZE + k});")
+            o.append(f"const int gpc = (gN + {G - 1}) / {G};")
+            o.append("const int ncomb = gN > 0 ? n_ac / gN : 0;")
+            o.append("const int NG = ncomb * gpc;")
+            o.append(f"const bool grp = {gi['bst']} != nullptr && beta_f >= 0.0f && n_ac <= {CH} && gN >= {G} "
+                     f"&& NG <= {GMAX};  // uniform over the CTA (one item per tile)")
             o.append("if (!grp) {")
-            o += ["  " + x for x in inner_loop_any(sa_fn)]
+            o += ["  " + x for x in inner_loop(sa_fn)]
             o.append("} else {")
             b: list[str] = []
             # per-state affine pieces (float), coordinates in grid units
@@ -1475,8 +1458,36 @@ class RegimeKernels:
                     h_i += 1
             b.append(f"  keyr[kb] = {gi['key']};")
             b.append("}")
-            b.append("const int jad = ad * n_ac;  // this discrete action's part of the cached table")
-            b.append("const int gad = ad * NG;    // ... and of the group statistics")
+            # the continuous-action table of this discrete action, whole
+            b.append("__syncthreads();")
+            b.append(f"for (int j = threadIdx.x; j < n_ac; j += {B}) {{")
+            b.append("  const i64 a = (i64)ad * n_ac + j;")
+            for k in range(nf):
+                b.append(f"  tabf[{k} * {CH} + j] = ({TT})atf[(i64){k} * n_actions + a];")
+            for k in range(ni):
+                b.append(f"  tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
+            b.append("}")
+            b.append("__syncthreads();")
+            # per-group utility maximum and action ranges
+            b.append(f"for (int g = threadIdx.x; g < NG; g += {B}) {{")
+            b.append("  const int o_ = g / gpc, gi_ = g - o_ * gpc;")
+            b.append(f"  const int jb = (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;")
+            b.append(f"  const int m = min({G}, gN - gi_ * {G});")
+            b.append(f"  float um = {ninf};")
+            for k in range(len(acts)):
+                b.append(f"  float lo{k} = lcm_lim<float>::inf(), hi{k} = {ninf};")
+            b.append("  for (int t = 0; t < m; ++t) {")
+            b.append("    const int j = jb + t * gS;")
+            b.append(f"    um = lcm_nanmax(um, tabf[{gi['uf']} * {CH} + j]);")
+            for nm, k in ks.items():
+                b.append(f"    {{ const float v = tabf[{gi['avf'][nm]} * {CH} + j]; lo{k} = fminf(lo{k}, v); "
+                         f"hi{k} = fmaxf(hi{k}, v); }}")
+            b.append("  }")
+            b.append("  gU[g] = um;")
+            for k in range(len(acts)):
+                b.append(f"  gLo[{k} * {GMAX} + g] = lo{k}; gHi[{k} * {GMAX} + g] = hi{k};")
+            b.append("}")
+            b.append("__syncthreads();")
             # pilot pass: a few spread actions per combination (every lane of
             # the state one of them) give a first threshold, the state's
             # second best over them (a top-2 reduction over its lanes)
@@ -1488,7 +1499,7 @@ class RegimeKernels:
             b.append(f"  for (int p = lane; p < ncomb * MPr; p += {LANES}) {{")
             b.append("    const int o_ = p / MPr, m_ = p - o_ * MPr;")
             b.append("    const int si = ((2 * m_ + 1) * gN) / (2 * MPr);")
-            b.append("    const int j = jad + (o_ / gS) * gN * gS + (o_ % gS) + si * gS;")
+            b.append("    const int j = (o_ / gS) * gN * gS + (o_ % gS) + si * gS;")
             b.append(f"    AFTab_{self.tag}<float> af{{tabf, tabi, j}};")
             b.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
             b.append("      float q;")
@@ -1566,9 +1577,9 @@ class RegimeKernels:
                 return [ind + x for x in L2]
 
             def group_vars(ind: str, g: str) -> list[str]:
-                L2 = [f"const float um = gU[gad + {g}];"]
+                L2 = [f"const float um = gU[{g}];"]
                 for k in range(len(acts)):
-                    L2.append(f"const float lo{k} = gLo[{k} * {GMAX} + gad + {g}], hi{k} = gHi[{k} * {GMAX} + gad + {g}];")
+                    L2.append(f"const float lo{k} = gLo[{k} * {GMAX} + {g}], hi{k} = gHi[{k} * {GMAX} + {g}];")
                     L2.append(f"const float am{k} = fmaxf(fabsf(lo{k}), fabsf(hi{k}));")
                 return [ind + x for x in L2]
 
@@ -1577,9 +1588,9 @@ class RegimeKernels:
                       f"const int jb = (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;",
                       f"const int m = min({G}, gN - gi_ * {G});",
                       f"for (int t = lane; t < m; t += {LANES}) {{",
-                      "  const int j = jad + jb + t * gS;",
+                      "  const int j = jb + t * gS;",
                       f"  AFTab_{self.tag}<float> af{{tabf, tabi, j}};",
-                      "  const int aidx = j;",
+                      "  const int aidx = ad * n_ac + j;",
                       f"  #pragma unroll\n  for (int kb = 0; kb < {SB}; ++kb) {{",
                       "    float q;",
                       f"    if ({cond} && {call}) {{ if (q != q) best[kb].nan = 1; else best[kb].add(q, aidx); }}",
@@ -1628,59 +1639,8 @@ class RegimeKernels:
             o.append("}")
             return o
 
-        ginfos = {ti: group_info(ti) for ti in range(len(self.targets))} if unswitch else {}
-        cache_on = any(v is not None for v in ginfos.values())
-
-        def cache_block() -> list[str]:
-            """Per tile: the whole action table (every discrete action) and
-            its group statistics, loaded into shared memory when the CTA's
-            tile moves to another item, so that the skipping loop runs
-            without barriers (a CTA's warps do not wait for each other between
-            tiles)."""
-            gi0 = next(v for v in ginfos.values() if v is not None)
-            acts = GP["acts"]
-            anames = [a.name for a in spec.actions]
-            cnames = GP["cacts"]
-            kscan = anames.index(cnames[GP["scan"]])
-            later = [anames.index(nm) for nm in cnames[GP["scan"] + 1:]]
-            ninf = "-lcm_lim<float>::inf()"
-            c = [f"const int gN = lcm_wi(it, {self.W_ASIZE + kscan});", "int gS = 1;"]
-            c += [f"gS *= lcm_wi(it, {self.W_ASIZE + k});" for k in later]
-            c += [f"const int gpc = (gN + {G - 1}) / {G};",
-                  "const int ncomb = gN > 0 ? n_ac / gN : 0;",
-                  "const int NG = ncomb * gpc;",
-                  f"const bool use_cache = n_actions <= {CH} && gN >= {G} && {ND} * NG <= {GMAX};  // uniform over the CTA",
-                  "if (use_cache && item != cached_item) {",
-                  "  __syncthreads();",
-                  f"  for (int a = threadIdx.x; a < n_actions; a += {B}) {{"]
-            c += [f"    tabf[{k} * {CH} + a] = ({TT})atf[(i64){k} * n_actions + a];" for k in range(nf)]
-            c += [f"    tabi[{k} * {CH} + a] = ati[(i64){k} * n_actions + a];" for k in range(ni)]
-            c += ["  }", "  __syncthreads();",
-                  f"  for (int g = threadIdx.x; g < {ND} * NG; g += {B}) {{",
-                  "    const int adg = g / NG, gr = g - adg * NG;",
-                  "    const int o_ = gr / gpc, gi_ = gr - o_ * gpc;",
-                  f"    const int jb = adg * n_ac + (o_ / gS) * gN * gS + (o_ % gS) + gi_ * {G} * gS;",
-                  f"    const int m = min({G}, gN - gi_ * {G});",
-                  f"    float um = {ninf};"]
-            for k in range(len(acts)):
-                c.append(f"    float lo{k} = lcm_lim<float>::inf(), hi{k} = {ninf};")
-            c += ["    for (int t = 0; t < m; ++t) {", "      const int j = jb + t * gS;",
-                  f"      um = lcm_nanmax(um, tabf[{gi0['uf']} * {CH} + j]);"]
-            for k, nm in enumerate(acts):
-                c.append(f"      {{ const float v = tabf[{gi0['avf'][nm]} * {CH} + j]; lo{k} = fminf(lo{k}, v); "
-                         f"hi{k} = fmaxf(hi{k}, v); }}")
-            c += ["    }", "    gU[g] = um;"]
-            for k in range(len(acts)):
-                c.append(f"    gLo[{k} * {GMAX} + g] = lo{k}; gHi[{k} * {GMAX} + g] = hi{k};")
-            c += ["  }", "  __syncthreads();", "  cached_item = item;", "}",
-                  "if (!use_cache) cached_item = -1;  // the chunked loop below overwrites the table"]
-            return ["    " + x for x in c]
-
         any_pruned = False
         n_gacts = 0
-        if cache_on:
-            L[cache_at:cache_at] = cache_block()
-            L.insert(citem_at, "  int cached_item = -1;  // the item whose action table the shared memory holds")
         if unswitch:
             rid_expr = f"(int)PVd[{[id(x) for x in bP].index(id(self.tr.regime_id))}]" if rid_phase == "P" else None
             if rid_phase == "D":
@@ -1690,20 +1650,20 @@ class RegimeKernels:
             for ti, t in enumerate(self.targets):
                 ap(f"      {'if' if first else 'else if'} (rid == {t.spec.rid}) {{")
                 first = False
-                gi = ginfos[ti]
+                gi = group_info(ti)
                 if gi is not None:
                     any_pruned = True
                     n_gacts = max(n_gacts, len(GP["acts"]))
-                body = inner_loop_any(SA.format(ti + 1)) if gi is None else inner_loop_groups(SA.format(ti + 1), gi)
+                body = inner_loop(SA.format(ti + 1)) if gi is None else inner_loop_groups(SA.format(ti + 1), gi)
                 for s_ in body:
                     ap("        " + s_)
                 ap("      }")
             ap("      else {")
-            for s_ in inner_loop_any(SA.format(0)):
+            for s_ in inner_loop(SA.format(0)):
                 ap("        " + s_)
             ap("      }")
         else:
-            for s_ in inner_loop_any(SA.format(0)):
+            for s_ in inner_loop(SA.format(0)):
                 ap("      " + s_)
         ap("    }")
         if any_pruned:
