@@ -625,3 +625,101 @@ __device__ __forceinline__ void lcm_row_read(const double* __restrict__ xp, cons
   lcm_bracket_read(xp[b], xp[b + 1], fp[b], fp[b + 1], dp ? dp[b] : 0.0, dp ? dp[b + 1] : 0.0, dp != nullptr, idx, xq,
                    val, slope_val);
 }
+
+// lcm_row_read of K rows at the same per-lane query, for the 32 converged
+// lanes of a warp that read the same K rows (row k: xp[k], fp[k], dp[k], L[k]
+// equal on every lane).  The rows' searches run interleaved -- one 32-ary
+// ballot search with 2K heads (each row's bracket of the warp's smallest and
+// largest query), then each row's window search -- so their dependent loads
+// overlap.  Every result equals lcm_row_read's.
+template <int K>
+__device__ __forceinline__ void lcm_row_read_warpk(const double* const* xp, const double* const* fp,
+                                                   const double* const* dp, const int* L, double xq, double* val,
+                                                   double* slope_val) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  double qmin = xq, qmax = xq;  // fmin / fmax skip NaN queries
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    qmin = fmin(qmin, __shfl_xor_sync(full, qmin, o));
+    qmax = fmax(qmax, __shfl_xor_sync(full, qmax, o));
+  }
+  const bool all_nan = qmin != qmin;
+  // heads 2k, 2k + 1: row k at qmin, qmax (rows of fewer than 2 nodes, or
+  // every query NaN: no search)
+  int lo[2 * K], hi[2 * K];
+#pragma unroll
+  for (int h = 0; h < 2 * K; ++h) {
+    lo[h] = 0;
+    hi[h] = (L[h >> 1] >= 2 && !all_nan) ? L[h >> 1] : 0;
+  }
+  bool active = true;
+  while (active) {
+    bool up[2 * K];
+    int s[2 * K];
+#pragma unroll
+    for (int h = 0; h < 2 * K; ++h) {
+      s[h] = (hi[h] - lo[h] + 31) >> 5;
+      const int m = lo[h] + (lane + 1) * s[h] - 1;
+      const double q = (h & 1) ? qmax : qmin;
+      up[h] = lo[h] < hi[h] && (m >= hi[h] || xp[h >> 1][m] > q);
+    }
+    active = false;
+#pragma unroll
+    for (int h = 0; h < 2 * K; ++h) {
+      const unsigned b = __ballot_sync(full, up[h]);
+      if (lo[h] < hi[h]) {
+        if (b == 0u) {
+          lo[h] = hi[h];
+        } else {
+          const int f = __ffs(b) - 1, mf = lo[h] + (f + 1) * s[h] - 1;
+          lo[h] += f * s[h];
+          hi[h] = mf < hi[h] ? mf : hi[h];
+        }
+      }
+      active = active || lo[h] < hi[h];
+    }
+  }
+  // each row's window (i_lo, i_hi]: one node per lane, then a shuffle search
+  double node[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int i_lo = lo[2 * k] - 1, W = lo[2 * k + 1] - lo[2 * k];
+    node[k] = (L[k] >= 2 && !all_nan && W <= 32 && lane < W) ? xp[k][i_lo + 1 + lane] : LCM_INF;
+  }
+  int idx[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int i_lo = lo[2 * k] - 1, W = lo[2 * k + 1] - lo[2 * k];
+    int a = 0, z = W;
+#pragma unroll
+    for (int st = 0; st < 6; ++st) {
+      const int mid = (a + z) >> 1;
+      const double x = __shfl_sync(full, node[k], mid & 31);
+      if (a < z && W <= 32) {
+        if (x > xq) z = mid; else a = mid + 1;
+      }
+    }
+    if (W > 32 && xq == xq) {
+      // every lane's first node above its query lies in [i_lo + 1, i_hi + 1]
+      a = i_lo + 1;
+      z = lo[2 * k + 1];
+      while (a < z) { const int mid = (a + z) >> 1; if (xp[k][mid] > xq) z = mid; else a = mid + 1; }
+      idx[k] = a - 1;
+    } else {
+      idx[k] = (xq != xq || all_nan) ? L[k] - 1 : i_lo + a;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int Lk = L[k];
+    if (Lk <= 0) { val[k] = slope_val[k] = LCM_NAN; continue; }
+    if (Lk == 1) { val[k] = fp[k][0]; slope_val[k] = dp[k] ? dp[k][0] : LCM_NAN; continue; }
+    const int ix = idx[k];
+    if (ix >= Lk - 1) { val[k] = fp[k][Lk - 1]; slope_val[k] = dp[k] ? dp[k][Lk - 1] : LCM_NAN; continue; }
+    const int b = ix < 0 ? 0 : ix;
+    const double* d = dp[k];
+    lcm_bracket_read(xp[k][b], xp[k][b + 1], fp[k][b], fp[k][b + 1], d ? d[b] : 0.0, d ? d[b + 1] : 0.0, d != nullptr,
+                     ix, xq, val[k], slope_val[k]);
+  }
+}

@@ -284,17 +284,41 @@ class EgmKernels:
                 body.append("      den += wt;")
                 body.append("      if (wt == 0.0) continue;")
                 body.append(f"      double vals[{nd_t}], mus[{nd_t}];")
-                body.append(f"      for (int d = 0; d < {nd_t}; ++d) {{")
-                body.append(f"        const i64 crow = (i64)jc * {nd_t} + d;")
-                body.append("        const int Lk = min(NK[crow], npad);")
                 # the shared search needs the row's control flow to be the
                 # same on every lane: the regime probability and the node
                 # weights must not depend on the savings node
                 uniform = not any(n is A_VAR for n in ir.topo_order([ir.const(x) for x in self._row_exprs(t)]))
                 flag = "warp_row" if uniform else "false"
-                body.append("        lcm_row_read(RG + crow * npad, RV + crow * npad, RM + crow * npad, NK[crow] > npad ? 0 : Lk, "
-                            f"Rn, vals[d], mus[d], {flag});")
-                body.append("      }")
+                single = [f"      for (int d = 0; d < {nd_t}; ++d) {{",
+                          f"        const i64 crow = (i64)jc * {nd_t} + d;",
+                          "        const int Lk = min(NK[crow], npad);",
+                          "        lcm_row_read(RG + crow * npad, RV + crow * npad, RM + crow * npad, "
+                          f"NK[crow] > npad ? 0 : Lk, Rn, vals[d], mus[d], {{flag}});",
+                          "      }"]
+                if uniform and nd_t >= 2:
+                    # a warp reading one candidate row reads the choices'
+                    # child rows in pairs, their searches interleaved
+                    body.append("      if (warp_row) {")
+                    for d0 in range(0, nd_t - 1, 2):
+                        body.append("        {")
+                        body.append("          const double* xs[2]; const double* fs[2]; const double* ds[2]; int Ls[2];")
+                        for k in range(2):
+                            body.append(f"          {{ const i64 crow = (i64)jc * {nd_t} + {d0 + k}; const int Lk = min(NK[crow], npad);")
+                            body.append(f"            xs[{k}] = RG + crow * npad; fs[{k}] = RV + crow * npad; ds[{k}] = RM + crow * npad;")
+                            body.append(f"            Ls[{k}] = NK[crow] > npad ? 0 : Lk; }}")
+                        body.append("          double pv[2], pm[2];")
+                        body.append("          lcm_row_read_warpk<2>(xs, fs, ds, Ls, Rn, pv, pm);")
+                        body.append(f"          vals[{d0}] = pv[0]; mus[{d0}] = pm[0]; vals[{d0 + 1}] = pv[1]; mus[{d0 + 1}] = pm[1];")
+                        body.append("        }")
+                    if nd_t % 2:
+                        body.append(f"        {{ const i64 crow = (i64)jc * {nd_t} + {nd_t - 1}; const int Lk = min(NK[crow], npad);")
+                        body.append("          lcm_row_read(RG + crow * npad, RV + crow * npad, RM + crow * npad, "
+                                    f"NK[crow] > npad ? 0 : Lk, Rn, vals[{nd_t - 1}], mus[{nd_t - 1}], true); }}")
+                    body.append("      } else {")
+                    body += ["  " + x.replace("{flag}", "false") for x in single]
+                    body.append("      }")
+                else:
+                    body += [x.replace("{flag}", flag) for x in single]
                 if tg.taste_shocks:
                     body.append("      double vmax = -LCM_INF;")
                     body.append(f"      for (int d = 0; d < {nd_t}; ++d) vmax = vals[d] > vmax ? vals[d] : vmax;")
