@@ -28,6 +28,7 @@ import numpy as np
 
 from pylcm_b200.codegen import LaunchConfig, RegimeKernels
 from pylcm_b200.exceptions import ModelInitializationError
+from pylcm_b200.runtime import bundle
 from pylcm_b200.egm import is_egm
 from pylcm_b200.spec import ParamResolver, RegimeSpec, TracedRegime, trace_regime
 
@@ -69,17 +70,17 @@ class _Records:
         arr = recs if isinstance(recs, np.ndarray) and recs.ndim == 2 else np.stack(recs)
         if arr.dtype != np.int64:
             arr = arr.astype(np.int64)
-        tiles = list(tiles_per_item)
-        self.launches.append(Launch(kind, rk, kernel, 0, 0, arr.shape[0], int(sum(tiles)), block, smem, period))
+        tiles = np.asarray(tiles_per_item, dtype=np.int64)
+        self.launches.append(Launch(kind, rk, kernel, 0, 0, arr.shape[0], int(tiles.sum()), block, smem, period))
         self.host.append((arr, tiles))
         self.shared.append(-1)
 
     def add_same_records(self, kind, rk, kernel, tiles_per_item, block, smem, period) -> None:
         """A launch over the previous launch's item records, own tiling."""
         src = len(self.launches) - 1
-        tiles = list(tiles_per_item)
+        tiles = np.asarray(tiles_per_item, dtype=np.int64)
         last = self.launches[src]
-        self.launches.append(Launch(kind, rk, kernel, 0, 0, last.n_items, int(sum(tiles)), block, smem, period))
+        self.launches.append(Launch(kind, rk, kernel, 0, 0, last.n_items, int(tiles.sum()), block, smem, period))
         self.host.append((self.host[src][0], tiles))
         self.shared.append(src)
 
@@ -445,6 +446,7 @@ class SolvePlan:
             self.items, self.prefix = b.tensors(torch, dev)
         self.graph = None
         self._prepared = None
+        self._bundled = None
         # grid-search records of endogenous-grid regimes (simulation only)
         self.sim_launches: list[Launch] = []
         self._sim_prepared = None
@@ -1008,7 +1010,9 @@ class SolvePlan:
             stream = self.torch.cuda.current_stream(self.dev).cuda_stream
         if self._prepared is None:
             self._prepared = self._prepare()
-        for launch in self._prepared:
+        if self._bundled is None:
+            self._bundled = bundle(self._prepared)
+        for launch in self._bundled:
             launch(stream)
 
     def run_collecting_carries(self) -> dict:
@@ -1044,6 +1048,20 @@ class SolvePlan:
         if cur is not None:
             snap(cur)
         return dict(sorted(out.items()))
+
+    def period_input_ops(self, period: int) -> list:
+        """The expectation and action-table launches of one period (the
+        simulation reads EV and the action table of that period), then the
+        simulation-only launches of that period, as per-launch callables."""
+        if self._prepared is None:
+            self._prepared = self._prepare()
+        ops = [launch for l, launch in zip(self.launches, self._prepared)
+               if l.period == period and l.kind in ("expect", "atab")]
+        if self.sim_launches:
+            if self._sim_prepared is None:
+                self._sim_prepared = self._prepare(self.sim_launches, self.sim_items, self.sim_prefix)
+            ops += [launch for l, launch in zip(self.sim_launches, self._sim_prepared) if l.period == period]
+        return ops
 
     def run_period_inputs(self, period: int, stream: int) -> None:
         """Re-issue the expectation and action-table launches of one period
@@ -1141,6 +1159,7 @@ class BatchPlan:
              for pl, sl in self._by_plan]
         )
         self._prepared = None
+        self._bundled = None
         self._inputs = None
 
     def _merge(self, sources):
@@ -1159,7 +1178,7 @@ class BatchPlan:
                     seq.setdefault(key_of(l), []).append((pl, l, h, gk))
                 cache[tag] = seq
             n_pl = pl.n
-            sub = None if list(sl) == list(range(n_pl)) else list(sl)
+            sub = None if list(sl) == list(range(n_pl)) else np.asarray(sl, dtype=np.int64)
             for k, lst in seq.items():
                 by_key.setdefault(k, []).append((lst, sl, sub))
         b = _Records()
@@ -1179,7 +1198,7 @@ class BatchPlan:
                     arr, tiles = h
                     if sub is not None:
                         arr = arr[sub]
-                        tiles = [tiles[i] for i in sub]
+                        tiles = tiles[sub]
                     g = groups.get(gk)
                     if g is None:
                         groups[gk] = [(l, arr, tiles)]
@@ -1187,9 +1206,12 @@ class BatchPlan:
                         g.append((l, arr, tiles))
                 for gk, members in groups.items():
                     l0 = members[0][0]
-                    recs = members[0][1] if len(members) == 1 else np.concatenate([a for _, a, _ in members])
-                    tiles = [t for _, _, ts in members for t in ts]
-                    smem = max(l.smem for l, _, _ in members)  # FUES: the longest candidate row
+                    if len(members) == 1:
+                        recs, tiles, smem = members[0][1], members[0][2], l0.smem
+                    else:
+                        recs = np.concatenate([a for _, a, _ in members])
+                        tiles = np.concatenate([ts for _, _, ts in members])
+                        smem = max(l.smem for l, _, _ in members)  # FUES: the longest candidate row
                     b.add(l0.kind, l0.module, l0.kernel, recs, tiles, l0.block, smem, k)
         items, prefix = b.tensors(self.torch, self.dev)
         return b.launches, items, prefix
@@ -1221,7 +1243,9 @@ class BatchPlan:
             stream = self.torch.cuda.current_stream(self.dev).cuda_stream
         if self._prepared is None:
             self._prepared = self._prepare(self.launches, self.items, self.prefix)
-        for launch in self._prepared:
+        if self._bundled is None:
+            self._bundled = bundle(self._prepared)
+        for launch in self._bundled:
             launch(stream)
 
     @property
@@ -1247,12 +1271,14 @@ class BatchPlan:
         launches, items, prefix = self._merge(sources)
         self._inputs = (launches, items, prefix, self._prepare(launches, items, prefix))
 
-    def run_period_inputs(self, period: int, stream: int) -> None:
+    def period_input_ops(self, period: int) -> list:
         self.ensure_sim_records()
         launches, _, _, prepared = self._inputs
-        for l, launch in zip(launches, prepared):
-            if l.period == period:
-                launch(stream)
+        return [launch for l, launch in zip(launches, prepared) if l.period == period]
+
+    def run_period_inputs(self, period: int, stream: int) -> None:
+        for launch in bundle(self.period_input_ops(period)):
+            launch(stream)
 
     def instance(self, idx: int):
         pl, slot = self.slots[idx]
