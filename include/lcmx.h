@@ -72,6 +72,17 @@ typedef struct {
   int smem_bytes;
 } lcmx_launch_args;
 
+/* One entry of lcmx_launch_list: a generated kernel of `module` over its
+ * item records; `seed` is passed only when `with_seed` is non-zero (the
+ * simulation kernels' launch seed). */
+typedef struct {
+  lcmx_module* module;
+  const char* kernel;
+  lcmx_launch_args args;
+  unsigned long long seed;
+  int with_seed;
+} lcmx_launch_rec;
+
 /* Create / destroy a context bound to CUDA device `device` (primary context). */
 int lcmx_ctx_create(int device, lcmx_ctx** out);
 int lcmx_ctx_destroy(lcmx_ctx* ctx);
@@ -116,6 +127,12 @@ int lcmx_simulate(lcmx_module* mod, const char* kernel, const lcmx_launch_args* 
 /* Kernel (c), part 1: DC-EGM Euler inversion and candidate generation. */
 int lcmx_egm_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args,
                   void* stream);
+/* `n` item launches (any of the four above) issued in order on `stream`: the
+ * per-period launch sequence of a solve or simulation plan in one call, in
+ * place of the reference's per-(period, regime) dispatch of compiled XLA
+ * programs (src/_lcm/solution/backward_induction.py:174-183).  Stops at the
+ * first failing launch and returns its status. */
+int lcmx_launch_list(const lcmx_launch_rec* recs, int n, void* stream);
 
 /* Kernel (c), part 2: FUES upper envelope of `n_rows` candidate rows of
  * length n_in (row-major; any order within a row, NaN entries are absent

@@ -17,9 +17,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <tuple>
 #include <unordered_map>
 #include <vector>
 
@@ -83,6 +85,9 @@ struct lcmx_module {
   std::string key;
   std::mutex mu;
   std::unordered_map<std::string, CUfunction> funcs;
+  // resident CTAs per SM of (kernel, block, dynamic shared bytes), with the
+  // shared-memory attributes already set: two driver queries per launch saved
+  std::map<std::tuple<CUfunction, int, int>, int> geometry;
   int refs = 1;
 };
 
@@ -338,17 +343,25 @@ static int launch_items(lcmx_module* mod, const char* kernel, const lcmx_launch_
   CUfunction f;
   int rc = get_func(mod, kernel, &f);
   if (rc) return rc;
+  int per_sm = 0;
   {
-    CUresult r = opt_in_smem(f, a->smem_bytes);
-    if (r != CUDA_SUCCESS) return set_err(mod->ctx, LCMX_ERR_LAUNCH, "smem attribute: " + cu_msg(r));
+    const auto key = std::make_tuple(f, a->block, a->smem_bytes);
+    std::unique_lock<std::mutex> g(mod->mu);
+    auto it = mod->geometry.find(key);
+    if (it != mod->geometry.end()) {
+      per_sm = it->second;
+    } else {
+      g.unlock();
+      CUresult r = opt_in_smem(f, a->smem_bytes);
+      if (r != CUDA_SUCCESS) return set_err(mod->ctx, LCMX_ERR_LAUNCH, "smem attribute: " + cu_msg(r));
+      g_drv.OccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, a->block, (size_t)a->smem_bytes);
+      if (per_sm < 1) per_sm = 1;
+      g.lock();
+      mod->geometry[key] = per_sm;
+    }
   }
   int grid = a->grid;
-  if (grid <= 0) {
-    int per_sm = 0;
-    g_drv.OccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, a->block, (size_t)a->smem_bytes);
-    if (per_sm < 1) per_sm = 1;
-    grid = mod->ctx->sm_count * per_sm;
-  }
+  if (grid <= 0) grid = mod->ctx->sm_count * per_sm;
   if (grid > a->n_tiles) grid = a->n_tiles;
   const void* items = a->items;
   const int* prefix = a->tile_prefix;
@@ -391,6 +404,20 @@ extern "C" int lcmx_simulate(lcmx_module* mod, const char* kernel, const lcmx_la
 
 extern "C" int lcmx_egm_step(lcmx_module* mod, const char* kernel, const lcmx_launch_args* args, void* stream) {
   return launch_items(mod, kernel, args, stream, nullptr);
+}
+
+// A list of item launches of generated kernels, issued in order on one
+// stream: the per-launch host cost of a plan's step (hundreds of small
+// launches) without a foreign-function call per launch.
+extern "C" int lcmx_launch_list(const lcmx_launch_rec* recs, int n, void* stream) {
+  if (n < 0 || (n > 0 && !recs)) return set_err(nullptr, LCMX_ERR_ARGS, "lcmx_launch_list: bad args");
+  for (int i = 0; i < n; ++i) {
+    const lcmx_launch_rec& r = recs[i];
+    if (!r.module || !r.kernel) return set_err(nullptr, LCMX_ERR_ARGS, "lcmx_launch_list: record without a kernel");
+    const int rc = launch_items(r.module, r.kernel, &r.args, stream, r.with_seed ? &r.seed : nullptr);
+    if (rc) return rc;
+  }
+  return LCMX_OK;
 }
 
 // ------------------------------------------------------- non-finite count

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes
 import threading
+from collections.abc import Callable
 from pathlib import Path
 
 from pylcm_b200.exceptions import KernelError
@@ -37,6 +38,7 @@ EXPORTED = (
     "lcmx_rfc_scan",
     "lcmx_mss_scan",
     "lcmx_envelope_step",
+    "lcmx_launch_list",
 )
 
 
@@ -49,6 +51,18 @@ class LaunchArgs(ctypes.Structure):
         ("grid", ctypes.c_int),
         ("block", ctypes.c_int),
         ("smem_bytes", ctypes.c_int),
+    ]
+
+
+class LaunchRec(ctypes.Structure):
+    """One entry of lcmx_launch_list (include/lcmx.h)."""
+
+    _fields_ = [
+        ("module", ctypes.c_void_p),
+        ("kernel", ctypes.c_char_p),
+        ("args", LaunchArgs),
+        ("seed", ctypes.c_ulonglong),
+        ("with_seed", ctypes.c_int),
     ]
 
 
@@ -98,6 +112,7 @@ def load_library() -> ctypes.CDLL:
             "lcmx_rfc_scan": ([vp, vp, vp, vp, vp, ip, ip, ip, ctypes.c_double, vp, vp, vp, ip, vp, vp], ip),
             "lcmx_mss_scan": ([vp, vp, vp, vp, ip, ip, vp, vp, vp, ip, vp, vp], ip),
             "lcmx_envelope_step": ([vp, ip, vp, vp, ip, ip, ip, vp], ip),
+            "lcmx_launch_list": ([ctypes.POINTER(LaunchRec), ip, vp], ip),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
@@ -199,29 +214,15 @@ class Module:
         self.h = h
         self.key = key
 
-    def prepared(self, kind: str, kernel: str, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid=0):
-        """A launch with its ctypes arguments built once (cheap to replay)."""
-        fn = {
-            "bellman": self.ctx.lib.lcmx_bellman_step,
-            "atab": self.ctx.lib.lcmx_bellman_step,
-            "expect": self.ctx.lib.lcmx_expectation,
-            "expect_tc": self.ctx.lib.lcmx_expectation,
-            "stats": self.ctx.lib.lcmx_expectation,
-            "egm": self.ctx.lib.lcmx_egm_step,
-        }[kind]
-        args = LaunchArgs(items_ptr, prefix_ptr, n_items, n_tiles, grid, block, smem)
-        name = kernel.encode()
-        h = self.h
-        ref = ctypes.byref(args)
-        ctx = self.ctx
-
-        def launch(stream):
-            rc = fn(h, name, ref, stream)
-            if rc:
-                ctx.check(rc)
-
-        launch.keepalive = (args, name)
-        return launch
+    def prepared(self, kind: str, kernel: str, items_ptr, prefix_ptr, n_items, n_tiles, block, smem, grid=0,
+                 seed=None) -> "PreparedLaunch":
+        """One item launch of a generated kernel, callable with a stream;
+        consecutive ones run as a single lcmx_launch_list call through
+        `bundle`."""
+        if kind not in _ITEM_KINDS:
+            raise KeyError(kind)
+        return PreparedLaunch(self.ctx, (self.h.value, kernel.encode(), items_ptr, prefix_ptr, n_items, n_tiles, grid,
+                                         block, smem, seed))
 
     def status(self, reset: bool = True) -> int:
         """The module's device status word (0: every bounded wait of its
@@ -270,3 +271,69 @@ def get_context(device: int = 0) -> Context:
             c = Context(device)
             _contexts[device] = c
         return c
+
+
+_ITEM_KINDS = frozenset(("bellman", "atab", "expect", "expect_tc", "stats", "egm", "sim"))
+
+
+class PreparedLaunch:
+    """One lcmx_launch_list entry: (module handle, kernel name, items,
+    tile prefix, n_items, n_tiles, grid, block, shared bytes, seed or None)."""
+
+    __slots__ = ("ctx", "rec", "_call")
+
+    def __init__(self, ctx, rec) -> None:
+        self.ctx = ctx
+        self.rec = rec
+        self._call = None
+
+    def __call__(self, stream) -> None:
+        if self._call is None:
+            self._call = launch_list(self.ctx, [self.rec])
+        self._call(stream)
+
+
+def launch_list(ctx, recs) -> Callable:
+    """A callable issuing the item launches `recs` (PreparedLaunch.rec
+    tuples) in order on a stream with one lcmx_launch_list call."""
+    n = len(recs)
+    arr = (LaunchRec * n)()
+    for i, (h, name, ib, pb, ni, nt, grid, block, smem, seed) in enumerate(recs):
+        r = arr[i]
+        r.module = h
+        r.kernel = name
+        a = r.args
+        a.items, a.tile_prefix, a.n_items, a.n_tiles, a.grid, a.block, a.smem_bytes = ib, pb, ni, nt, grid, block, smem
+        if seed is not None:
+            r.seed = seed
+            r.with_seed = 1
+    names = [x[1] for x in recs]
+    fn = ctx.lib.lcmx_launch_list
+
+    def launch(stream):
+        rc = fn(arr, n, stream)
+        if rc:
+            ctx.check(rc)
+
+    launch.keepalive = (arr, names)
+    return launch
+
+
+def bundle(ops) -> list:
+    """Callables of `ops` (per-launch callables) with every run of
+    consecutive PreparedLaunch entries merged into one lcmx_launch_list call."""
+    out: list = []
+    pend: list = []
+    ctx = None
+    for op in ops:
+        if isinstance(op, PreparedLaunch):
+            pend.append(op.rec)
+            ctx = op.ctx
+            continue
+        if pend:
+            out.append(launch_list(ctx, pend))
+            pend = []
+        out.append(op)
+    if pend:
+        out.append(launch_list(ctx, pend))
+    return out

@@ -30,6 +30,7 @@ import numpy as np
 
 from pylcm_b200.exceptions import InvalidInitialConditionsError, InvalidParamsError
 from pylcm_b200.grids import DiscreteGrid
+from pylcm_b200.runtime import bundle
 
 
 class SimulationResult:
@@ -198,6 +199,7 @@ class SimPlan:
         import torch
 
         self.torch = torch
+        self._bundled = None
         self.plan = solve_plan
         dev = solve_plan.dev
         if rng not in ("philox", "jax"):
@@ -372,13 +374,21 @@ class SimPlan:
         torch = self.torch
         if stream is None:
             stream = torch.cuda.current_stream(self.plan.dev).cuda_stream
-        ib, pb = self.items.data_ptr(), self.prefix.data_ptr()
-        done_inputs = set()
-        for period, rk, off, poff, n_items, tiles in self.launches:
-            if period not in done_inputs:
-                self.plan.run_period_inputs(period, stream)
-                done_inputs.add(period)
-            rk.module.simulate(rk.sim_name(), ib + 8 * off, pb + 4 * poff, n_items, tiles, 256, 0, 0, stream)
+        if self._bundled is None:
+            # each period's inputs (expectation and action tables), then its
+            # simulation launches: one launch list per run of item launches
+            ib, pb = self.items.data_ptr(), self.prefix.data_ptr()
+            ops: list = []
+            done_inputs = set()
+            for period, rk, off, poff, n_items, tiles in self.launches:
+                if period not in done_inputs:
+                    ops += self.plan.period_input_ops(period)
+                    done_inputs.add(period)
+                ops.append(rk.module.prepared("sim", rk.sim_name(), ib + 8 * off, pb + 4 * poff, n_items, tiles, 256, 0,
+                                              seed=0))
+            self._bundled = bundle(ops)
+        for launch in self._bundled:
+            launch(stream)
 
     @property
     def gpu_launches(self) -> int:

@@ -47,3 +47,31 @@ def test_compile_rejects_null_arguments_without_gpu():
     out = ctypes.c_void_p()
     rc = lib.lcmx_module_compile(None, b"", b"k", None, ctypes.byref(out))
     assert rc == 1  # LCMX_ERR_ARGS
+
+
+def test_launch_record_layout_matches_the_header(tmp_path):
+    """lcmx_launch_rec / lcmx_launch_args as the C compiler lays them out and
+    as the ctypes mirrors in runtime.py do."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    from pylcm_b200.runtime import LaunchArgs, LaunchRec
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "lcmx.h"\n'
+        "int main(void) { printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(lcmx_launch_rec),"
+        " offsetof(lcmx_launch_rec, kernel), offsetof(lcmx_launch_rec, args), offsetof(lcmx_launch_rec, seed),"
+        " offsetof(lcmx_launch_rec, with_seed), sizeof(lcmx_launch_args)); return 0; }\n"
+    )
+    exe = tmp_path / "layout"
+    subprocess.run([cc, f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    want = [ctypes.sizeof(LaunchRec), LaunchRec.kernel.offset, LaunchRec.args.offset, LaunchRec.seed.offset,
+            LaunchRec.with_seed.offset, ctypes.sizeof(LaunchArgs)]
+    assert got == want
