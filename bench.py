@@ -1083,8 +1083,8 @@ def main() -> None:
     ap.add_argument("--cpu-cores", type=int, default=0, help="host processes of the CPU baseline (0: all)")
     ap.add_argument("--serve-requests", type=int, default=4096)
     ap.add_argument("--agents", type=int, default=10_000)
-    ap.add_argument("--serve-batch", type=int, default=32)
-    ap.add_argument("--serve-streams", type=int, default=2)
+    ap.add_argument("--serve-batch", type=int, default=64)
+    ap.add_argument("--serve-streams", type=int, default=4)
     ap.add_argument("--plain-requests", type=int, default=32)
     ap.add_argument("--no-extra", action="store_true", help="skip the serving / DC-EGM / two-state sections")
     ap.add_argument("--dcegm-batch", type=int, default=32)

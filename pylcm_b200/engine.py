@@ -1053,15 +1053,22 @@ class SolvePlan:
         """The expectation and action-table launches of one period (the
         simulation reads EV and the action table of that period), then the
         simulation-only launches of that period, as per-launch callables."""
-        if self._prepared is None:
-            self._prepared = self._prepare()
-        ops = [launch for l, launch in zip(self.launches, self._prepared)
-               if l.period == period and l.kind in ("expect", "atab")]
-        if self.sim_launches:
-            if self._sim_prepared is None:
-                self._sim_prepared = self._prepare(self.sim_launches, self.sim_items, self.sim_prefix)
-            ops += [launch for l, launch in zip(self.sim_launches, self._sim_prepared) if l.period == period]
-        return ops
+        self.ensure_sim_records()
+        by_period = self.__dict__.get("_inputs_by_period")
+        if by_period is None:
+            if self._prepared is None:
+                self._prepared = self._prepare()
+            by_period = {}
+            for l, launch in zip(self.launches, self._prepared):
+                if l.kind in ("expect", "atab"):
+                    by_period.setdefault(l.period, []).append(launch)
+            if self.sim_launches:
+                if self._sim_prepared is None:
+                    self._sim_prepared = self._prepare(self.sim_launches, self.sim_items, self.sim_prefix)
+                for l, launch in zip(self.sim_launches, self._sim_prepared):
+                    by_period.setdefault(l.period, []).append(launch)
+            self._inputs_by_period = by_period
+        return list(by_period.get(period, []))
 
     def run_period_inputs(self, period: int, stream: int) -> None:
         """Re-issue the expectation and action-table launches of one period
@@ -1273,8 +1280,14 @@ class BatchPlan:
 
     def period_input_ops(self, period: int) -> list:
         self.ensure_sim_records()
-        launches, _, _, prepared = self._inputs
-        return [launch for l, launch in zip(launches, prepared) if l.period == period]
+        by_period = self.__dict__.get("_inputs_by_period")
+        if by_period is None:
+            launches, _, _, prepared = self._inputs
+            by_period = {}
+            for l, launch in zip(launches, prepared):
+                by_period.setdefault(l.period, []).append(launch)
+            self._inputs_by_period = by_period
+        return by_period.get(period, [])
 
     def run_period_inputs(self, period: int, stream: int) -> None:
         for launch in bundle(self.period_input_ops(period)):
