@@ -49,6 +49,7 @@ class Launch:
     block: int
     smem: int
     period: int
+    grid: int = 0  # CTAs of the launch (0: SM count x resident CTAs per SM)
 
 
 class _Records:
@@ -679,6 +680,11 @@ class SolvePlan:
                 ncols = int(X[k][0, 7])
                 b.add("expect_tc", rk, rk.expect_tc_name(t), X[k], [math.ceil(ncols / 128)] * len(tiles), 128,
                       sh["smem"], period)
+                # the driver's occupancy query answers one CTA per SM for this
+                # kernel; registers and shared memory allow three, and the
+                # padded shared memory keeps every CTA's tensor-memory
+                # allocation within the SM's 512 columns
+                b.launches[-1].grid = SM_COUNT * min(3, sh["max_ctas"])
             else:
                 b.add("expect", rk, rk.expect_name(t), X[k], tiles, 256, 0, period)
             st = g["stats"].get(id(t))
@@ -999,7 +1005,8 @@ class SolvePlan:
                 continue
             out.append(
                 l.module.module.prepared(
-                    l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem
+                    l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem,
+                    grid=l.grid,
                 )
             )
         return out
@@ -1220,6 +1227,7 @@ class BatchPlan:
                         tiles = np.concatenate([ts for _, _, ts in members])
                         smem = max(l.smem for l, _, _ in members)  # FUES: the longest candidate row
                     b.add(l0.kind, l0.module, l0.kernel, recs, tiles, l0.block, smem, k)
+                    b.launches[-1].grid = l0.grid
         items, prefix = b.tensors(self.torch, self.dev)
         return b.launches, items, prefix
 
@@ -1240,7 +1248,8 @@ class BatchPlan:
                 continue
             out.append(
                 l.module.module.prepared(
-                    l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem
+                    l.kind, l.kernel, ib + 8 * l.item_off, pb + 4 * l.prefix_off, l.n_items, l.n_tiles, l.block, l.smem,
+                    grid=l.grid,
                 )
             )
         return out
