@@ -455,6 +455,9 @@ class LaunchConfig:
     # the full search on the human-capital model: off unless asked for)
     prune_multi: bool = False
     group: int = 16  # actions per skipped group (raised to `lanes` if smaller)
+    # single-precision search: read a target with two continuous axes from
+    # per-tile collapsed rows where eligible (see RegimeKernels._collapse_info)
+    collapse: bool = True
 
     @property
     def states_per_tile(self) -> int:
@@ -662,6 +665,58 @@ class RegimeKernels:
                 x0 = ir.substitute(x, cv, 0.0)
                 out[(ti, pos)] = (x0, g, cv)
         return out
+
+    COLLAPSE_MAX_OUTER = 8  # largest action grid read in the collapsed rows
+
+    def _collapse_info(self, ti: int, t) -> dict | None:
+        """Collapsed rows for target `t` in the single-precision search.
+
+        Eligible when `t` has two continuous axes and no deterministic
+        discrete ones, its expectation row is keyed by discrete states only,
+        and one axis (B) has an affine coordinate in one continuous action
+        `ob` of at most COLLAPSE_MAX_OUTER points whose state part does not
+        read the *line state* -- the current regime's continuous state named
+        like the other axis (A).  The kernel then walks the states with the
+        line state fastest, so that a tile covers at most two lines (all
+        other states fixed); per tile it interpolates axis B once per (line,
+        value of `ob`) into rows over axis A in shared memory, and each
+        (state, action) pair reads its row with a 1-D interpolation instead
+        of the bilinear read.  The candidates are re-evaluated in double
+        precision as everywhere in this search."""
+        spec = self.spec
+        if self.precision != "fp32" or not self.cfg.collapse or self._groups or spec.terminal:
+            return None
+        if t.scalar or t.unreachable or len(t.cont_pos) != 2 or t.det_pos:
+            return None
+        if any(kind != "state" for kind, _, _ in t.key_vars):
+            return None
+        cont_states = [a.name for a in spec.states if a.kind == "continuous"]
+        names = [a.name for a in spec.actions]
+        for cb, posB in enumerate(t.cont_pos):
+            if (ti, posB) not in self._affine:
+                continue
+            ca, posA = 1 - cb, t.cont_pos[1 - cb]
+            line = t.spec.states[posA].name
+            if line not in cont_states:
+                continue
+            x0, g, cv = self._affine[(ti, posB)]
+            ob = cv.args[1]
+            kob = names.index(ob)
+            if spec.actions[kob].size > self.COLLAPSE_MAX_OUTER:
+                continue
+            if any(a.kind != "continuous" for a in spec.actions[kob:]):
+                continue
+            deps: set = set()
+            for e in (x0, g):
+                if isinstance(e, ir.Expr):
+                    deps |= set(e.deps())
+            if any(k not in ("state", "param", "period", "age") for k, _ in deps) or ("state", line) in deps:
+                continue
+            namax = (t.spec.states[posA].size + 31) // 32 * 32
+            return {"ti": ti, "ca": ca, "cb": cb, "posA": posA, "posB": posB, "line": line,
+                    "kline": [a.name for a in spec.states].index(line), "ob": ob, "kob": kob,
+                    "nob": spec.actions[kob].size, "x0": x0, "g": g, "namax": namax}
+        return None
 
     # group skipping: tiles of the block statistics of a target with two
     # continuous axes (axis 1 x axis 2); one continuous axis uses 16-column blocks
@@ -916,6 +971,16 @@ class RegimeKernels:
         NDS = max(len(dstates), 1)
         nP, nD, nS, nSD = (max(len(x), 1) for x in (bP, bD, bS, bSD))
         pv = lambda: {id(ir.var("period", "period", "i")): "period", id(ir.var("age", "age", "f")): "age"}  # noqa: E731
+        # targets the single-precision search reads from collapsed rows (one
+        # line state for the whole kernel)
+        cinfo: dict = {}
+        if unswitch and fp32 and not taste:
+            for ti_, t_ in enumerate(self.targets):
+                c_ = self._collapse_info(ti_, t_)
+                if c_ is not None and (not cinfo or c_["kline"] == next(iter(cinfo.values()))["kline"]):
+                    cinfo[ti_] = c_
+        rows_off = NF * CH * 4 + NI * CH * 4  # the collapsed rows follow the action table
+        rows_bytes = max((2 * c["nob"] * c["namax"] * 4 for c in cinfo.values()), default=0)
 
         L: list[str] = []
         ap = L.append
@@ -966,6 +1031,13 @@ class RegimeKernels:
             f"  __device__ __forceinline__ T F(int f) const {{ return (T)tabf[f * {CH} + j]; }}\n"
             f"  __device__ __forceinline__ int I(int f) const {{ return tabi[f * {CH} + j]; }} }};"
         )
+        if cinfo:
+            ap(
+                f"template <typename T> struct AFCol_{self.tag} {{ const {TT}* tabf; const int* tabi; int j; "
+                f"const float* R;\n"
+                f"  __device__ __forceinline__ T F(int f) const {{ return (T)tabf[f * {CH} + j]; }}\n"
+                f"  __device__ __forceinline__ int I(int f) const {{ return tabi[f * {CH} + j]; }} }};"
+            )
         ap(
             f"struct AFLoc_{self.tag} {{ double v[{NF}]; int vi[{NI}];\n"
             f"  __device__ __forceinline__ double F(int f) const {{ return v[f]; }}\n"
@@ -977,7 +1049,7 @@ class RegimeKernels:
         # the selected target (TSEL < 0: all targets by probability / id)
         proc_names = [a.name for a in spec.states if a.kind == "process"]
 
-        def sa_body(T: str, E: str, tsel: int, sim: bool = False) -> list[str]:
+        def sa_body(T: str, E: str, tsel: int, sim: bool = False, coll: dict | None = None) -> list[str]:
             prov = pv()
             for i, n in enumerate(bP):
                 prov[id(n)] = _cast(f"PVd[{i}]", n.dtype, T)
@@ -1087,6 +1159,8 @@ class RegimeKernels:
                     for pos in t.cont_pos:
                         cblk = f"{cblk} * C.n{ti}_{pos}"
                     for ci, pos in enumerate(t.cont_pos):
+                        if coll is not None and ti == coll["ti"] and ci == coll["cb"]:
+                            continue  # axis B comes interpolated in the collapsed row AF.R
                         ax = t.spec.states[pos]
                         x = xn[(ti, pos)]
                         kind = ax.grid.kind
@@ -1105,6 +1179,9 @@ class RegimeKernels:
                             cc = f"lcm_coord_irreg<{T}>(({T})({x}), C.p{ti}_{ci}, C.n{ti}_{pos})"
                         inner.append(f"{T} c{ci} = {cc};")
                     rows = [] if multi else [("row", off)] + ([("rowh", off_hi)] if off_hi is not None else [])
+                    if coll is not None and ti == coll["ti"]:
+                        rows = []
+                        inner.append(f"{T} ev = lcm_interp1s<{T}>(AF.R, C.n{ti}_{coll['posA']}, c{coll['ca']});")
                     if multi:
                         inner.append(f"{T} ev = ({T})0;")
                         inner += self._sim_extrapolated_expectation(ti, t, T, E, None, proc_names, dn, mk)
@@ -1151,6 +1228,17 @@ class RegimeKernels:
                 f"const double* SDV, const AFN& AF, const int* SI, {di_params}int period, double age, T& Q) {{"
             )
             for s_ in sa_body("T", "E", tsel):
+                ap("  " + s_)
+            ap("  return true;\n}")
+        for ti_, c_ in cinfo.items():
+            # target ti_ read from the collapsed rows (AFCol's R)
+            ap(
+                f"template <typename T, typename E, typename AFN>\n"
+                f"__device__ __forceinline__ bool lcm_sc{ti_ + 1}_{self.tag}(const Ctx_{self.tag}<T, E>& C, "
+                f"const double* __restrict__ PV, const double* PVd, const double* DV, const double* SV, "
+                f"const double* SDV, const AFN& AF, const int* SI, {di_params}int period, double age, T& Q) {{"
+            )
+            for s_ in sa_body("T", "E", ti_, coll=c_):
                 ap("  " + s_)
             ap("  return true;\n}")
 
@@ -1237,13 +1325,29 @@ class RegimeKernels:
         if not bP:
             ap("    PVd[0] = 0.0;")
         ap(f"    int SI[{SB}][{NDS}]; double SV[{SB}][{nS}]; bool act[{SB}]; int sidx[{SB}];")
+        kline = next(iter(cinfo.values()))["kline"] if cinfo else -1
+        if cinfo:
+            # states walked with the line state fastest (a tile then covers at
+            # most two lines); sidx is the state's index in the declared order
+            ap(f"    int lslot[{SB}];")
+            ap(f"    const int nLine = lcm_wi(it, {self.W_SSIZE + kline});")
+            ap(f"    const int line0 = ((tile - tile_prefix[item]) * {SPT}) / nLine;")
         ap(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
         ap(f"      const int s = sbase + kb * {SPB};")
         ap("      act[kb] = s < n_states; sidx[kb] = s;")
         ap("      int srem = act[kb] ? s : 0;")
-        for k in range(len(spec.states) - 1, -1, -1):
+        order = list(range(len(spec.states) - 1, -1, -1))
+        if cinfo:
+            order = [kline] + [k for k in order if k != kline]
+        for k in order:
             ax = spec.states[k]
             ap(f"      const int si_{ax.name} = srem % lcm_wi(it, {self.W_SSIZE + k}); srem /= lcm_wi(it, {self.W_SSIZE + k});")
+        if cinfo:
+            phys = "0"
+            for k, ax in enumerate(spec.states):
+                phys = f"({phys}) * lcm_wi(it, {self.W_SSIZE + k}) + si_{ax.name}"
+            ap(f"      if (act[kb]) sidx[kb] = {phys};")
+            ap("      lslot[kb] = act[kb] ? s / nLine - line0 : 0;")
         for k, ax in enumerate(spec.states):
             if ax.kind == "continuous":
                 ap(f"      const double sv_{ax.name} = lcm_wp<const double>(it, {self.W_SGRID + k})[si_{ax.name}];")
@@ -1639,6 +1743,100 @@ class RegimeKernels:
             o.append("}")
             return o
 
+        def inner_loop_collapse(ti: int, c: dict) -> list[str]:
+            """The inner loop of target ti read from collapsed rows, built per
+            tile in shared memory; the plain loop where an item's sizes do not
+            allow them (a line shorter than a tile, rows longer than
+            reserved, another size of the outer action grid)."""
+            t = self.targets[ti]
+            nob, namax, posA, posB, cb = c["nob"], c["namax"], c["posA"], c["posB"], c["cb"]
+            o = ["{"]
+            o.append(f"  const int nA = C.n{ti}_{posA}, nB = C.n{ti}_{posB};")
+            o.append(f"  if (nLine >= {SPT} && nA <= {namax} && lcm_wi(it, {self.W_ASIZE + c['kob']}) == {nob}) {{")
+            o.append(f"    float* crow = reinterpret_cast<float*>(lcm_smem + {rows_off});")
+            o.append(f"    const double* obg = lcm_wp<const double>(it, {self.W_AGRID + c['kob']});")
+            ostr = "1"
+            for k in range(c["kob"] + 1, len(spec.actions)):
+                ostr = f"{ostr} * lcm_wi(it, {self.W_ASIZE + k})"
+            o.append(f"    const int ostr = {ostr};")
+            o.append("    const int nLines = n_states / nLine;")
+            o.append("    __syncthreads();  // the previous tile's reads of the rows are done")
+            o.append(f"    for (int e = threadIdx.x; e < 2 * {nob} * nA; e += {B}) {{")
+            o.append(f"      const int w = e % nA, r = e / nA, ob = r % {nob}, line = line0 + r / {nob};")
+            o.append("      float val = lcm_lim<float>::nan();")
+            o.append("      if (line < nLines) {")
+            o.append("        int lrem = line;")
+            for k in range(len(spec.states) - 1, -1, -1):
+                ax = spec.states[k]
+                if k == kline:
+                    o.append(f"        const int si_{ax.name} = 0;")
+                else:
+                    o.append(f"        const int si_{ax.name} = lrem % lcm_wi(it, {self.W_SSIZE + k}); "
+                             f"lrem /= lcm_wi(it, {self.W_SSIZE + k});")
+            for k, ax in enumerate(spec.states):
+                if ax.kind == "continuous":
+                    o.append(f"        const double sv_{ax.name} = lcm_wp<const double>(it, {self.W_SGRID + k})[si_{ax.name}];")
+            o += ["        " + x for x in s_lines]
+            o.append(f"        double SVl[{nS}];")
+            for i, v in enumerate(s_vals):
+                o.append(f"        SVl[{i}] = (double)({v});")
+            if not bS:
+                o.append("        SVl[0] = 0.0;")
+            prov = pv()
+            for i, n in enumerate(bP):
+                prov[id(n)] = _cast(f"PVd[{i}]", n.dtype, "float")
+            for i, n in enumerate(bS):
+                prov[id(n)] = _cast(f"SVl[{i}]", n.dtype, "float")
+            for i, a in enumerate(dstates):
+                prov[id(ir.var("state", a.name, "i"))] = f"si_{a.name}"
+            e = Emitter("float", self.param_off, prov, "w")
+            x0s, gs = e.emit(c["x0"]), e.emit(c["g"])
+            o += ["        " + x for x in e.lines]
+            key = "0"
+            for kind, name, size in t.key_vars:
+                key = f"({key}) * {size} + si_{name}"
+            o.append(f"        const float cB = (((float)({x0s})) - C.a{ti}_{cb}) * C.b{ti}_{cb} + "
+                     f"(((float)({gs})) * C.b{ti}_{cb}) * (float)obg[ob];")
+            o.append("        float fB; const int lB = lcm_lower(cB, nB, fB); const float uB = cB - fB;")
+            o.append(f"        const float* blk = C.ev{ti} + (i64)({key}) * ((i64)nA * nB);")
+            if cb == 1:
+                o.append("        const float va = blk[(i64)w * nB + lB], vb = blk[(i64)w * nB + lB + 1];")
+            else:
+                o.append("        const float va = blk[(i64)lB * nA + w], vb = blk[(i64)(lB + 1) * nA + w];")
+            o.append("        val = va + uB * (vb - va);")
+            o.append("        if (!lcm_isfinite(val)) val = lcm_zs(1.0f - uB, va) + lcm_zs(uB, vb);")
+            o.append("      }")
+            o.append("      crow[e] = val;")
+            o.append("    }")
+            o.append(f"    for (int c0 = 0; c0 < n_ac; c0 += {CH}) {{")
+            o.append(f"      const int cn = min({CH}, n_ac - c0);")
+            o.append("      __syncthreads();")
+            o.append(f"      for (int j = threadIdx.x; j < cn; j += {B}) {{")
+            o.append("        const i64 a = (i64)ad * n_ac + c0 + j;")
+            for k in range(nf):
+                o.append(f"        tabf[{k} * {CH} + j] = ({TT})atf[(i64){k} * n_actions + a];")
+            for k in range(ni):
+                o.append(f"        tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
+            o.append("      }")
+            o.append("      __syncthreads();")
+            o.append(f"      for (int j = lane; j < cn; j += {LANES}) {{")
+            o.append("        const int aidx = ad * n_ac + c0 + j;")
+            o.append(f"        const int obi = ((c0 + j) / ostr) % {nob};")
+            o.append(f"        #pragma unroll\n        for (int kb = 0; kb < {SB}; ++kb) {{")
+            o.append(f"          AFCol_{self.tag}<{ST}> af{{tabf, tabi, j, crow + (lslot[kb] * {nob} + obi) * nA}};")
+            o.append(f"          {ST} q;")
+            di_args = "".join(f"DI_{a.name}, " for a in dacts)
+            o.append(f"          if (lcm_sc{ti + 1}_{self.tag}<{ST}, {ST}>(C, PV, PVd, DV, SV[kb], SDV[kb], af, SI[kb], "
+                     f"{di_args}period, age, q)) best[kb].push(q, aidx);")
+            o.append("        }")
+            o.append("      }")
+            o.append("    }")
+            o.append("  } else {")
+            o += ["    " + x for x in inner_loop(SA.format(ti + 1))]
+            o.append("  }")
+            o.append("}")
+            return o
+
         any_pruned = False
         n_gacts = 0
         if unswitch:
@@ -1654,7 +1852,10 @@ class RegimeKernels:
                 if gi is not None:
                     any_pruned = True
                     n_gacts = max(n_gacts, len(GP["acts"]))
-                body = inner_loop(SA.format(ti + 1)) if gi is None else inner_loop_groups(SA.format(ti + 1), gi)
+                if ti in cinfo:
+                    body = inner_loop_collapse(ti, cinfo[ti])
+                else:
+                    body = inner_loop(SA.format(ti + 1)) if gi is None else inner_loop_groups(SA.format(ti + 1), gi)
                 for s_ in body:
                     ap("        " + s_)
                 ap("      }")
@@ -1758,7 +1959,7 @@ class RegimeKernels:
         ap("    }")
         ap("  }")
         ap("}")
-        self.smem_bytes = NF * CH * (4 if fp32 else 8) + NI * CH * 4
+        self.smem_bytes = NF * CH * (4 if fp32 else 8) + NI * CH * 4 + rows_bytes
         self.atab_words = nf * 2 + ni
 
         # ----------------------------------------------------------------

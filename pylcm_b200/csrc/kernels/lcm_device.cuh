@@ -140,6 +140,22 @@ __device__ __forceinline__ T lcm_interp1(const S* __restrict__ row, int n, T c) 
   return lcm_zs(wl, v0) + lcm_zs(wu, v1);
 }
 
+// 1-D linear read of a float row in shared memory (the collapsed rows of the
+// single-precision search), with lcm_interp1's extrapolation and zero-safe
+// fallback.
+template <typename T>
+__device__ __forceinline__ T lcm_interp1s(const float* row, int n, T c) {
+  T lof;
+  int lo = lcm_lower(c, n, lof);
+  T wu = c - lof;
+  T wl = T(1) - wu;
+  T v0 = (T)row[lo];
+  T v1 = (T)row[lo + 1];
+  T r = wl * v0 + wu * v1;
+  if (lcm_isfinite(r)) return r;
+  return lcm_zs(wl, v0) + lcm_zs(wu, v1);
+}
+
 // 2-D bilinear read; `blk` is an (n0 x n1) row-major block.  Corner order and
 // left-to-right summation follow map_coordinates (ndimage.py:71-97).
 template <typename T, typename S>

@@ -96,3 +96,26 @@ def test_phase_split_hoists_utility_out_of_the_state_loop():
     inner = rk.src.split("__device__ __forceinline__ bool lcm_sa0_")[1].split("return true;")[0]
     assert "log(" not in inner
     assert "log(" in rk.src.split("lcm_atab_")[-1]
+
+
+def test_collapsed_rows_eligibility():
+    """The single-precision search reads a target with two continuous axes
+    from collapsed rows when one axis is affine in a small action grid and its
+    state part does not read the line state; never in double precision or
+    when switched off."""
+    import dataclasses
+
+    from pylcm_b200.engine import default_config
+
+    model, params = M.hc_model(3, 10, 4, 4, 8), M.hc_params(0, 4)
+    alive = next(s for s in model.regime_specs if s.name == "alive")
+
+    def src(precision, **kw):
+        cfg = {s.name: dataclasses.replace(default_config(s, precision, 1), **kw) for s in model.regime_specs}
+        eng = SolveEngine(model, precision, configs=cfg)
+        return eng.kernels(alive, eng.targets_at(alive, 0), params).source()
+
+    s32 = src("fp32")
+    assert "lcm_sc1_" in s32 and "lcm_interp1s" in s32 and "nLine" in s32
+    assert "lcm_sc1_" not in src("fp32", collapse=False)
+    assert "lcm_sc1_" not in src("fp64")

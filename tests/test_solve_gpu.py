@@ -22,6 +22,9 @@ CASES = {
     "retirement": (lambda: M.retirement_model(5, 100, 100), M.retirement_params),
     "stochastic": (lambda: M.stochastic_model(6, 60, 80), M.stochastic_params),
     "hc": (lambda: M.hc_model(4, 30, 6, 5, 25), lambda: M.hc_params(1, 5)),
+    # a wealth line longer than a tile (512 states): the single-precision
+    # search reads this model from collapsed rows
+    "hc_rows": (lambda: M.hc_model(4, 600, 8, 4, 60), lambda: M.hc_params(2, 4)),
     **{f"grid_{k}": (lambda k=k: M.grid_kinds_model(k), M.grid_kinds_params)
        for k in ("irreg", "log", "piece_lin", "piece_log")},
 }
@@ -219,3 +222,32 @@ def test_batch_solver_overlapped_download_equals_the_device_arrays(precision):
         for per in V1:
             for r in V1[per]:
                 assert np.array_equal(V1[per][r].cpu().numpy(), keep[i][per][r], equal_nan=True)
+
+
+def test_collapsed_rows_agree_with_the_bilinear_search():
+    """The single-precision search with and without the collapsed rows: the
+    same argmax wherever the double-precision gap exceeds the search's
+    resolution, values within 1e-6 (both are re-evaluated in FP64)."""
+    import dataclasses
+
+    import numpy as np
+
+    from pylcm_b200.engine import SolveEngine, default_config
+
+    model, params = M.hc_model(4, 600, 8, 4, 60), [M.hc_params(s, 4) for s in range(3)]
+    out = {}
+    for coll in (True, False):
+        cfg = {s.name: dataclasses.replace(default_config(s, "fp32", 3), collapse=coll) for s in model.regime_specs}
+        eng = SolveEngine(model, "fp32", configs=cfg)
+        plan = eng.plan(params)
+        plan.run()
+        out[coll] = ({r: v.cpu().numpy() for r, v in plan.V.items()}, {r: v.cpu().numpy() for r, v in plan.pol.items()})
+        srcs = [rk.src for rk in eng._kernels.values()]
+        assert any("lcm_sc" in x for x in srcs) == coll
+    (Va, Pa), (Vb, Pb) = out[True], out[False]
+    for r in Va:
+        fin = np.isfinite(Vb[r])
+        assert np.array_equal(np.isfinite(Va[r]), fin)
+        rel = np.abs(Va[r][fin] - Vb[r][fin]) / np.maximum(1.0, np.abs(Vb[r][fin]))
+        assert rel.max() <= 1e-6
+        assert (Pa[r] == Pb[r]).mean() >= 0.999
