@@ -718,6 +718,38 @@ class RegimeKernels:
                     "nob": spec.actions[kob].size, "x0": x0, "g": g, "namax": namax}
         return None
 
+    def _budget_bound(self):
+        """(action position, bound node, strict) of a constraint a <= b (or
+        b >= a, or strict) in F, where `a` is the slowest continuous action --
+        every action before it discrete, so that its index is the slowest
+        part of the continuous-action index and, its grid being ascending, the
+        feasible actions of a state form a prefix of the table -- and `b` reads
+        no action.  None if F has no such constraint."""
+        spec = self.spec
+        names = [a.name for a in spec.actions]
+        kc = next((k for k, a in enumerate(spec.actions) if a.kind == "continuous"), None)
+        if kc is None:
+            return None
+        cname = names[kc]
+        F = ir.const(self.tr.F)
+        stack = [F] if isinstance(F, ir.Expr) else []
+        while stack:
+            n = stack.pop()
+            if n.op == "and":
+                stack.extend(a for a in n.args if isinstance(a, ir.Expr))
+                continue
+            if n.op != "cmp" or n.args[0] not in ("<", "<=", ">", ">="):
+                continue
+            lhs, rhs = n.args[1], n.args[2]
+            if n.args[0] in (">", ">="):
+                lhs, rhs = rhs, lhs
+            if not (isinstance(lhs, ir.Expr) and lhs.op == "var" and tuple(lhs.args[:2]) == ("action", cname)):
+                continue
+            if isinstance(rhs, ir.Expr) and any(k == "action" for k, _ in rhs.deps()):
+                continue
+            return kc, rhs
+        return None
+
     # group skipping: tiles of the block statistics of a target with two
     # continuous axes (axis 1 x axis 2); one continuous axis uses 16-column blocks
     GROUP_TILE = (16, 2)
@@ -1808,6 +1840,34 @@ class RegimeKernels:
             o.append("      }")
             o.append("      crow[e] = val;")
             o.append("    }")
+            # the budget constraint a <= b on the slowest continuous action:
+            # a state's feasible actions are a prefix of the table; a warp
+            # stops at the longest prefix among its states (two grid points of
+            # slack for the single-precision test)
+            bb = self._budget_bound()
+            bexpr = None
+            if bb is not None:
+                kc, bnode = bb
+                if isinstance(bnode, (int, float)):
+                    bexpr = repr(float(bnode))
+                elif id(bnode) in {id(x) for x in bS}:
+                    bexpr = f"SV[kb][{[id(x) for x in bS].index(id(bnode))}]"
+                elif id(bnode) in {id(x) for x in bP}:
+                    bexpr = f"PVd[{[id(x) for x in bP].index(id(bnode))}]"
+            if bexpr is None:
+                o.append("    const int jfe = n_ac;")
+            else:
+                o.append(f"    const double* cgr = lcm_wp<const double>(it, {self.W_AGRID + kc});")
+                o.append(f"    const int ncg = lcm_wi(it, {self.W_ASIZE + kc});")
+                o.append("    int jfe = 0;")
+                o.append(f"    #pragma unroll\n    for (int kb = 0; kb < {SB}; ++kb) {{")
+                o.append("      if (!act[kb]) continue;")
+                o.append(f"      const double wv = (double)({bexpr});")
+                o.append("      int lo = 0, hi = ncg;  // grid points at or below the bound")
+                o.append("      while (lo < hi) { const int mid = (lo + hi) >> 1; if (cgr[mid] <= wv) lo = mid + 1; else hi = mid; }")
+                o.append("      jfe = max(jfe, min(lo + 2, ncg) * (n_ac / ncg));")
+                o.append("    }")
+                o.append("    jfe = __reduce_max_sync(0xffffffffu, jfe);")
             o.append(f"    for (int c0 = 0; c0 < n_ac; c0 += {CH}) {{")
             o.append(f"      const int cn = min({CH}, n_ac - c0);")
             o.append("      __syncthreads();")
@@ -1819,7 +1879,8 @@ class RegimeKernels:
                 o.append(f"        tabi[{k} * {CH} + j] = ati[(i64){k} * n_actions + a];")
             o.append("      }")
             o.append("      __syncthreads();")
-            o.append(f"      for (int j = lane; j < cn; j += {LANES}) {{")
+            o.append("      const int jend = min(cn, jfe - c0);")
+            o.append(f"      for (int j = lane; j < jend; j += {LANES}) {{")
             o.append("        const int aidx = ad * n_ac + c0 + j;")
             o.append(f"        const int obi = ((c0 + j) / ostr) % {nob};")
             o.append(f"        #pragma unroll\n        for (int kb = 0; kb < {SB}; ++kb) {{")
