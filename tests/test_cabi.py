@@ -75,3 +75,47 @@ def test_launch_record_layout_matches_the_header(tmp_path):
     want = [ctypes.sizeof(LaunchRec), LaunchRec.kernel.offset, LaunchRec.args.offset, LaunchRec.seed.offset,
             LaunchRec.with_seed.offset, ctypes.sizeof(LaunchArgs)]
     assert got == want
+
+
+def test_launch_list_rejects_bad_arguments_without_gpu():
+    """Argument validation of lcmx_launch_list happens before any CUDA call."""
+    from pylcm_b200 import runtime
+
+    lib = runtime.load_library()
+    assert lib.lcmx_launch_list(None, 0, None) == 0  # nothing to launch
+    assert lib.lcmx_launch_list(None, 2, None) == 1  # LCMX_ERR_ARGS
+    recs = (runtime.LaunchRec * 1)()  # a record without module or kernel
+    assert lib.lcmx_launch_list(recs, 1, None) == 1
+
+
+def test_bundle_merges_runs_of_item_launches():
+    """runtime.bundle: consecutive PreparedLaunch entries become one launch
+    list (in order), other callables stay where they are."""
+    from pylcm_b200 import runtime
+
+    calls = []
+
+    class FakeLib:
+        def lcmx_launch_list(self, arr, n, stream):
+            calls.append(("list", [arr[i].kernel for i in range(n)], stream))
+            return 0
+
+    class FakeCtx:
+        lib = FakeLib()
+
+        def check(self, rc):
+            raise AssertionError(rc)
+
+    def prep(name, seed=None):
+        return runtime.PreparedLaunch(FakeCtx(), (1, name.encode(), 16, 32, 1, 1, 0, 256, 0, seed))
+
+    def other(stream):
+        calls.append(("other", stream))
+
+    ops = [prep("a"), prep("b", seed=3), other, prep("c"), other, other, prep("d")]
+    out = runtime.bundle(ops)
+    assert len(out) == 6
+    for f in out:
+        f(7)
+    assert calls == [("list", [b"a", b"b"], 7), ("other", 7), ("list", [b"c"], 7), ("other", 7), ("other", 7),
+                     ("list", [b"d"], 7)]
