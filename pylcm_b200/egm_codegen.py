@@ -23,7 +23,6 @@ library FUES scan (``lcmx_fues_scan``):
 from __future__ import annotations
 
 import hashlib
-import itertools
 
 from pylcm_b200 import ir
 from pylcm_b200.codegen import _EXTRA_DEVICE, Emitter, device_header

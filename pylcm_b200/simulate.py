@@ -24,7 +24,7 @@ in:
 from __future__ import annotations
 
 import math
-from typing import Any, Mapping
+from typing import Mapping
 
 import numpy as np
 
