@@ -119,3 +119,23 @@ def test_collapsed_rows_eligibility():
     assert "lcm_sc1_" in s32 and "lcm_interp1s" in s32 and "nLine" in s32
     assert "lcm_sc1_" not in src("fp32", collapse=False)
     assert "lcm_sc1_" not in src("fp64")
+
+
+def test_collapsed_rows_refused_when_the_collapsed_axis_reads_the_line_state(monkeypatch):
+    """Human capital whose law reads wealth (the line state) cannot be
+    interpolated once per line: the search keeps the bilinear read."""
+    import dataclasses
+
+    from pylcm_b200 import examples as EX
+    from pylcm_b200.engine import default_config
+
+    def next_hc(human_capital, hours, wealth):
+        return 0.95 * human_capital + 0.1 * hours + 1e-4 * wealth
+
+    monkeypatch.setattr(EX, "_hc_next_hc", next_hc)
+    model, params = EX.hc_model(3, 10, 4, 4, 8), EX.hc_params(0, 4)
+    alive = next(s for s in model.regime_specs if s.name == "alive")
+    cfg = {s.name: default_config(s, "fp32", 1) for s in model.regime_specs}
+    eng = SolveEngine(model, "fp32", configs=cfg)
+    src = eng.kernels(alive, eng.targets_at(alive, 0), params).source()
+    assert "lcm_sc1_" not in src and "nLine" not in src
