@@ -52,6 +52,8 @@ from pylcm_b200.regime import (
 )
 from pylcm_b200.solvers import (
     DCEGM,
+    EGM,
+    NEGM,
     ExactEnvelope,
     FUESEnvelope,
     GridSearch,
@@ -62,6 +64,8 @@ from pylcm_b200.solvers import (
 
 __all__ = [
     "DCEGM",
+    "EGM",
+    "NEGM",
     "AdmissionError",
     "AgeGrid",
     "ConsumptionSavingsRegime",

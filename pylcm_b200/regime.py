@@ -75,6 +75,15 @@ class Regime:
         overlap = set(self.states) & set(self.actions)
         if overlap:
             raise RegimeInitializationError(f"names used as both state and action: {sorted(overlap)}")
+        if isinstance(self.solver, (_solvers.EGM, _solvers.NEGM)):
+            raise NotImplementedError(
+                f"{type(self.solver).__name__} is not implemented on the GPU path; GridSearch and DCEGM are "
+                "(DCEGM solves the one-asset problem without discrete choices too)"
+            )
+        if not isinstance(self.solver, (_solvers.GridSearch, _solvers.DCEGM)):
+            raise RegimeInitializationError(
+                f"unknown solver {type(self.solver).__name__}: use GridSearch or DCEGM"
+            )
         if not isinstance(self, ConsumptionSavingsRegime) and isinstance(self.solver, _solvers.DCEGM):
             raise RegimeInitializationError(
                 "EGM-family solvers require regime-owned margin declarations: use "

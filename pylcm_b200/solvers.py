@@ -94,3 +94,31 @@ class DCEGM:
             raise ValueError("refined_grid_factor must be >= 1")
         if self.n_constrained_points < 1:
             raise ValueError("n_constrained_points must be >= 1")
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
+class EGM:
+    """The plain one-asset endogenous grid method (``src/_lcm/solution/egm.py:70-90``).
+
+    Accepted as a configuration so that models naming it load; a regime
+    declaring it is refused when the regime is built (the GPU path implements
+    ``DCEGM``, which solves the same one-state, no-kink problem: its envelope
+    keeps every candidate of a monotone row).
+    """
+
+    savings_grid: Any
+
+
+@dataclasses.dataclass(frozen=True, kw_only=True)
+class NEGM:
+    """Nested EGM: an outer grid search over a second continuous margin with an
+    inner ``DCEGM`` solve (``src/_lcm/solution/negm.py:72-120``).  Accepted as a
+    configuration; a regime declaring it is refused when the regime is built."""
+
+    inner: Any
+    outer_grid: Any
+    outer_batch_size: int = 0
+
+    def __post_init__(self) -> None:
+        if int(self.outer_batch_size) < 0:
+            raise ValueError("outer_batch_size must be >= 0")

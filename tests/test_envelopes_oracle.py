@@ -196,3 +196,27 @@ def test_every_envelope_is_the_identity_on_one_concave_branch():
         keep = ~np.isnan(rg)
         assert n == 5
         np.testing.assert_allclose(np.interp(q, rg[keep], rv[keep]), np.interp(q, g, v), atol=1e-12)
+
+
+def test_egm_and_negm_configurations_are_refused_clearly():
+    """EGM and NEGM load as configurations (so models naming them import) and
+    a regime declaring either is refused with NotImplementedError; an unknown
+    solver object is refused too."""
+    import pytest
+
+    from pylcm_b200 import EGM, NEGM, DCEGM, IrregSpacedGrid, LinSpacedGrid, Regime
+    from pylcm_b200.exceptions import RegimeInitializationError
+
+    sav = IrregSpacedGrid(points=(0.0, 1.0, 2.0))
+    egm = EGM(savings_grid=sav)
+    negm = NEGM(inner=DCEGM(savings_grid=sav), outer_grid=LinSpacedGrid(start=0, stop=1, n_points=3))
+    with pytest.raises(ValueError):
+        NEGM(inner=DCEGM(savings_grid=sav), outer_grid=sav, outer_batch_size=-1)
+    base = dict(actions={"c": LinSpacedGrid(start=1, stop=2, n_points=3)},
+                states={"w": LinSpacedGrid(start=1, stop=2, n_points=3)},
+                functions={"utility": lambda c: c}, transition=lambda: 0)
+    for solver in (egm, negm):
+        with pytest.raises(NotImplementedError, match=type(solver).__name__):
+            Regime(solver=solver, **base)
+    with pytest.raises(RegimeInitializationError, match="unknown solver"):
+        Regime(solver=object(), **base)
